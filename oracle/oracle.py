@@ -1,0 +1,461 @@
+"""Test infrastructure only: ctypes access to the two CPU oracles.
+
+``Oracle``    -- this project's C restatement (oracle/liboracle.so, oracle.c).
+``Reference`` -- the reference LinAlgLib host path compiled from its own sources
+                 (oracle/_ref/liblinalg_ref.so, built by oracle/Makefile), or
+                 None-returning ``load_reference()`` where it was not built.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline arm use this
+module, as the checker; the CUDA library never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "liblinalg_ref.so")
+
+_i = C.c_int
+_d = C.c_double
+_p = C.c_void_p
+
+
+def build(reference: bool = True) -> None:
+    """Compile the oracle (and, where the reference sources exist, oracle/_ref)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if reference:
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class _Csr(C.Structure):
+    _fields_ = [("m", _i), ("n", _i), ("nnz", _i), ("rp", C.POINTER(_i)),
+                ("ci", C.POINTER(_i)), ("v", C.POINTER(_d))]
+
+
+def _csr_in(rp, ci, v, n=None):
+    rp = np.ascontiguousarray(rp, dtype=np.int32)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    m = rp.size - 1
+    s = _Csr(m, m if n is None else n, int(rp[-1]),
+             rp.ctypes.data_as(C.POINTER(_i)), ci.ctypes.data_as(C.POINTER(_i)),
+             v.ctypes.data_as(C.POINTER(_d)))
+    s._keep = (rp, ci, v)
+    return s
+
+
+def _csr_out(s: _Csr):
+    m, nnz = s.m, s.nnz
+    rp = np.ctypeslib.as_array(s.rp, shape=(m + 1,)).copy()
+    ci = np.ctypeslib.as_array(s.ci, shape=(max(nnz, 1),))[:nnz].copy()
+    v = np.ctypeslib.as_array(s.v, shape=(max(nnz, 1),))[:nnz].copy()
+    return rp, ci, v, s.n
+
+
+class _Hier(C.Structure):
+    _fields_ = [("levels", _i), ("A", _Csr * 21), ("P", _Csr * 20), ("R", _Csr * 20),
+                ("coarse_inv", C.POINTER(_d))]
+
+
+class Oracle:
+    """The C restatement (oracle.c)."""
+
+    SA, UA, RS = 0, 1, 2
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build(reference=False)
+        L = C.CDLL(path)
+        self.L = L
+        P = C.POINTER(_Csr)
+        L.orc_csr_free.argtypes = [P]
+        L.orc_spmv.argtypes = [P, _d, _p, _d, _p]
+        L.orc_residual.argtypes = [P, _p, _p, _p]
+        L.orc_transpose.argtypes = [P, P]
+        L.orc_spgemm.argtypes = [P, P, P]
+        L.orc_spgeam.argtypes = [_d, P, _d, P, P]
+        L.orc_strength.argtypes = [P, _d, _p]
+        L.orc_pmis.argtypes = [P, _p, _p, _p]
+        L.orc_sa_prolongation.argtypes = [P, _p, _p, _d, P]
+        L.orc_ua_prolongation.argtypes = [P, _p, P]
+        L.orc_classical_strength.argtypes = [P, _d, _p, P]
+        L.orc_cfpoints.argtypes = [P, P, _p]
+        L.orc_direct_interpolation.argtypes = [P, P, _p, P]
+        L.orc_amg_setup.argtypes = [_i, P, _i]
+        L.orc_amg_setup.restype = C.POINTER(_Hier)
+        L.orc_hier_free.argtypes = [C.POINTER(_Hier)]
+        L.orc_vcycle.argtypes = [C.POINTER(_Hier), _i, _p, _p, _i, _i, _i, _d, _i]
+        L.orc_amg_pcg.argtypes = [C.POINTER(_Hier), _p, _p, _i, _i, _i, _d, _i, _d, _d, _i,
+                                  C.POINTER(_d)]
+        L.orc_amg_solve.argtypes = [C.POINTER(_Hier), _p, _p, _i, _i, _i, _d, _i, _d, _d, _i]
+        L.orc_cg.argtypes = [P, _p, _p, _i, _d, _d, _i]
+        L.orc_exclusive_scan_i64.argtypes = [_p, _i]
+
+    # -- kernels
+    def spmv(self, A, x, alpha=1.0, beta=0.0, y=None):
+        s = _csr_in(*A[:3], n=A[3] if len(A) > 3 else None)
+        y = np.zeros(s.m) if y is None else np.array(y, dtype=np.float64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        self.L.orc_spmv(C.byref(s), alpha, _ptr(x), beta, _ptr(y))
+        return y
+
+    def residual(self, A, x, b):
+        s = _csr_in(*A[:3], n=A[3] if len(A) > 3 else None)
+        r = np.zeros(s.m)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.L.orc_residual(C.byref(s), _ptr(x), _ptr(b), _ptr(r))
+        return r
+
+    def _out(self, fn, *args):
+        o = _Csr()
+        fn(*args, C.byref(o))
+        res = _csr_out(o)
+        self.L.orc_csr_free(C.byref(o))
+        return res
+
+    def transpose(self, A):
+        s = _csr_in(*A[:3], n=A[3] if len(A) > 3 else None)
+        return self._out(self.L.orc_transpose, C.byref(s))
+
+    def spgemm(self, A, B):
+        a = _csr_in(*A[:3], n=A[3] if len(A) > 3 else None)
+        b = _csr_in(*B[:3], n=B[3] if len(B) > 3 else None)
+        return self._out(self.L.orc_spgemm, C.byref(a), C.byref(b))
+
+    def spgeam(self, alpha, A, beta, B):
+        a = _csr_in(*A[:3], n=A[3] if len(A) > 3 else None)
+        b = _csr_in(*B[:3], n=B[3] if len(B) > 3 else None)
+        return self._out(self.L.orc_spgeam, alpha, C.byref(a), beta, C.byref(b))
+
+    def strength(self, A, eps):
+        s = _csr_in(*A[:3])
+        conn = np.zeros(s.nnz, dtype=np.int32)
+        self.L.orc_strength(C.byref(s), eps, _ptr(conn))
+        return conn
+
+    def pmis(self, A, conn):
+        s = _csr_in(*A[:3])
+        conn = np.ascontiguousarray(conn, dtype=np.int32)
+        agg = np.zeros(s.m, dtype=np.int64)
+        rounds = _i(0)
+        self.L.orc_pmis(C.byref(s), _ptr(conn), _ptr(agg), C.byref(rounds))
+        return agg, rounds.value
+
+    def sa_prolongation(self, A, conn, agg, relax=2.0 / 3.0):
+        s = _csr_in(*A[:3])
+        conn = np.ascontiguousarray(conn, dtype=np.int32)
+        agg = np.ascontiguousarray(agg, dtype=np.int64)
+        return self._out(self.L.orc_sa_prolongation, C.byref(s), _ptr(conn), _ptr(agg), relax)
+
+    def ua_prolongation(self, A, agg):
+        s = _csr_in(*A[:3])
+        agg = np.ascontiguousarray(agg, dtype=np.int64)
+        return self._out(self.L.orc_ua_prolongation, C.byref(s), _ptr(agg))
+
+    def classical_strength(self, A, theta=0.2):
+        s = _csr_in(*A[:3])
+        conn = np.zeros(s.nnz, dtype=np.int32)
+        S = self._out(self.L.orc_classical_strength, C.byref(s), theta, _ptr(conn))
+        return conn, S
+
+    def cfpoints(self, S):
+        s = _csr_in(*S[:3])
+        st = _Csr()
+        self.L.orc_transpose(C.byref(s), C.byref(st))
+        cf = np.zeros(s.m, dtype=np.uint32)
+        self.L.orc_cfpoints(C.byref(s), C.byref(st), _ptr(cf))
+        self.L.orc_csr_free(C.byref(st))
+        return cf
+
+    def direct_interpolation(self, A, S, cf):
+        a = _csr_in(*A[:3])
+        s = _csr_in(*S[:3])
+        cf = np.ascontiguousarray(cf, dtype=np.uint32)
+        return self._out(self.L.orc_direct_interpolation, C.byref(a), C.byref(s), _ptr(cf))
+
+    def exclusive_scan(self, x):
+        x = np.array(x, dtype=np.int64)
+        self.L.orc_exclusive_scan_i64(_ptr(x), x.size)
+        return x
+
+    # -- hierarchy / solvers
+    def amg_setup(self, A, kind=0, max_level=20):
+        return OracleHierarchy(self, A, kind, max_level)
+
+    def cg(self, A, b, x0=None, jacobi=False, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000):
+        s = _csr_in(*A[:3])
+        x = np.zeros(s.m) if x0 is None else np.array(x0, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        it = self.L.orc_cg(C.byref(s), _ptr(b), _ptr(x), int(jacobi), rel_tol, abs_tol, max_iter)
+        return x, it
+
+
+class OracleHierarchy:
+    def __init__(self, orc: Oracle, A, kind, max_level):
+        self.orc = orc
+        s = _csr_in(*A[:3])
+        self.h = orc.L.orc_amg_setup(kind, C.byref(s), max_level)
+
+    def __del__(self):
+        try:
+            self.orc.L.orc_hier_free(self.h)
+        except Exception:
+            pass
+
+    @property
+    def levels(self):
+        return self.h.contents.levels
+
+    def A(self, l):
+        return _csr_out(self.h.contents.A[l])
+
+    def P(self, l):
+        return _csr_out(self.h.contents.P[l])
+
+    def R(self, l):
+        return _csr_out(self.h.contents.R[l])
+
+    def vcycle(self, b, n1=1, n2=1, smoother=0, omega=1.0, coarse=0, x0=None):
+        m = self.h.contents.A[0].m
+        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.orc.L.orc_vcycle(self.h, 0, _ptr(x), _ptr(b), n1, n2, smoother, omega, coarse)
+        return x
+
+    def pcg(self, b, x0=None, n1=1, n2=1, smoother=0, omega=1.0, coarse=0, rel_tol=1e-8,
+            abs_tol=0.0, max_iter=1000):
+        m = self.h.contents.A[0].m
+        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        rel = _d(0)
+        it = self.orc.L.orc_amg_pcg(self.h, _ptr(b), _ptr(x), n1, n2, smoother, omega, coarse,
+                                    rel_tol, abs_tol, max_iter, C.byref(rel))
+        return x, it, rel.value
+
+    def amg_solve(self, b, x0=None, n1=1, n2=1, smoother=0, omega=1.0, coarse=0,
+                  rel_tol=1e-6, abs_tol=1e-6, max_cycle=200):
+        m = self.h.contents.A[0].m
+        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        it = self.orc.L.orc_amg_solve(self.h, _ptr(b), _ptr(x), n1, n2, smoother, omega, coarse,
+                                      rel_tol, abs_tol, max_cycle)
+        return x, it
+
+
+# ----------------------------------------------------------------- reference
+class Reference:
+    """The reference host library compiled from its sources (oracle/_ref)."""
+
+    SA, UA, RS = 0, 1, 2
+
+    def __init__(self, path: str = REF_SO):
+        L = C.CDLL(path)
+        self.L = L
+        L.ref_amg_setup.restype = _p
+        L.ref_amg_setup.argtypes = [_i, _i, _i, _i, _p, _p, _p, _i]
+        L.ref_hier_free.argtypes = [_p]
+        L.ref_hier_levels.argtypes = [_p]
+        L.ref_hier_dims.argtypes = [_p, _i, _i, _p, _p, _p]
+        L.ref_hier_copy.argtypes = [_p, _i, _i, _p, _p, _p]
+        L.ref_amg_pcg.argtypes = [_p, _p, _p, _i, _i, _i, _d, _d, _i]
+        L.ref_amg_solve.argtypes = [_p, _p, _p, _i, _i, _i, _i, _d, _d, _i]
+        L.ref_amg_vcycle.argtypes = [_p, _p, _p, _i, _i, _i]
+        L.ref_cg.argtypes = [_i, _i, _p, _p, _p, _p, _p, _i, _d, _d, _i]
+        L.ref_gmres.argtypes = [_i, _i, _p, _p, _p, _p, _p, _i, _p, _i, _i, _d, _d, _i]
+        L.ref_spmv.argtypes = [_i, _i, _i, _p, _p, _p, _d, _p, _d, _p]
+        L.ref_residual.argtypes = [_i, _i, _i, _p, _p, _p, _p, _p, _p]
+        L.ref_spgemm.restype = _p
+        L.ref_spgemm.argtypes = [_i, _i, _i, _p, _p, _p, _i, _i, _i, _p, _p, _p]
+        L.ref_spgeam.restype = _p
+        L.ref_spgeam.argtypes = [_d, _i, _i, _i, _p, _p, _p, _d, _i, _p, _p, _p]
+        L.ref_transpose.restype = _p
+        L.ref_transpose.argtypes = [_i, _i, _i, _p, _p, _p]
+        L.ref_mat_dims.argtypes = [_p, _p, _p, _p]
+        L.ref_mat_copy.argtypes = [_p, _p, _p, _p]
+        L.ref_mat_free.argtypes = [_p]
+        L.ref_strength.argtypes = [_i, _i, _p, _p, _p, _d, _p]
+        L.ref_pmis.argtypes = [_i, _i, _p, _p, _p, _p, _p]
+        L.ref_classical_strength.restype = _p
+        L.ref_classical_strength.argtypes = [_i, _i, _p, _p, _p, _d, _p]
+        L.ref_cfpoints.argtypes = [_i, _i, _p, _p, _p, _p]
+        L.ref_exclusive_scan_i64.argtypes = [_p, _i]
+
+    @staticmethod
+    def _arr(A):
+        rp = np.ascontiguousarray(A[0], dtype=np.int32)
+        ci = np.ascontiguousarray(A[1], dtype=np.int32)
+        v = np.ascontiguousarray(A[2], dtype=np.float64)
+        n = A[3] if len(A) > 3 else rp.size - 1
+        return rp, ci, v, rp.size - 1, n, int(rp[-1])
+
+    def _mat(self, M):
+        m, n, z = _i(), _i(), _i()
+        self.L.ref_mat_dims(M, C.byref(m), C.byref(n), C.byref(z))
+        rp = np.zeros(m.value + 1, dtype=np.int32)
+        ci = np.zeros(max(z.value, 1), dtype=np.int32)
+        v = np.zeros(max(z.value, 1), dtype=np.float64)
+        self.L.ref_mat_copy(M, _ptr(rp), _ptr(ci), _ptr(v))
+        self.L.ref_mat_free(M)
+        return rp, ci[:z.value], v[:z.value], n.value
+
+    def spmv(self, A, x, alpha=1.0, beta=0.0, y=None):
+        rp, ci, v, m, n, z = self._arr(A)
+        y = np.zeros(m) if y is None else np.array(y, dtype=np.float64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        self.L.ref_spmv(m, n, z, _ptr(rp), _ptr(ci), _ptr(v), alpha, _ptr(x), beta, _ptr(y))
+        return y
+
+    def residual(self, A, x, b):
+        rp, ci, v, m, n, z = self._arr(A)
+        r = np.zeros(m)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.L.ref_residual(m, n, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(x), _ptr(b), _ptr(r))
+        return r
+
+    def spgemm(self, A, B):
+        a = self._arr(A)
+        b = self._arr(B)
+        M = self.L.ref_spgemm(a[3], a[4], a[5], _ptr(a[0]), _ptr(a[1]), _ptr(a[2]),
+                              b[3], b[4], b[5], _ptr(b[0]), _ptr(b[1]), _ptr(b[2]))
+        return self._mat(M)
+
+    def spgeam(self, alpha, A, beta, B):
+        a = self._arr(A)
+        b = self._arr(B)
+        M = self.L.ref_spgeam(alpha, a[3], a[4], a[5], _ptr(a[0]), _ptr(a[1]), _ptr(a[2]),
+                              beta, b[5], _ptr(b[0]), _ptr(b[1]), _ptr(b[2]))
+        return self._mat(M)
+
+    def transpose(self, A):
+        a = self._arr(A)
+        return self._mat(self.L.ref_transpose(a[3], a[4], a[5], _ptr(a[0]), _ptr(a[1]),
+                                              _ptr(a[2])))
+
+    def strength(self, A, eps):
+        rp, ci, v, m, n, z = self._arr(A)
+        conn = np.zeros(z, dtype=np.int32)
+        self.L.ref_strength(m, z, _ptr(rp), _ptr(ci), _ptr(v), eps, _ptr(conn))
+        return conn
+
+    def pmis(self, A, conn):
+        rp, ci, v, m, n, z = self._arr(A)
+        conn = np.ascontiguousarray(conn, dtype=np.int32)
+        agg = np.zeros(m, dtype=np.int64)
+        self.L.ref_pmis(m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(conn), _ptr(agg))
+        return agg
+
+    def classical_strength(self, A, theta=0.2):
+        rp, ci, v, m, n, z = self._arr(A)
+        conn = np.zeros(z, dtype=np.int32)
+        M = self.L.ref_classical_strength(m, z, _ptr(rp), _ptr(ci), _ptr(v), theta, _ptr(conn))
+        return conn, self._mat(M)
+
+    def cfpoints(self, S):
+        rp, ci, v, m, n, z = self._arr(S)
+        cf = np.zeros(m, dtype=np.uint32)
+        self.L.ref_cfpoints(m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(cf))
+        return cf
+
+    def exclusive_scan(self, x):
+        x = np.array(x, dtype=np.int64)
+        self.L.ref_exclusive_scan_i64(_ptr(x), x.size)
+        return x
+
+    def amg_setup(self, A, kind=0, max_level=20):
+        return ReferenceHierarchy(self, A, kind, max_level)
+
+    def cg(self, A, b, x0=None, jacobi=False, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000):
+        rp, ci, v, m, n, z = self._arr(A)
+        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        it = self.L.ref_cg(m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(b), _ptr(x), int(jacobi),
+                           rel_tol, abs_tol, max_iter)
+        return x, it
+
+    def gmres(self, A, b, restart=30, hier=None, x0=None, rel_tol=1e-6, abs_tol=1e-6,
+              max_iter=1000):
+        rp, ci, v, m, n, z = self._arr(A)
+        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        it = self.L.ref_gmres(m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(b), _ptr(x), restart,
+                              hier.h if hier is not None else None, 1, 1, rel_tol, abs_tol,
+                              max_iter)
+        return x, it
+
+
+class ReferenceHierarchy:
+    def __init__(self, ref: Reference, A, kind, max_level):
+        self.ref = ref
+        rp, ci, v, m, n, z = ref._arr(A)
+        self.h = ref.L.ref_amg_setup(kind, m, n, z, _ptr(rp), _ptr(ci), _ptr(v), max_level)
+
+    def __del__(self):
+        try:
+            self.ref.L.ref_hier_free(self.h)
+        except Exception:
+            pass
+
+    @property
+    def levels(self):
+        return self.ref.L.ref_hier_levels(self.h)
+
+    def _get(self, l, which):
+        m, n, z = _i(), _i(), _i()
+        self.ref.L.ref_hier_dims(self.h, l, which, C.byref(m), C.byref(n), C.byref(z))
+        rp = np.zeros(m.value + 1, dtype=np.int32)
+        ci = np.zeros(max(z.value, 1), dtype=np.int32)
+        v = np.zeros(max(z.value, 1), dtype=np.float64)
+        self.ref.L.ref_hier_copy(self.h, l, which, _ptr(rp), _ptr(ci), _ptr(v))
+        return rp, ci[:z.value], v[:z.value], n.value
+
+    def A(self, l):
+        return self._get(l, 0)
+
+    def P(self, l):
+        return self._get(l, 1)
+
+    def R(self, l):
+        return self._get(l, 2)
+
+    def vcycle(self, b, n1=1, n2=1, smoother=0):
+        m = self.A(0)[0].size - 1
+        z = np.zeros(m)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.ref.L.ref_amg_vcycle(self.h, _ptr(b), _ptr(z), n1, n2, smoother)
+        return z
+
+    def pcg(self, b, x0=None, n1=1, n2=1, smoother=0, rel_tol=1e-8, abs_tol=1e-300,
+            max_iter=1000):
+        m = self.A(0)[0].size - 1
+        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        it = self.ref.L.ref_amg_pcg(self.h, _ptr(b), _ptr(x), n1, n2, smoother, rel_tol,
+                                    abs_tol, max_iter)
+        return x, it
+
+    def amg_solve(self, b, x0=None, n1=1, n2=1, cycle=0, smoother=0, rel_tol=1e-6,
+                  abs_tol=1e-6, max_cycle=200):
+        m = self.A(0)[0].size - 1
+        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        it = self.ref.L.ref_amg_solve(self.h, _ptr(b), _ptr(x), n1, n2, cycle, smoother,
+                                      rel_tol, abs_tol, max_cycle)
+        return x, it
+
+
+def load_reference():
+    """The compiled reference, or None where oracle/_ref was not built."""
+    if os.path.exists(REF_SO):
+        return Reference(REF_SO)
+    return None
