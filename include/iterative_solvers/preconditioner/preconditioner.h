@@ -1,0 +1,91 @@
+// Preconditioner plug-in point (library/include/iterative_solvers/preconditioner/preconditioner.h:59-99)
+// with the Jacobi preconditioner (101-118) and the AMG preconditioner the
+// reference lacks: one multigrid cycle from a zero guess per application.
+#ifndef LINALG_B200_PRECONDITIONER_H
+#define LINALG_B200_PRECONDITIONER_H
+
+#include "../../csr_matrix.h"
+#include "../amg/amg.h"
+#include "lab.h"
+
+namespace linalg
+{
+    class preconditioner
+    {
+    public:
+        preconditioner() {}
+        virtual ~preconditioner() {}
+        virtual void build(const csr_matrix<double>& A)                          = 0;
+        virtual void solve(const vector<double>& rhs, vector<double>& x) const = 0;
+        virtual void move_to_device()                                            = 0;
+        virtual void move_to_host()                                              = 0;
+        virtual bool is_on_host() const                                          = 0;
+
+        // Device preconditioner handle for the fused GPU solvers (null for a
+        // user-defined subclass, which the solvers call through solve()).
+        virtual lab_precond device_handle() const
+        {
+            return nullptr;
+        }
+    };
+
+    class jacobi_precond : public preconditioner
+    {
+    private:
+        lab_precond M       = nullptr;
+        bool        on_host = true;
+
+    public:
+        jacobi_precond();
+        ~jacobi_precond();
+        void        build(const csr_matrix<double>& A) override;
+        void        solve(const vector<double>& rhs, vector<double>& x) const override;
+        void        move_to_device() override;
+        void        move_to_host() override;
+        bool        is_on_host() const override;
+        lab_precond device_handle() const override
+        {
+            return M;
+        }
+    };
+
+    // AMG preconditioner: z = cycle(0; r).  build() runs the setup of `kind`
+    // on A; alternatively attach an existing hierarchy (not owned).
+    class amg_precond : public preconditioner
+    {
+    private:
+        hierarchy        own;
+        const hierarchy* h       = nullptr;
+        lab_precond      M       = nullptr;
+        lab_amg_options  opts;
+        int              kind      = LAB_AMG_SA;
+        int              max_level = 20;
+        bool             on_host   = true;
+
+    public:
+        // Reference defaults for the composition: V-cycle, 1+1 Jacobi sweeps.
+        explicit amg_precond(int presmoothing = 1, int postsmoothing = 1,
+                             cycle cyc = cycle::vcycle, smoother sm = smoother::jacobi,
+                             double jacobi_omega = 1.0);
+        ~amg_precond();
+        void set_setup(lab_amg_kind kind, int max_level);
+        void set_precision(lab_precision p);
+        void set_coarse_solver(lab_coarse c);
+        void attach(const hierarchy& hier);
+        void build(const csr_matrix<double>& A) override;
+        void solve(const vector<double>& rhs, vector<double>& x) const override;
+        void move_to_device() override;
+        void move_to_host() override;
+        bool is_on_host() const override;
+        lab_precond device_handle() const override
+        {
+            return M;
+        }
+        const hierarchy& get_hierarchy() const
+        {
+            return *h;
+        }
+    };
+}
+
+#endif

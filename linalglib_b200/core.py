@@ -1,0 +1,345 @@
+"""Thin Python objects over the C ABI: device CSR matrices, hierarchies,
+preconditioners and solves.  Vectors are float64 CUDA tensors (torch is used
+only for device memory and the current stream).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from ._lib import AmgOptions, IterControl, SolveInfo, call, lib
+
+_initialised = False
+
+
+def init():
+    """Bind the library to torch's current CUDA device (fails loudly without one)."""
+    global _initialised
+    if _initialised:
+        return
+    if not torch.cuda.is_available():
+        raise L.LabError(L.LAB_NO_DEVICE, "linalglib_b200 needs a CUDA device (sm_100a)")
+    torch.cuda.init()
+    call("lab_init", torch.cuda.current_device())
+    _initialised = True
+
+
+def stream_handle(stream=None):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return C.c_void_p(t.ctypes.data)
+    assert t.is_cuda and t.is_contiguous(), "expected a contiguous CUDA tensor"
+    return C.c_void_p(t.data_ptr())
+
+
+def vec(x, dtype=torch.float64):
+    """A contiguous float64 CUDA tensor from numpy / list / tensor."""
+    if isinstance(x, torch.Tensor):
+        return x.to(device="cuda", dtype=dtype).contiguous()
+    return torch.as_tensor(np.asarray(x), dtype=dtype, device="cuda").contiguous()
+
+
+class CsrMatrix:
+    """Device CSR matrix owned by the library (lab_csr)."""
+
+    def __init__(self, handle, owner=True, keep=None):
+        self.h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+        self.owner = owner
+        self._keep = keep  # keeps a parent (e.g. hierarchy) alive for borrowed handles
+
+    @classmethod
+    def from_arrays(cls, row_ptr, col_ind, val, n=None, stream=None):
+        init()
+        if isinstance(row_ptr, torch.Tensor) and row_ptr.is_cuda:
+            rp = row_ptr.to(torch.int32).contiguous()
+            ci = col_ind.to(torch.int32).contiguous()
+            v = val.to(torch.float64).contiguous()
+            where = L.MEM_DEVICE
+            m = rp.numel() - 1
+            nnz = v.numel()
+        else:
+            rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+            ci = np.ascontiguousarray(col_ind, dtype=np.int32)
+            v = np.ascontiguousarray(val, dtype=np.float64)
+            where = L.MEM_HOST
+            m = rp.size - 1
+            nnz = v.size
+        n = m if n is None else n
+        h = C.c_void_p()
+        call("lab_csr_create", C.byref(h), m, n, nnz, ptr(rp), ptr(ci), ptr(v), where,
+             stream_handle(stream))
+        return cls(h)
+
+    def __del__(self):
+        try:
+            if self.owner and self.h:
+                lib().lab_csr_destroy(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+    def info(self):
+        m, n, z = C.c_int64(), C.c_int64(), C.c_int64()
+        call("lab_csr_info", self.h, C.byref(m), C.byref(n), C.byref(z))
+        return m.value, n.value, z.value
+
+    @property
+    def m(self):
+        return self.info()[0]
+
+    @property
+    def n(self):
+        return self.info()[1]
+
+    @property
+    def nnz(self):
+        return self.info()[2]
+
+    def to_numpy(self):
+        m, n, z = self.info()
+        rp = np.zeros(m + 1, dtype=np.int32)
+        ci = np.zeros(max(z, 1), dtype=np.int32)
+        v = np.zeros(max(z, 1), dtype=np.float64)
+        call("lab_csr_copy_to", self.h, ptr(rp), ptr(ci), ptr(v), L.MEM_HOST, stream_handle())
+        return rp, ci[:z], v[:z], n
+
+    def analyse(self):
+        call("lab_spmv_analysis", self.h, stream_handle())
+
+    def set_algorithm(self, alg, lanes=0):
+        call("lab_spmv_set_algorithm", self.h, alg, lanes)
+        self.analyse()
+
+    def algorithm(self):
+        a, w = C.c_int(), C.c_int()
+        call("lab_spmv_get_algorithm", self.h, C.byref(a), C.byref(w))
+        return a.value, w.value
+
+    def spmv(self, x, y=None, alpha=1.0, beta=0.0, stream=None):
+        if y is None:
+            y = torch.zeros(self.m, dtype=torch.float64, device="cuda")
+        call("lab_spmv", alpha, self.h, ptr(x), beta, ptr(y), stream_handle(stream))
+        return y
+
+    def residual(self, x, b, r=None, stream=None):
+        if r is None:
+            r = torch.empty(self.m, dtype=torch.float64, device="cuda")
+        call("lab_residual", self.h, ptr(x), ptr(b), ptr(r), stream_handle(stream))
+        return r
+
+    def spmm(self, X, Y=None, alpha=1.0, beta=0.0):
+        """X: (nrhs, n) row-major tensor == column-major n x nrhs."""
+        k = X.shape[0]
+        if Y is None:
+            Y = torch.zeros((k, self.m), dtype=torch.float64, device="cuda")
+        call("lab_spmm", alpha, self.h, k, ptr(X), X.shape[1], beta, ptr(Y), Y.shape[1],
+             stream_handle())
+        return Y
+
+    def diagonal(self):
+        d = torch.empty(self.m, dtype=torch.float64, device="cuda")
+        call("lab_diagonal", self.h, ptr(d), stream_handle())
+        return d
+
+    def _new(self, fn, *args):
+        h = C.c_void_p()
+        call(fn, *args, C.byref(h), stream_handle())
+        return CsrMatrix(h)
+
+    def transpose(self):
+        return self._new("lab_transpose", self.h)
+
+    def spgemm(self, B):
+        return self._new("lab_spgemm", self.h, B.h)
+
+    def spgeam(self, alpha, beta, B):
+        return self._new("lab_spgeam", alpha, self.h, beta, B.h)
+
+
+# ---------------------------------------------------------------- BLAS-1
+def dot(x, y):
+    r = C.c_double()
+    call("lab_dot", x.numel(), ptr(x), ptr(y), C.byref(r), stream_handle())
+    return r.value
+
+
+def norm_inf(x):
+    r = C.c_double()
+    call("lab_norm_inf", x.numel(), ptr(x), C.byref(r), stream_handle())
+    return r.value
+
+
+def norm_euclid(x):
+    r = C.c_double()
+    call("lab_norm_euclid", x.numel(), ptr(x), C.byref(r), stream_handle())
+    return r.value
+
+
+def axpy(alpha, x, y):
+    call("lab_axpy", x.numel(), alpha, ptr(x), ptr(y), stream_handle())
+
+
+def axpby(alpha, x, beta, y):
+    call("lab_axpby", x.numel(), alpha, ptr(x), beta, ptr(y), stream_handle())
+
+
+def axpbypgz(alpha, x, beta, y, gamma, z):
+    call("lab_axpbypgz", x.numel(), alpha, ptr(x), beta, ptr(y), gamma, ptr(z), stream_handle())
+
+
+def exclusive_scan(x):
+    """In-place exclusive scan of an int32/int64 CUDA tensor."""
+    fn = "lab_exclusive_scan_i64" if x.dtype == torch.int64 else "lab_exclusive_scan_i32"
+    call(fn, x.numel(), ptr(x), stream_handle())
+    return x
+
+
+def launch_count():
+    return lib().lab_launch_count()
+
+
+# ---------------------------------------------------------------- options
+def amg_options(n1=1, n2=1, cycle=L.CYCLE_V, smoother=L.SMOOTH_JACOBI, omega=1.0,
+                omega_sor=0.5, coarse=L.COARSE_DIRECT, precision=L.PREC_FP64):
+    o = AmgOptions()
+    lib().lab_amg_options_default(C.byref(o))
+    o.n1, o.n2, o.cycle, o.smoother = n1, n2, cycle, smoother
+    o.omega, o.omega_sor, o.coarse, o.precision = omega, omega_sor, coarse, precision
+    return o
+
+
+def iter_control(rel_tol=1e-6, abs_tol=1e-6, max_iter=1000, max_cycle=200):
+    c = IterControl()
+    c.rel_tol, c.abs_tol, c.max_iter, c.max_cycle = rel_tol, abs_tol, max_iter, max_cycle
+    return c
+
+
+# ---------------------------------------------------------------- AMG
+class Hierarchy:
+    def __init__(self, A: CsrMatrix, kind=L.AMG_SA, max_level=20, stream=None):
+        init()
+        self.h = C.c_void_p()
+        call("lab_amg_setup", kind, A.h, max_level, C.byref(self.h), stream_handle(stream))
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().lab_hierarchy_destroy(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+    @property
+    def levels(self):
+        n = C.c_int()
+        call("lab_hierarchy_levels", self.h, C.byref(n))
+        return n.value
+
+    def setup_ms(self):
+        d = C.c_double()
+        call("lab_hierarchy_setup_ms", self.h, C.byref(d))
+        return d.value
+
+    def _level(self, l, which):
+        hs = [C.c_void_p(), C.c_void_p(), C.c_void_p()]
+        args = [C.byref(hs[k]) if k == which else None for k in range(3)]
+        call("lab_hierarchy_level", self.h, l, *args)
+        return CsrMatrix(hs[which], owner=False, keep=self)
+
+    def A(self, l):
+        return self._level(l, 0)
+
+    def P(self, l):
+        return self._level(l, 1)
+
+    def R(self, l):
+        return self._level(l, 2)
+
+    def cycle(self, b, x=None, options=None):
+        options = options or amg_options()
+        if x is None:
+            x = torch.zeros_like(b)
+        call("lab_amg_cycle", self.h, C.byref(options), ptr(b), ptr(x), stream_handle())
+        return x
+
+    def solve(self, b, x=None, options=None, control=None):
+        options = options or amg_options()
+        control = control or iter_control()
+        if x is None:
+            x = torch.zeros_like(b)
+        info = SolveInfo()
+        call("lab_amg_solve", self.h, C.byref(options), ptr(b), ptr(x), C.byref(control),
+             C.byref(info), stream_handle())
+        return x, info
+
+
+class Preconditioner:
+    def __init__(self, h, keep=None):
+        self.h = h
+        self._keep = keep
+
+    @classmethod
+    def amg(cls, hier: Hierarchy, options=None):
+        options = options or amg_options()
+        h = C.c_void_p()
+        call("lab_precond_create_amg", hier.h, C.byref(options), C.byref(h), stream_handle())
+        return cls(h, keep=hier)
+
+    @classmethod
+    def jacobi(cls, A: CsrMatrix):
+        h = C.c_void_p()
+        call("lab_precond_create_jacobi", A.h, C.byref(h), stream_handle())
+        return cls(h, keep=A)
+
+    def apply(self, r, z=None):
+        if z is None:
+            z = torch.empty_like(r)
+        call("lab_precond_apply", self.h, ptr(r), ptr(z), stream_handle())
+        return z
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().lab_precond_destroy(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+
+def pcg(A: CsrMatrix, b, x=None, M: Preconditioner | None = None, control=None):
+    control = control or iter_control()
+    if x is None:
+        x = torch.zeros_like(b)
+    info = SolveInfo()
+    call("lab_pcg_solve", A.h, M.h if M is not None else None, ptr(b), ptr(x),
+         C.byref(control), C.byref(info), stream_handle())
+    return x, info
+
+
+def pcg_host(A: CsrMatrix, b: np.ndarray, x: np.ndarray, M=None, control=None):
+    """PCG with host (numpy) b and x: the copies happen inside the call."""
+    control = control or iter_control()
+    info = SolveInfo()
+    call("lab_pcg_solve_host", A.h, M.h if M is not None else None, ptr(b), ptr(x),
+         C.byref(control), C.byref(info), stream_handle())
+    return x, info
+
+
+def gmres(A: CsrMatrix, b, x=None, M: Preconditioner | None = None, restart=30, control=None):
+    control = control or iter_control()
+    if x is None:
+        x = torch.zeros_like(b)
+    info = SolveInfo()
+    call("lab_gmres_solve", A.h, M.h if M is not None else None, restart, ptr(b), ptr(x),
+         C.byref(control), C.byref(info), stream_handle())
+    return x, info

@@ -1,0 +1,974 @@
+// AMG setup on the device: strength of connection, PMIS aggregation, SA / UA
+// prolongation, RS C/F splitting and direct interpolation, and the level loop.
+// Integer outputs and every floating-point value of P and A_c are bit-identical
+// to the reference host implementation (see the per-kernel citations).
+#include "amg.cuh"
+#include "esc.cuh"
+
+#include <cfloat>
+#include <chrono>
+
+namespace lab
+{
+    // ------------------------------------------------------------ strength
+    // host_amg_strength.cpp:33-70:
+    //   conn[j] = (c != i) && |a_ij| >= eps * sqrt(|d_i| * |d_c|)
+    template <int LANES>
+    __global__ void k_strength(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                               const double* __restrict__ v, const double* __restrict__ d,
+                               int64_t m, double eps, int32_t* __restrict__ conn)
+    {
+        int64_t t    = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        int64_t i    = t / LANES;
+        int     lane = (int)(t % LANES);
+        if(i >= m)
+            return;
+        const double di = fabs(d[i]);
+        for(int j = rp[i] + lane; j < rp[i + 1]; j += LANES)
+        {
+            const int    c   = ci[j];
+            const double thr = __dmul_rn(eps, __dsqrt_rn(__dmul_rn(di, fabs(d[c]))));
+            conn[j]          = (c != i) && (fabs(v[j]) >= thr);
+        }
+    }
+
+    __global__ void k_diag_only(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                const double* __restrict__ v, int64_t m, double* __restrict__ d)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        double dd = 0.0;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+            if(ci[j] == i)
+            {
+                dd = v[j];
+                break;
+            }
+        d[i] = dd;
+    }
+
+    lab_status amg_strength(const lab_csr_impl* A, double eps, int32_t* conn, cudaStream_t s)
+    {
+        if(A->m == 0)
+            return LAB_OK;
+        dbuf<double> d;
+        LAB_TRY(d.alloc((size_t)A->m, s));
+        LAB_LAUNCH(k_diag_only, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, s, A->row_ptr,
+                   A->col_ind, A->val, A->m, d.get());
+        double avg = (double)A->nnz / (double)A->m;
+        if(avg <= 12.0)
+            LAB_LAUNCH(k_strength<1>, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, s,
+                       A->row_ptr, A->col_ind, A->val, d.get(), A->m, eps, conn);
+        else
+            LAB_LAUNCH(k_strength<32>, (unsigned)ceil_div<int64_t>(A->m * 32, 256), 256, 0, s,
+                       A->row_ptr, A->col_ind, A->val, d.get(), A->m, eps, conn);
+        return LAB_OK;
+    }
+
+    // ------------------------------------------------------------ PMIS
+    // host_amg_aggregation.cpp:32-38
+    __device__ __forceinline__ unsigned int pmis_hash(unsigned int x)
+    {
+        x = ((x >> 16) ^ x) * 0x45d9f3bu;
+        x = ((x >> 16) ^ x) * 0x45d9f3bu;
+        x = (x >> 16) ^ x;
+        return x / 2u;
+    }
+
+    // host_amg_aggregation.cpp:40-68
+    __global__ void k_pmis_init(const int32_t* __restrict__ rp, const int32_t* __restrict__ conn,
+                                int64_t m, int32_t* __restrict__ state, int32_t* __restrict__ hash,
+                                int64_t* __restrict__ agg)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int s = -2;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+            if(conn[j] == 1)
+            {
+                s = 0;
+                break;
+            }
+        state[i] = s;
+        hash[i]  = (int32_t)pmis_hash((unsigned int)i);
+        agg[i]   = 0;
+    }
+
+    // One round of host_find_maximum_distance_two_node (host_amg_aggregation.cpp:95-180).
+    // Reads the round's snapshot `st`, writes max_state / agg for its own row only,
+    // so the parallel round equals the sequential one.  The lexicographic maximum
+    // replaces the running winner only on a strictly larger (state, hash), so the
+    // CSR scan order decides ties exactly as in the reference (lines 77-93).
+    // Rounds after the first complete one return at once (amg_aggregation.cpp:154).
+    __global__ void k_pmis_round(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                 const int32_t* __restrict__ conn, int64_t m,
+                                 const int32_t* __restrict__ st, const int32_t* __restrict__ hash,
+                                 int32_t* __restrict__ max_state, int64_t* __restrict__ agg,
+                                 int32_t* flags, int round)
+    {
+        if(round > 0 && flags[round - 1] == 0)
+            return;
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int bs = st[i], bh = hash[i], br = (int)i;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+        {
+            if(conn[j] != 1)
+                continue;
+            int c = ci[j], cs = st[c], chh = hash[c];
+            if(cs > bs || (cs == bs && chh > bh))
+            {
+                bs = cs;
+                bh = chh;
+                br = c;
+            }
+        }
+        const int r = br;
+        for(int j = rp[r]; j < rp[r + 1]; j++)
+        {
+            if(conn[j] != 1)
+                continue;
+            int c = ci[j], cs = st[c], chh = hash[c];
+            if(cs > bs || (cs == bs && chh > bh))
+            {
+                bs = cs;
+                bh = chh;
+                br = c;
+            }
+        }
+        if(st[i] == 0)
+        {
+            if(br == i)
+            {
+                max_state[i] = 1;
+                agg[i]       = 1;
+            }
+            else if(bs == 1)
+            {
+                max_state[i] = -1;
+                agg[i]       = 0;
+            }
+            else
+                flags[round] = 1;
+        }
+    }
+
+    // host_add_unassigned_nodes_to_closest_aggregation (host_amg_aggregation.cpp:182-221)
+    __global__ void k_pmis_attach(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                  const int32_t* __restrict__ conn, int64_t m,
+                                  const int32_t* __restrict__ st, int32_t* __restrict__ max_state,
+                                  int64_t* __restrict__ agg)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int s = st[i];
+        if(s == -1)
+        {
+            for(int j = rp[i]; j < rp[i + 1]; j++)
+            {
+                if(conn[j] == 1 && st[ci[j]] == 1)
+                {
+                    agg[i]       = agg[ci[j]];
+                    max_state[i] = 1;
+                    break;
+                }
+            }
+        }
+        else if(s == -2)
+            agg[i] = -2;
+    }
+
+    __global__ void k_count_rounds(const int32_t* flags, int* out)
+    {
+        int r = 0;
+        while(r < 20 && flags[r] != 0)
+            r++;
+        *out = r;
+    }
+
+    // amg_aggregation.cpp:168-177: roots are the nodes marked 1 before the scan
+    __global__ void k_pmis_roots(const int64_t* __restrict__ agg, int64_t m, int64_t* roots)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i < m)
+            roots[i] = agg[i] == 1 ? 1 : -1;
+    }
+
+    // compute_aggregates_using_pmis (amg_aggregation.cpp:106-215)
+    lab_status amg_pmis(const lab_csr_impl* A, const int32_t* conn, int64_t* agg, int* rounds,
+                        cudaStream_t s, int64_t* roots = nullptr)
+    {
+        const int64_t m = A->m;
+        if(m == 0)
+        {
+            if(rounds)
+                *rounds = 0;
+            return LAB_OK;
+        }
+        dbuf<int32_t> state, snap, hash, flags;
+        LAB_TRY(state.alloc((size_t)m, s));
+        LAB_TRY(snap.alloc((size_t)m, s));
+        LAB_TRY(hash.alloc((size_t)m, s));
+        LAB_TRY(flags.alloc(24, s));
+        LAB_CUDA(cudaMemsetAsync(flags.get(), 0, sizeof(int32_t) * 24, s));
+        const unsigned g = (unsigned)ceil_div<int64_t>(m, 256);
+        LAB_LAUNCH(k_pmis_init, g, 256, 0, s, A->row_ptr, conn, m, state.get(), hash.get(), agg);
+        for(int r = 0; r < 20; r++)
+        {
+            LAB_CUDA(cudaMemcpyAsync(snap.get(), state.get(), sizeof(int32_t) * m,
+                                     cudaMemcpyDeviceToDevice, s));
+            LAB_LAUNCH(k_pmis_round, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m, snap.get(),
+                       hash.get(), state.get(), agg, flags.get(), r);
+        }
+        if(rounds)
+        {
+            dbuf<int> d;
+            LAB_TRY(d.alloc(1, s));
+            LAB_LAUNCH(k_count_rounds, 1, 1, 0, s, flags.get(), d.get());
+            LAB_TRY(copy_d2h_sync(rounds, d.get(), sizeof(int), s));
+        }
+        if(roots)
+            LAB_LAUNCH(k_pmis_roots, g, 256, 0, s, (const int64_t*)agg, m, roots);
+        LAB_TRY(scan_i64(agg, m, s));
+        for(int k = 0; k < 2; k++)
+        {
+            LAB_CUDA(cudaMemcpyAsync(snap.get(), state.get(), sizeof(int32_t) * m,
+                                     cudaMemcpyDeviceToDevice, s));
+            LAB_LAUNCH(k_pmis_attach, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m, snap.get(),
+                       state.get(), agg);
+        }
+        return LAB_OK;
+    }
+
+    // ------------------------------------------------------------ SA prolongation
+    // construct_prolongation_using_smoothed_aggregation (saamg.cpp:51-207).
+    // Items of row i, in CSR order: every diagonal or strong entry whose column
+    // has an aggregate >= 0, keyed by that aggregate, valued
+    //   1 - relax                      (diagonal)
+    //   (-relax * (1 / dtilde)) * a_ij  (strong), dtilde = a_ii - sum_weak a_ij
+    // summed per aggregate in CSR order (std::map accumulation, lines 177-187).
+    struct exp_sap
+    {
+        const int32_t* rp;
+        const int32_t* ci;
+        const double*  v;
+        const int32_t* conn;
+        const int64_t* agg;
+        double         relax;
+        const int32_t* out_rp = nullptr;
+
+        template <class G>
+        __device__ int expand(int row, uint64_t* keys, double* vals) const
+        {
+            __shared__ int s_pref[32];
+            const int      a0 = rp[row], a1 = rp[row + 1];
+            // saamg.cpp:145-163, sequential in CSR order (every thread computes it)
+            double dg = 0.0;
+            for(int j = a0; j < a1; j++)
+            {
+                if(ci[j] == row)
+                    dg = __dadd_rn(dg, v[j]);
+                else if(conn[j] == 0)
+                    dg = __dsub_rn(dg, v[j]);
+            }
+            const double inv  = __ddiv_rn(1.0, dg);
+            const double coef = __dmul_rn(-relax, inv);
+            const double dval = __dsub_rn(1.0, relax);
+            int          n    = 0;
+            for(int base = a0; base < a1; base += G::size)
+            {
+                int  j  = base + G::rank();
+                bool q  = false;
+                int  c  = 0;
+                int64_t ag = -1;
+                if(j < a1)
+                {
+                    c = ci[j];
+                    if(c == row || conn[j] == 1)
+                    {
+                        ag = agg[c];
+                        q  = ag >= 0;
+                    }
+                }
+                int tot;
+                int pos = n + group_prefix<G>(q, s_pref, tot);
+                if(q)
+                {
+                    keys[pos] = make_key((int)ag, pos);
+                    vals[pos] = (c == row) ? dval : __dmul_rn(coef, v[j]);
+                }
+                n += tot;
+            }
+            G::sync();
+            return n;
+        }
+        __device__ int32_t out_start(int row) const
+        {
+            return out_rp[row];
+        }
+    };
+
+    lab_status amg_sa_prolongation(const lab_csr_impl* A, const int32_t* conn, const int64_t* agg,
+                                   double relax, lab_csr_impl** P, cudaStream_t s)
+    {
+        int64_t mx = -1;
+        if(A->m > 0)
+            LAB_TRY(max_i64(agg, A->m, &mx, s));
+        int64_t nc = (mx > -1 ? mx : -1) + 1; // saamg.cpp:68-76
+        dbuf<int32_t> upper;
+        LAB_TRY(upper.alloc((size_t)A->m + 1, s));
+        LAB_TRY(row_lengths(A->row_ptr, A->m, upper.get(), s));
+        exp_sap e{A->row_ptr, A->col_ind, A->val, conn, agg, relax};
+        return esc_build(e, upper.get(), A->m, nc, P, s);
+    }
+
+    // ------------------------------------------------------------ UA prolongation
+    __global__ void k_ua_count(const int64_t* __restrict__ agg, int64_t m, int32_t* cnt)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i < m)
+            cnt[i] = agg[i] >= 0 ? 1 : 0;
+    }
+
+    __global__ void k_ua_fill(const int64_t* __restrict__ agg, int64_t m,
+                              const int32_t* __restrict__ rp, int32_t* ci, double* v)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i < m && agg[i] >= 0)
+        {
+            ci[rp[i]] = (int32_t)agg[i];
+            v[rp[i]]  = 1.0;
+        }
+    }
+
+    // construct_prolongation_using_unsmoothed_aggregation (uaamg.cpp:49-128)
+    lab_status amg_ua_prolongation(const lab_csr_impl* A, const int64_t* agg, lab_csr_impl** P,
+                                   cudaStream_t s)
+    {
+        const int64_t m  = A->m;
+        int64_t       mx = -1;
+        if(m > 0)
+            LAB_TRY(max_i64(agg, m, &mx, s));
+        int64_t       nc = (mx > -1 ? mx : -1) + 1;
+        dbuf<int32_t> cnt, rp;
+        LAB_TRY(cnt.alloc((size_t)m + 1, s));
+        LAB_TRY(rp.alloc((size_t)m + 1, s));
+        if(m > 0)
+            LAB_LAUNCH(k_ua_count, (unsigned)ceil_div<int64_t>(m, 256), 256, 0, s, agg, m, cnt.get());
+        int64_t nnz = 0;
+        LAB_TRY(counts_to_rowptr(cnt.get(), rp.get(), m, &nnz, s));
+        lab_csr_impl* out = nullptr;
+        LAB_TRY(csr_alloc(&out, m, nc, nnz, s));
+        LAB_CUDA(cudaMemcpyAsync(out->row_ptr, rp.get(), sizeof(int32_t) * (m + 1),
+                                 cudaMemcpyDeviceToDevice, s));
+        if(m > 0)
+            LAB_LAUNCH(k_ua_fill, (unsigned)ceil_div<int64_t>(m, 256), 256, 0, s, agg, m,
+                       out->row_ptr, out->col_ind, out->val);
+        *P = out;
+        return LAB_OK;
+    }
+
+    // ------------------------------------------------------------ RS strength
+    // host_amg_strength.cpp:72-156
+    __global__ void k_classical_strength(const int32_t* __restrict__ rp,
+                                         const int32_t* __restrict__ ci,
+                                         const double* __restrict__ v, int64_t m, double theta,
+                                         int32_t* __restrict__ conn, int32_t* __restrict__ cnt)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        double mx = -DBL_MAX;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+            if(ci[j] != i)
+                mx = (mx < -v[j]) ? -v[j] : mx; // std::max(mx, -a_ij)
+        const double thr = __dmul_rn(theta, mx);
+        int          c   = 0;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+        {
+            int str = (-v[j] >= thr && ci[j] != i);
+            conn[j] = str;
+            c += str;
+        }
+        cnt[i] = c;
+    }
+
+    __global__ void k_fill_s(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                             const double* __restrict__ v, const int32_t* __restrict__ conn,
+                             int64_t m, const int32_t* __restrict__ srp, int32_t* sci, double* sv)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int p = srp[i];
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+            if(conn[j] == 1)
+            {
+                sci[p] = ci[j];
+                sv[p]  = v[j];
+                p++;
+            }
+    }
+
+    lab_status amg_classical_strength(const lab_csr_impl* A, double theta, int32_t* conn,
+                                      lab_csr_impl** S, cudaStream_t s)
+    {
+        const int64_t m = A->m;
+        dbuf<int32_t> cnt, rp;
+        LAB_TRY(cnt.alloc((size_t)m + 1, s));
+        LAB_TRY(rp.alloc((size_t)m + 1, s));
+        if(m > 0)
+            LAB_LAUNCH(k_classical_strength, (unsigned)ceil_div<int64_t>(m, 256), 256, 0, s,
+                       A->row_ptr, A->col_ind, A->val, m, theta, conn, cnt.get());
+        int64_t nnz = 0;
+        LAB_TRY(counts_to_rowptr(cnt.get(), rp.get(), m, &nnz, s));
+        lab_csr_impl* out = nullptr;
+        LAB_TRY(csr_alloc(&out, m, A->n, nnz, s));
+        LAB_CUDA(cudaMemcpyAsync(out->row_ptr, rp.get(), sizeof(int32_t) * (m + 1),
+                                 cudaMemcpyDeviceToDevice, s));
+        if(m > 0)
+            LAB_LAUNCH(k_fill_s, (unsigned)ceil_div<int64_t>(m, 256), 256, 0, s, A->row_ptr,
+                       A->col_ind, A->val, conn, m, out->row_ptr, out->col_ind, out->val);
+        *S = out;
+        return LAB_OK;
+    }
+
+    // ------------------------------------------------------------ RS C/F splitting
+    // host_compute_cfpoint_first_pass / second_pass (host_amg_aggregation.cpp:228-519).
+    // The greedy bucket algorithm is inherently sequential (each choice reorders
+    // the buckets the next choice reads), so it runs as one device thread over
+    // L2-resident arrays; it is bit-exact by construction.
+    constexpr uint32_t kF = 0, kC = 1, kU = 2, kFF = 3;
+
+    __global__ void k_cf_first_pass(const int32_t* __restrict__ srp, const int32_t* __restrict__ sci,
+                                    const int32_t* __restrict__ trp, const int32_t* __restrict__ tci,
+                                    int m, uint32_t* cf, int* lambda, int* ptr, int* count,
+                                    int* i2n, int* n2i, int first, int second)
+    {
+        if(threadIdx.x != 0 || blockIdx.x != 0)
+            return;
+        if(!first)
+            goto second_pass;
+        for(int i = 0; i <= m; i++)
+        {
+            ptr[i]   = 0;
+            count[i] = 0;
+        }
+        ptr[m + 1] = 0;
+        for(int i = 0; i < m; i++)
+        {
+            cf[i]     = kU;
+            lambda[i] = trp[i + 1] - trp[i];
+        }
+        for(int i = 0; i < m; i++)
+            ptr[lambda[i] + 1]++;
+        for(int i = 0; i < m; i++)
+            ptr[i + 1] += ptr[i];
+        for(int i = 0; i < m; i++)
+        {
+            int lam    = lambda[i];
+            int idx    = ptr[lam] + count[lam];
+            i2n[idx]   = i;
+            n2i[i]     = idx;
+            count[lam] = count[lam] + 1;
+        }
+        for(int i = m - 1; i >= 0; i--)
+        {
+            int node = i2n[i];
+            if(lambda[node] <= 0)
+                break;
+            if(cf[node] != kU)
+                continue;
+            cf[node] = kC;
+            for(int j = trp[node]; j < trp[node + 1]; j++)
+                if(cf[tci[j]] == kU)
+                    cf[tci[j]] = kFF;
+            for(int j = trp[node]; j < trp[node + 1]; j++)
+            {
+                int f = tci[j];
+                if(cf[f] != kFF)
+                    continue;
+                cf[f] = kF;
+                for(int k = srp[f]; k < srp[f + 1]; k++)
+                {
+                    int u = sci[k];
+                    if(cf[u] != kU)
+                        continue;
+                    int lu = lambda[u], op = n2i[u], np = ptr[lu] + count[lu] - 1;
+                    n2i[i2n[op]] = np;
+                    n2i[i2n[np]] = op;
+                    int t        = i2n[op];
+                    i2n[op]      = i2n[np];
+                    i2n[np]      = t;
+                    count[lu]--;
+                    count[lu + 1]++;
+                    ptr[lu + 1] = ptr[lu] + count[lu];
+                    lambda[u]++;
+                }
+            }
+            for(int j = srp[node]; j < srp[node + 1]; j++)
+            {
+                int u = sci[j];
+                if(cf[u] != kU || lambda[u] <= 0)
+                    continue;
+                int lu = lambda[u], op = n2i[u], np = ptr[lu];
+                n2i[i2n[op]] = np;
+                n2i[i2n[np]] = op;
+                int t        = i2n[op];
+                i2n[op]      = i2n[np];
+                i2n[np]      = t;
+                count[lu]--;
+                count[lu - 1]++;
+                ptr[lu]++;
+                lambda[u]--;
+            }
+        }
+        for(int i = 0; i < m; i++)
+            if(cf[i] == kU)
+                cf[i] = kF;
+    second_pass:
+        if(!second)
+            return;
+        for(int i = 0; i < m; i++)
+        {
+            if(cf[i] != kF)
+                continue;
+            int s0 = srp[i], s1 = srp[i + 1], cand = -1;
+            for(int j = s0; j < s1; j++)
+            {
+                int c = sci[j];
+                if(cf[c] != kF)
+                    continue;
+                int  a = s0, b = srp[c], be = srp[c + 1];
+                bool found = false;
+                while(a < s1 && b < be)
+                {
+                    int c1 = sci[a], c2 = sci[b];
+                    if(c1 < c2)
+                        a++;
+                    else if(c2 < c1)
+                        b++;
+                    else
+                    {
+                        a++;
+                        b++;
+                        if(cf[c1] == kC)
+                        {
+                            found = true;
+                            break;
+                        }
+                    }
+                }
+                if(!found)
+                {
+                    if(cand >= 0)
+                        cf[cand] = kF;
+                    cand  = c;
+                    cf[c] = kC;
+                }
+            }
+        }
+    }
+
+    lab_status amg_cfpoints(const lab_csr_impl* S, uint32_t* cf, cudaStream_t s, int first,
+                            int second)
+    {
+        const int64_t m = S->m;
+        if(m == 0)
+            return LAB_OK;
+        lab_csr_impl* ST = nullptr;
+        LAB_TRY(transpose(S, &ST, s));
+        dbuf<int> lambda, ptr, count, i2n, n2i;
+        lab_status st = lambda.alloc((size_t)m + 2, s);
+        if(st == LAB_OK)
+            st = ptr.alloc((size_t)m + 2, s);
+        if(st == LAB_OK)
+            st = count.alloc((size_t)m + 2, s);
+        if(st == LAB_OK)
+            st = i2n.alloc((size_t)m + 1, s);
+        if(st == LAB_OK)
+            st = n2i.alloc((size_t)m + 1, s);
+        if(st == LAB_OK)
+        {
+            k_cf_first_pass<<<1, 1, 0, s>>>(S->row_ptr, S->col_ind, ST->row_ptr, ST->col_ind,
+                                            (int)m, cf, lambda.get(), ptr.get(), count.get(),
+                                            i2n.get(), n2i.get(), first, second);
+            g_launches.fetch_add(1);
+            cudaError_t e = cudaGetLastError();
+            if(e != cudaSuccess)
+                st = cuda_status(e, "k_cf_first_pass", __FILE__, __LINE__);
+        }
+        csr_release(ST);
+        return st;
+    }
+
+    // ------------------------------------------------------------ RS direct interpolation
+    __global__ void k_di_count(const int32_t* __restrict__ srp, const int32_t* __restrict__ sci,
+                               const uint32_t* __restrict__ cf, int64_t m, int32_t* cnt,
+                               int32_t* cflag)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        cflag[i] = (int32_t)cf[i];
+        if(cf[i] == kC)
+        {
+            cnt[i] = 1;
+            return;
+        }
+        int c = 0;
+        for(int j = srp[i]; j < srp[i + 1]; j++)
+            c += cf[sci[j]] == kC;
+        cnt[i] = c;
+    }
+
+    // rsamg.cpp:765-865, including the index quirk at line 818 (A's column array
+    // read at S positions).
+    __global__ void k_di_fill(const int32_t* __restrict__ arp, const int32_t* __restrict__ aci,
+                              const double* __restrict__ av, const int32_t* __restrict__ srp,
+                              const int32_t* __restrict__ sci, const double* __restrict__ sv,
+                              const uint32_t* __restrict__ cf, const int32_t* __restrict__ cidx,
+                              int64_t m, const int32_t* __restrict__ prp, int32_t* pci, double* pv)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int p = prp[i];
+        if(cf[i] == kC)
+        {
+            pci[p] = cidx[i];
+            pv[p]  = 1.0;
+            return;
+        }
+        double dg = 0.0, pos = 0.0, neg = 0.0;
+        for(int j = arp[i]; j < arp[i + 1]; j++)
+        {
+            if(aci[j] == i)
+                dg = av[j];
+            else if(av[j] < 0.0)
+                neg = __dadd_rn(neg, av[j]);
+            else
+                pos = __dadd_rn(pos, av[j]);
+        }
+        double spos = 0.0, sneg = 0.0;
+        for(int j = srp[i]; j < srp[i + 1]; j++)
+        {
+            if(cf[aci[j]] == kC)
+            {
+                if(sv[j] < 0.0)
+                    sneg = __dadd_rn(sneg, sv[j]);
+                else
+                    spos = __dadd_rn(spos, sv[j]);
+            }
+        }
+        const double alpha = __ddiv_rn(neg, sneg);
+        const double beta  = __ddiv_rn(pos, spos);
+        for(int j = srp[i]; j < srp[i + 1]; j++)
+        {
+            int c = sci[j];
+            if(cf[c] != kC)
+                continue;
+            pci[p] = cidx[c];
+            pv[p]  = sv[j] < 0.0 ? __ddiv_rn(__dmul_rn(-alpha, sv[j]), dg)
+                                 : __ddiv_rn(__dmul_rn(-beta, sv[j]), dg);
+            p++;
+        }
+    }
+
+    lab_status amg_direct_interpolation(const lab_csr_impl* A, const lab_csr_impl* S,
+                                        const uint32_t* cf, lab_csr_impl** P, cudaStream_t s)
+    {
+        const int64_t m = A->m;
+        dbuf<int32_t> cnt, rp, cidx;
+        LAB_TRY(cnt.alloc((size_t)m + 1, s));
+        LAB_TRY(rp.alloc((size_t)m + 1, s));
+        LAB_TRY(cidx.alloc((size_t)m + 1, s));
+        if(m > 0)
+            LAB_LAUNCH(k_di_count, (unsigned)ceil_div<int64_t>(m, 256), 256, 0, s, S->row_ptr,
+                       S->col_ind, cf, m, cnt.get(), cidx.get());
+        int64_t nc = 0;
+        // cidx = exclusive scan of the C flags; total = number of C points
+        LAB_TRY(counts_to_rowptr(cidx.get(), cidx.get(), m, &nc, s));
+        int64_t nnz = 0;
+        LAB_TRY(counts_to_rowptr(cnt.get(), rp.get(), m, &nnz, s));
+        lab_csr_impl* out = nullptr;
+        LAB_TRY(csr_alloc(&out, m, nc, nnz, s));
+        LAB_CUDA(cudaMemcpyAsync(out->row_ptr, rp.get(), sizeof(int32_t) * (m + 1),
+                                 cudaMemcpyDeviceToDevice, s));
+        if(m > 0)
+            LAB_LAUNCH(k_di_fill, (unsigned)ceil_div<int64_t>(m, 256), 256, 0, s, A->row_ptr,
+                       A->col_ind, A->val, S->row_ptr, S->col_ind, S->val, cf, cidx.get(), m,
+                       out->row_ptr, out->col_ind, out->val);
+        *P = out;
+        return LAB_OK;
+    }
+
+    // ------------------------------------------------------------ level loop
+    lab_status hierarchy_release(hierarchy_impl* h)
+    {
+        if(!h)
+            return LAB_OK;
+        cudaDeviceSynchronize();
+        solver_cache_forget(h);
+        for(int l = 0; l <= kMaxLevels; l++)
+        {
+            if(h->A[l])
+                csr_release(h->A[l]);
+            level_ws& w = h->ws[l];
+            void*     ptrs[] = {w.x, w.b, w.r, w.t, w.xf, w.bf, w.rf, w.tf, w.colour};
+            for(void* p : ptrs)
+                if(p)
+                    cudaFree(p);
+            delete[] w.colour_ptr_h;
+        }
+        for(int l = 0; l < kMaxLevels; l++)
+        {
+            if(h->P[l])
+                csr_release(h->P[l]);
+            if(h->R[l])
+                csr_release(h->R[l]);
+        }
+        if(h->coarse_inv)
+            cudaFree(h->coarse_inv);
+        if(h->coarse_inv32)
+            cudaFree(h->coarse_inv32);
+        delete static_cast<lab_hier_s*>(h);
+        return LAB_OK;
+    }
+
+    // saamg_setup (saamg.cpp:210-282), uaamg_setup (uaamg.cpp:131-224),
+    // rsamg_setup (rsamg.cpp:869-947)
+    static lab_status amg_setup(int kind, const lab_csr_impl* A0, int max_level,
+                                hierarchy_impl* h, cudaStream_t s)
+    {
+        max_level = std::min(max_level, kMaxLevels);
+        h->kind   = kind;
+        LAB_TRY(csr_alloc(&h->A[0], A0->m, A0->n, A0->nnz, s));
+        LAB_CUDA(cudaMemcpyAsync(h->A[0]->row_ptr, A0->row_ptr, sizeof(int32_t) * (A0->m + 1),
+                                 cudaMemcpyDeviceToDevice, s));
+        if(A0->nnz)
+        {
+            LAB_CUDA(cudaMemcpyAsync(h->A[0]->col_ind, A0->col_ind, sizeof(int32_t) * A0->nnz,
+                                     cudaMemcpyDeviceToDevice, s));
+            LAB_CUDA(cudaMemcpyAsync(h->A[0]->val, A0->val, sizeof(double) * A0->nnz,
+                                     cudaMemcpyDeviceToDevice, s));
+        }
+        double eps   = kind == LAB_AMG_UA ? 0.001 : 0.08;
+        double relax = 2.0 / 3.0;
+        double theta = 0.2;
+        int    level = 0;
+        while(level < max_level)
+        {
+            lab_csr_impl* Af = h->A[level];
+            lab_csr_impl* P  = nullptr;
+            dbuf<int32_t> conn;
+            LAB_TRY(conn.alloc((size_t)std::max<int64_t>(Af->nnz, 1), s));
+            if(Af->nnz)
+                LAB_CUDA(cudaMemsetAsync(conn.get(), 0, sizeof(int32_t) * Af->nnz, s));
+            if(kind == LAB_AMG_RS)
+            {
+                lab_csr_impl*  S = nullptr;
+                dbuf<uint32_t> cf;
+                LAB_TRY(cf.alloc((size_t)Af->m + 1, s));
+                LAB_TRY(amg_classical_strength(Af, theta, conn.get(), &S, s));
+                lab_status st = amg_cfpoints(S, cf.get(), s, 1, 1);
+                if(st == LAB_OK)
+                    st = amg_direct_interpolation(Af, S, cf.get(), &P, s);
+                csr_release(S);
+                LAB_TRY(st);
+            }
+            else
+            {
+                dbuf<int64_t> agg;
+                LAB_TRY(agg.alloc((size_t)Af->m + 1, s));
+                LAB_TRY(amg_strength(Af, eps, conn.get(), s));
+                LAB_TRY(amg_pmis(Af, conn.get(), agg.get(), nullptr, s, nullptr));
+                if(kind == LAB_AMG_SA)
+                    LAB_TRY(amg_sa_prolongation(Af, conn.get(), agg.get(), relax, &P, s));
+                else
+                    LAB_TRY(amg_ua_prolongation(Af, agg.get(), &P, s));
+            }
+            if(P->n == 0)
+            {
+                csr_release(P);
+                break;
+            }
+            h->P[level] = P;
+            LAB_TRY(transpose(P, &h->R[level], s));
+            lab_csr_impl* AP = nullptr;
+            LAB_TRY(spgemm(Af, P, &AP, s));
+            lab_status st = spgemm(h->R[level], AP, &h->A[level + 1], s);
+            csr_release(AP);
+            LAB_TRY(st);
+            level++;
+            eps *= 0.5;
+        }
+        h->levels = level;
+        return LAB_OK;
+    }
+}
+
+using namespace lab;
+
+extern "C" {
+
+LAB_API lab_status lab_strength(lab_csr A, double eps, int32_t* conn, lab_stream s)
+{
+    LAB_ARG(A && (conn || A->nnz == 0), "null argument");
+    LAB_TRY(ensure_init());
+    return amg_strength(A, eps, conn, to_stream(s));
+}
+
+LAB_API lab_status lab_classical_strength(lab_csr A, double theta, int32_t* conn, lab_csr* S,
+                                          lab_stream s)
+{
+    LAB_ARG(A && S && (conn || A->nnz == 0), "null argument");
+    LAB_TRY(ensure_init());
+    lab_csr_impl* out = nullptr;
+    LAB_TRY(amg_classical_strength(A, theta, conn, &out, to_stream(s)));
+    *S = static_cast<lab_csr>(out);
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_pmis_aggregate(lab_csr A, const int32_t* conn, int64_t* aggregates,
+                                      int* rounds, lab_stream s)
+{
+    LAB_ARG(A && (aggregates || A->m == 0), "null argument");
+    LAB_TRY(ensure_init());
+    return amg_pmis(A, conn, aggregates, rounds, to_stream(s), nullptr);
+}
+
+LAB_API lab_status lab_sa_prolongation(lab_csr A, const int32_t* conn, const int64_t* aggregates,
+                                       double relax, lab_csr* P, lab_stream s)
+{
+    LAB_ARG(A && P, "null argument");
+    LAB_TRY(ensure_init());
+    lab_csr_impl* out = nullptr;
+    LAB_TRY(amg_sa_prolongation(A, conn, aggregates, relax, &out, to_stream(s)));
+    *P = static_cast<lab_csr>(out);
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_ua_prolongation(lab_csr A, const int64_t* aggregates, lab_csr* P,
+                                       lab_stream s)
+{
+    LAB_ARG(A && P, "null argument");
+    LAB_TRY(ensure_init());
+    lab_csr_impl* out = nullptr;
+    LAB_TRY(amg_ua_prolongation(A, aggregates, &out, to_stream(s)));
+    *P = static_cast<lab_csr>(out);
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_cfpoints(lab_csr S, uint32_t* cf, lab_stream s)
+{
+    LAB_ARG(S && (cf || S->m == 0), "null argument");
+    LAB_ARG(S->m == S->n, "S must be square");
+    LAB_TRY(ensure_init());
+    return amg_cfpoints(S, cf, to_stream(s), 1, 1);
+}
+
+LAB_API lab_status lab_cfpoints_passes(lab_csr S, uint32_t* cf, int first, int second,
+                                       lab_stream s)
+{
+    LAB_ARG(S && (cf || S->m == 0), "null argument");
+    LAB_ARG(S->m == S->n, "S must be square");
+    LAB_TRY(ensure_init());
+    return amg_cfpoints(S, cf, to_stream(s), first, second);
+}
+
+LAB_API lab_status lab_pmis_aggregate_roots(lab_csr A, const int32_t* conn, int64_t* aggregates,
+                                            int64_t* root_nodes, int* rounds, lab_stream s)
+{
+    LAB_ARG(A && (aggregates || A->m == 0), "null argument");
+    LAB_TRY(ensure_init());
+    return amg_pmis(A, conn, aggregates, rounds, to_stream(s), root_nodes);
+}
+
+LAB_API lab_status lab_direct_interpolation(lab_csr A, lab_csr S, const uint32_t* cf,
+                                            lab_csr* P, lab_stream s)
+{
+    LAB_ARG(A && S && P, "null argument");
+    LAB_TRY(ensure_init());
+    lab_csr_impl* out = nullptr;
+    LAB_TRY(amg_direct_interpolation(A, S, cf, &out, to_stream(s)));
+    *P = static_cast<lab_csr>(out);
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_amg_setup(lab_amg_kind kind, lab_csr A, int max_level, lab_hierarchy* out,
+                                 lab_stream ls)
+{
+    LAB_ARG(A && out, "null argument");
+    LAB_ARG(kind == LAB_AMG_SA || kind == LAB_AMG_UA || kind == LAB_AMG_RS, "unknown AMG kind");
+    LAB_ARG(A->m == A->n, "AMG needs a square matrix");
+    LAB_ARG(max_level >= 0, "negative max_level");
+    LAB_TRY(ensure_init());
+    cudaStream_t s = to_stream(ls);
+    lab_hier_s*  h = new(std::nothrow) lab_hier_s();
+    if(!h)
+        return LAB_OOM;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    lab_status st = amg_setup(kind, A, max_level, h, s);
+    cudaEventRecord(e1, s);
+    if(st == LAB_OK)
+    {
+        cudaError_t e = cudaEventSynchronize(e1);
+        if(e != cudaSuccess)
+            st = cuda_status(e, "lab_amg_setup", __FILE__, __LINE__);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        h->setup_ms = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if(st != LAB_OK)
+    {
+        hierarchy_release(h);
+        return st;
+    }
+    *out = h;
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_hierarchy_destroy(lab_hierarchy h)
+{
+    return hierarchy_release(h);
+}
+
+LAB_API lab_status lab_hierarchy_levels(lab_hierarchy h, int* n)
+{
+    LAB_ARG(h && n, "null argument");
+    *n = h->levels;
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_hierarchy_level(lab_hierarchy h, int l, lab_csr* A, lab_csr* P, lab_csr* R)
+{
+    LAB_ARG(h, "null hierarchy");
+    LAB_ARG(l >= 0 && l <= h->levels, "level out of range");
+    LAB_ARG(l < h->levels || (!P && !R), "no P/R on the coarsest level");
+    if(A)
+        *A = static_cast<lab_csr>(h->A[l]);
+    if(P)
+        *P = static_cast<lab_csr>(h->P[l]);
+    if(R)
+        *R = static_cast<lab_csr>(h->R[l]);
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_hierarchy_setup_ms(lab_hierarchy h, double* ms)
+{
+    LAB_ARG(h && ms, "null argument");
+    *ms = h->setup_ms;
+    return LAB_OK;
+}
+
+} // extern "C"

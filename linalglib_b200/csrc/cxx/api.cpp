@@ -1,0 +1,1296 @@
+// C++ API (namespace linalg): the reference's containers, free functions and
+// solver classes on the AMG-PCG path, implemented over the C ABI in lab.h.
+// All arithmetic runs on the GPU; this file moves data and maps status codes to
+// the reference's conventions (iteration counts, bool, printed errors).
+#include "linalg.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <tuple>
+#include <type_traits>
+
+namespace linalg
+{
+    // ------------------------------------------------------------ status mapping
+    static bool ok(lab_status s, const char* what)
+    {
+        if(s == LAB_OK || s == LAB_NOT_CONVERGED)
+            return true;
+        std::cerr << "Error: " << what << ": " << lab_status_string(s) << ": " << lab_last_error()
+                  << std::endl;
+        return false;
+    }
+
+    // ============================================================ vector<T>
+    template <typename T>
+    vector<T>::vector()
+    {
+    }
+
+    template <typename T>
+    vector<T>::vector(size_t size)
+        : h(size)
+        , n(size)
+    {
+    }
+
+    template <typename T>
+    vector<T>::vector(size_t size, T val)
+        : h(size, val)
+        , n(size)
+    {
+    }
+
+    template <typename T>
+    vector<T>::vector(const std::vector<T>& v)
+        : h(v)
+        , n(v.size())
+    {
+    }
+
+    template <typename T>
+    vector<T>::~vector()
+    {
+        if(d)
+            lab_free(d, nullptr);
+    }
+
+    template <typename T>
+    void vector<T>::sync_host() const
+    {
+        if(valid & 1)
+            return;
+        h.resize(n);
+        if(n)
+        {
+            ok(lab_memcpy(h.data(), d, n * sizeof(T), nullptr), "vector download");
+            lab_synchronize(nullptr);
+        }
+        valid |= 1;
+    }
+
+    // Size changes always go through the host copy (resize / clear set valid = 1),
+    // so a device buffer that is too small never holds the only current copy.
+    template <typename T>
+    static void ensure_capacity(T*& d, size_t& dcap, size_t n, int& valid)
+    {
+        if(d && dcap >= n)
+            return;
+        T* nd = nullptr;
+        if(!ok(lab_malloc(reinterpret_cast<void**>(&nd), (n ? n : 1) * sizeof(T), nullptr),
+               "vector allocation"))
+            return;
+        if(d)
+            lab_free(d, nullptr);
+        d    = nd;
+        dcap = n ? n : 1;
+        valid &= ~2;
+    }
+
+    template <typename T>
+    void vector<T>::sync_device() const
+    {
+        ensure_capacity(d, dcap, n, valid);
+        if(valid & 2)
+            return;
+        if(n)
+            ok(lab_memcpy(d, h.data(), n * sizeof(T), nullptr), "vector upload");
+        valid |= 2;
+    }
+
+    template <typename T>
+    T& vector<T>::operator[](size_t index)
+    {
+        sync_host();
+        valid = 1;
+        return h[index];
+    }
+
+    template <typename T>
+    const T& vector<T>::operator[](size_t index) const
+    {
+        sync_host();
+        return h[index];
+    }
+
+    template <typename T>
+    bool vector<T>::is_on_host() const
+    {
+        return on_host;
+    }
+
+    template <typename T>
+    size_t vector<T>::get_size() const
+    {
+        return n;
+    }
+
+    template <typename T>
+    T* vector<T>::get_vec()
+    {
+        if(on_host)
+        {
+            sync_host();
+            valid = 1;
+            return h.data();
+        }
+        sync_device();
+        valid = 2;
+        return d;
+    }
+
+    template <typename T>
+    const T* vector<T>::get_vec() const
+    {
+        if(on_host)
+        {
+            sync_host();
+            return h.data();
+        }
+        sync_device();
+        return d;
+    }
+
+    template <typename T>
+    void vector<T>::resize(size_t size)
+    {
+        resize(size, T(0));
+    }
+
+    template <typename T>
+    void vector<T>::resize(size_t size, T val)
+    {
+        sync_host();
+        h.resize(size, val);
+        n     = size;
+        valid = 1;
+    }
+
+    template <typename T>
+    void vector<T>::clear()
+    {
+        h.clear();
+        n     = 0;
+        valid = 1;
+    }
+
+    template <typename T>
+    void vector<T>::copy_from(const vector& x)
+    {
+        // vector.cpp:141-163: copies x.get_size() elements, no resize
+        size_t k = std::min(n, x.n);
+        if(k == 0)
+            return;
+        if(!on_host || ((x.valid & 2) && !(x.valid & 1)))
+        {
+            const T* src = x.device_read();
+            T*       dst = (k == n) ? device_write() : device_readwrite();
+            ok(lab_memcpy(dst, src, k * sizeof(T), nullptr), "vector copy");
+            return;
+        }
+        x.sync_host();
+        sync_host();
+        std::copy(x.h.begin(), x.h.begin() + k, h.begin());
+        valid = 1;
+    }
+
+    template <typename T>
+    void vector<T>::fill(T val)
+    {
+        if(!on_host && std::is_same<T, double>::value && n)
+        {
+            ok(lab_fill((int64_t)n, (double)val, reinterpret_cast<double*>(device_write()),
+                        nullptr),
+               "vector fill");
+            return;
+        }
+        h.assign(n, val);
+        valid = 1;
+    }
+
+    template <typename T>
+    void vector<T>::zeros()
+    {
+        fill(T(0));
+    }
+
+    template <typename T>
+    void vector<T>::ones()
+    {
+        fill(T(1));
+    }
+
+    template <typename T>
+    void vector<T>::rand(T min, T max)
+    {
+        sync_host();
+        for(size_t i = 0; i < n; i++)
+            h[i] = min + (T)((max - min) * ((double)std::rand() / RAND_MAX));
+        valid = 1;
+    }
+
+    template <typename T>
+    void vector<T>::move_to_device()
+    {
+        on_host = false;
+        sync_device();
+    }
+
+    template <typename T>
+    void vector<T>::move_to_host()
+    {
+        on_host = true;
+        sync_host();
+    }
+
+    template <typename T>
+    void vector<T>::print_vector(const std::string name) const
+    {
+        sync_host();
+        std::cout << name << std::endl;
+        for(size_t i = 0; i < n; i++)
+            std::cout << h[i] << " ";
+        std::cout << std::endl;
+    }
+
+    template <typename T>
+    const T* vector<T>::device_read() const
+    {
+        sync_device();
+        return d;
+    }
+
+    template <typename T>
+    T* vector<T>::device_write()
+    {
+        ensure_capacity(d, dcap, n, valid);
+        valid = 2;
+        return d;
+    }
+
+    template <typename T>
+    T* vector<T>::device_readwrite()
+    {
+        sync_device();
+        valid = 2;
+        return d;
+    }
+
+    template class vector<double>;
+    template class vector<float>;
+    template class vector<int>;
+    template class vector<int64_t>;
+    template class vector<uint32_t>;
+
+    // ============================================================ csr_matrix<T>
+    static std::shared_ptr<lab_csr_s> wrap(lab_csr A, bool owned)
+    {
+        if(owned)
+            return std::shared_ptr<lab_csr_s>(A, [](lab_csr_s* p) { lab_csr_destroy(p); });
+        return std::shared_ptr<lab_csr_s>(A, [](lab_csr_s*) {});
+    }
+
+    template <typename T>
+    csr_matrix<T>::csr_matrix()
+        : m(0)
+        , n(0)
+        , nnz(0)
+        , on_host(true)
+    {
+        csr_row_ptr.resize(1);
+    }
+
+    template <typename T>
+    csr_matrix<T>::csr_matrix(const std::vector<int>& rp, const std::vector<int>& ci,
+                              const std::vector<T>& v, int m_, int n_, int nnz_)
+        : m(m_)
+        , n(n_)
+        , nnz(nnz_)
+        , on_host(true)
+    {
+        csr_row_ptr.resize(rp.size());
+        csr_col_ind.resize(ci.size());
+        csr_val.resize(v.size());
+        std::copy(rp.begin(), rp.end(), csr_row_ptr.get_vec());
+        std::copy(ci.begin(), ci.end(), csr_col_ind.get_vec());
+        std::copy(v.begin(), v.end(), csr_val.get_vec());
+    }
+
+    template <typename T>
+    csr_matrix<T>::~csr_matrix()
+    {
+    }
+
+    template <typename T>
+    void csr_matrix<T>::sync_host() const
+    {
+        if(host_valid)
+            return;
+        csr_row_ptr.resize(m + 1);
+        csr_col_ind.resize(nnz);
+        csr_val.resize(nnz);
+        ok(lab_csr_copy_to(dev.get(), csr_row_ptr.get_vec(), csr_col_ind.get_vec(),
+                           reinterpret_cast<double*>(csr_val.get_vec()), LAB_MEM_HOST, nullptr),
+           "matrix download");
+        host_valid = true;
+    }
+
+    template <typename T>
+    lab_csr csr_matrix<T>::device() const
+    {
+        if(!dev)
+        {
+            lab_csr A = nullptr;
+            if(ok(lab_csr_create(&A, m, n, nnz, csr_row_ptr.get_vec(), csr_col_ind.get_vec(),
+                                 reinterpret_cast<const double*>(csr_val.get_vec()), LAB_MEM_HOST,
+                                 nullptr),
+                  "matrix upload"))
+                dev = wrap(A, true);
+        }
+        return dev.get();
+    }
+
+    template <typename T>
+    void csr_matrix<T>::adopt(lab_csr A, bool owned)
+    {
+        int64_t mm = 0, nn = 0, zz = 0;
+        lab_csr_info(A, &mm, &nn, &zz);
+        m          = (int)mm;
+        n          = (int)nn;
+        nnz        = (int)zz;
+        dev        = wrap(A, owned);
+        host_valid = false;
+    }
+
+    template <typename T>
+    void csr_matrix<T>::reset()
+    {
+        dev.reset();
+        m = n = nnz = 0;
+        csr_row_ptr.resize(1);
+        csr_col_ind.clear();
+        csr_val.clear();
+        csr_row_ptr[0] = 0;
+        host_valid     = true;
+    }
+
+    template <typename T>
+    bool csr_matrix<T>::is_on_host() const
+    {
+        return on_host;
+    }
+    template <typename T>
+    int csr_matrix<T>::get_m() const
+    {
+        return m;
+    }
+    template <typename T>
+    int csr_matrix<T>::get_n() const
+    {
+        return n;
+    }
+    template <typename T>
+    int csr_matrix<T>::get_nnz() const
+    {
+        return nnz;
+    }
+
+    template <typename T>
+    const int* csr_matrix<T>::get_row_ptr() const
+    {
+        if(!on_host)
+        {
+            int32_t* p = nullptr;
+            lab_csr_device_arrays(device(), &p, nullptr, nullptr);
+            return p;
+        }
+        sync_host();
+        return csr_row_ptr.get_vec();
+    }
+    template <typename T>
+    const int* csr_matrix<T>::get_col_ind() const
+    {
+        if(!on_host)
+        {
+            int32_t* p = nullptr;
+            lab_csr_device_arrays(device(), nullptr, &p, nullptr);
+            return p;
+        }
+        sync_host();
+        return csr_col_ind.get_vec();
+    }
+    template <typename T>
+    const T* csr_matrix<T>::get_val() const
+    {
+        if(!on_host)
+        {
+            double* p = nullptr;
+            lab_csr_device_arrays(device(), nullptr, nullptr, &p);
+            return reinterpret_cast<const T*>(p);
+        }
+        sync_host();
+        return csr_val.get_vec();
+    }
+
+    // Mutable access: the caller may change entries, so cached device data goes.
+    template <typename T>
+    int* csr_matrix<T>::get_row_ptr()
+    {
+        if(!on_host)
+        {
+            int32_t* p = nullptr;
+            lab_csr_device_arrays(device(), &p, nullptr, nullptr);
+            lab_csr_values_changed(dev.get());
+            return p;
+        }
+        sync_host();
+        dev.reset();
+        return csr_row_ptr.get_vec();
+    }
+    template <typename T>
+    int* csr_matrix<T>::get_col_ind()
+    {
+        if(!on_host)
+        {
+            int32_t* p = nullptr;
+            lab_csr_device_arrays(device(), nullptr, &p, nullptr);
+            lab_csr_values_changed(dev.get());
+            return p;
+        }
+        sync_host();
+        dev.reset();
+        return csr_col_ind.get_vec();
+    }
+    template <typename T>
+    T* csr_matrix<T>::get_val()
+    {
+        if(!on_host)
+        {
+            double* p = nullptr;
+            lab_csr_device_arrays(device(), nullptr, nullptr, &p);
+            lab_csr_values_changed(dev.get());
+            return reinterpret_cast<T*>(p);
+        }
+        sync_host();
+        dev.reset();
+        return csr_val.get_vec();
+    }
+
+    template <typename T>
+    void csr_matrix<T>::resize(int m_, int n_, int nnz_)
+    {
+        sync_host();
+        dev.reset();
+        csr_row_ptr.resize(m_ + 1);
+        csr_col_ind.resize(nnz_);
+        csr_val.resize(nnz_);
+        m   = m_;
+        n   = n_;
+        nnz = nnz_;
+    }
+
+    template <typename T>
+    void csr_matrix<T>::copy_from(const csr_matrix<T>& A)
+    {
+        if(A.dev && !A.host_valid)
+        {
+            lab_csr C = nullptr;
+            if(ok(lab_csr_clone(A.dev.get(), &C, nullptr), "matrix copy"))
+                adopt(C, true);
+            return;
+        }
+        A.sync_host();
+        m   = A.m;
+        n   = A.n;
+        nnz = A.nnz;
+        csr_row_ptr.resize(m + 1);
+        csr_col_ind.resize(nnz);
+        csr_val.resize(nnz);
+        std::copy(A.csr_row_ptr.get_vec(), A.csr_row_ptr.get_vec() + m + 1, csr_row_ptr.get_vec());
+        std::copy(A.csr_col_ind.get_vec(), A.csr_col_ind.get_vec() + nnz, csr_col_ind.get_vec());
+        std::copy(A.csr_val.get_vec(), A.csr_val.get_vec() + nnz, csr_val.get_vec());
+        host_valid = true;
+        dev.reset();
+    }
+
+    template <typename T>
+    void csr_matrix<T>::move_to_device()
+    {
+        on_host = false;
+        device();
+    }
+
+    template <typename T>
+    void csr_matrix<T>::move_to_host()
+    {
+        on_host = true;
+        sync_host();
+    }
+
+    template <typename T>
+    void csr_matrix<T>::extract_diagonal(vector<T>& diag) const
+    {
+        if(diag.get_size() < (size_t)m)
+            diag.resize(m);
+        ok(lab_diagonal(device(), reinterpret_cast<double*>(diag.device_write()), nullptr),
+           "extract_diagonal");
+    }
+
+    template <typename T>
+    void csr_matrix<T>::multiply_by_vector(vector<T>& y, const vector<T>& x) const
+    {
+        if(y.get_size() < (size_t)m)
+            y.resize(m);
+        ok(lab_spmv(1.0, device(), reinterpret_cast<const double*>(x.device_read()), 0.0,
+                    reinterpret_cast<double*>(y.device_write()), nullptr),
+           "multiply_by_vector");
+    }
+
+    template <typename T>
+    void csr_matrix<T>::multiply_by_vector_and_add(vector<T>& y, const vector<T>& x) const
+    {
+        ok(lab_spmv(1.0, device(), reinterpret_cast<const double*>(x.device_read()), 1.0,
+                    reinterpret_cast<double*>(y.device_readwrite()), nullptr),
+           "multiply_by_vector_and_add");
+    }
+
+    template <typename T>
+    void csr_matrix<T>::multiply_by_matrix(csr_matrix<T>& C, const csr_matrix<T>& B) const
+    {
+        lab_csr out = nullptr;
+        if(ok(lab_spgemm(device(), B.device(), &out, nullptr), "multiply_by_matrix"))
+            C.adopt(out, true);
+    }
+
+    template <typename T>
+    void csr_matrix<T>::transpose(csr_matrix<T>& Trans) const
+    {
+        lab_csr out = nullptr;
+        if(ok(lab_transpose(device(), &out, nullptr), "transpose"))
+            Trans.adopt(out, true);
+    }
+
+    // Matrix Market coordinate real (general or symmetric), 1-based; rows are
+    // sorted by column and duplicate entries summed.
+    template <typename T>
+    bool csr_matrix<T>::read_mtx(const std::string& filename)
+    {
+        std::ifstream f(filename);
+        if(!f)
+            return false;
+        std::string line;
+        std::getline(f, line);
+        bool symmetric = line.find("symmetric") != std::string::npos;
+        bool pattern   = line.find("pattern") != std::string::npos;
+        while(std::getline(f, line) && (line.empty() || line[0] == '%'))
+        {
+        }
+        std::istringstream hdr(line);
+        long               M = 0, N = 0, Z = 0;
+        hdr >> M >> N >> Z;
+        std::vector<std::tuple<int, int, double>> e;
+        e.reserve(symmetric ? 2 * Z : Z);
+        for(long k = 0; k < Z; k++)
+        {
+            long   i, j;
+            double v = 1.0;
+            if(pattern)
+                f >> i >> j;
+            else
+                f >> i >> j >> v;
+            if(!f)
+                return false;
+            e.emplace_back((int)i - 1, (int)j - 1, v);
+            if(symmetric && i != j)
+                e.emplace_back((int)j - 1, (int)i - 1, v);
+        }
+        std::sort(e.begin(), e.end(), [](const auto& a, const auto& b) {
+            return std::get<0>(a) != std::get<0>(b) ? std::get<0>(a) < std::get<0>(b)
+                                                    : std::get<1>(a) < std::get<1>(b);
+        });
+        std::vector<int>    rp(M + 1, 0), ci;
+        std::vector<double> vv;
+        for(size_t k = 0; k < e.size(); k++)
+        {
+            if(!ci.empty() && k > 0 && std::get<0>(e[k]) == std::get<0>(e[k - 1]) &&
+               std::get<1>(e[k]) == std::get<1>(e[k - 1]))
+            {
+                vv.back() += std::get<2>(e[k]);
+                continue;
+            }
+            rp[std::get<0>(e[k]) + 1]++;
+            ci.push_back(std::get<1>(e[k]));
+            vv.push_back(std::get<2>(e[k]));
+        }
+        for(long i = 0; i < M; i++)
+            rp[i + 1] += rp[i];
+        resize((int)M, (int)N, (int)ci.size());
+        std::copy(rp.begin(), rp.end(), csr_row_ptr.get_vec());
+        std::copy(ci.begin(), ci.end(), csr_col_ind.get_vec());
+        std::copy(vv.begin(), vv.end(), csr_val.get_vec());
+        host_valid = true;
+        dev.reset();
+        return true;
+    }
+
+    template <typename T>
+    bool csr_matrix<T>::write_mtx(const std::string& filename)
+    {
+        sync_host();
+        std::ofstream f(filename);
+        if(!f)
+            return false;
+        f << "%%MatrixMarket matrix coordinate real general\n";
+        f << m << " " << n << " " << nnz << "\n";
+        f.precision(17);
+        const int* rp = csr_row_ptr.get_vec();
+        const int* ci = csr_col_ind.get_vec();
+        const T*   v  = csr_val.get_vec();
+        for(int i = 0; i < m; i++)
+            for(int j = rp[i]; j < rp[i + 1]; j++)
+                f << i + 1 << " " << ci[j] + 1 << " " << v[j] << "\n";
+        return true;
+    }
+
+    template <typename T>
+    void csr_matrix<T>::print_matrix(const std::string name) const
+    {
+        sync_host();
+        std::cout << name << " (" << m << " x " << n << ", " << nnz << " nonzeros)" << std::endl;
+        const int* rp = csr_row_ptr.get_vec();
+        const int* ci = csr_col_ind.get_vec();
+        const T*   v  = csr_val.get_vec();
+        for(int i = 0; i < m; i++)
+        {
+            for(int j = rp[i]; j < rp[i + 1]; j++)
+                std::cout << "(" << ci[j] << ", " << v[j] << ") ";
+            std::cout << std::endl;
+        }
+    }
+
+    template class csr_matrix<double>;
+
+    // ============================================================ free functions
+    void axpy(double alpha, const vector<double>& x, vector<double>& y)
+    {
+        ok(lab_axpy((int64_t)x.get_size(), alpha, x.device_read(), y.device_readwrite(), nullptr),
+           "axpy");
+    }
+
+    void axpby(double alpha, const vector<double>& x, double beta, vector<double>& y)
+    {
+        ok(lab_axpby((int64_t)x.get_size(), alpha, x.device_read(), beta, y.device_readwrite(),
+                     nullptr),
+           "axpby");
+    }
+
+    void axpbypgz(double alpha, const vector<double>& x, double beta, const vector<double>& y,
+                  double gamma, vector<double>& z)
+    {
+        ok(lab_axpbypgz((int64_t)x.get_size(), alpha, x.device_read(), beta, y.device_read(),
+                        gamma, z.device_readwrite(), nullptr),
+           "axpbypgz");
+    }
+
+    void transpose_matrix(const csr_matrix<double>& A, csr_matrix<double>& transposeA)
+    {
+        A.transpose(transposeA);
+    }
+
+    double dot_product(const vector<double>& x, const vector<double>& y)
+    {
+        double r = 0.0;
+        ok(lab_dot((int64_t)x.get_size(), x.device_read(), y.device_read(), &r, nullptr),
+           "dot_product");
+        return r;
+    }
+
+    void compute_residual(const csr_matrix<double>& A, const vector<double>& x,
+                          const vector<double>& b, vector<double>& res)
+    {
+        if(res.get_size() < (size_t)A.get_m())
+            res.resize(A.get_m());
+        ok(lab_residual(A.device(), x.device_read(), b.device_read(), res.device_write(), nullptr),
+           "compute_residual");
+    }
+
+    void diagonal(const csr_matrix<double>& A, vector<double>& d)
+    {
+        A.extract_diagonal(d);
+    }
+
+    double norm_euclid(const vector<double>& a)
+    {
+        double r = 0.0;
+        ok(lab_norm_euclid((int64_t)a.get_size(), a.device_read(), &r, nullptr), "norm_euclid");
+        return r;
+    }
+
+    double norm_inf(const vector<double>& a)
+    {
+        double r = 0.0;
+        ok(lab_norm_inf((int64_t)a.get_size(), a.device_read(), &r, nullptr), "norm_inf");
+        return r;
+    }
+
+    struct csrmv_descr
+    {
+        int analysed = 0;
+    };
+    struct csrgeam_descr
+    {
+        lab_csr C = nullptr;
+    };
+    struct csrgemm_descr
+    {
+        int dummy = 0;
+    };
+
+    void create_csrmv_descr(csrmv_descr** d)
+    {
+        *d = new csrmv_descr();
+    }
+    void destroy_csrmv_descr(csrmv_descr* d)
+    {
+        delete d;
+    }
+    void csrmv_analysis(const csr_matrix<double>& A, csrmv_algorithm alg, csrmv_descr* d)
+    {
+        lab_csr dA = A.device();
+        if(alg == csrmv_algorithm::merge_path || alg == csrmv_algorithm::nnzsplit)
+            lab_spmv_set_algorithm(dA, LAB_SPMV_MERGE, 0);
+        ok(lab_spmv_analysis(dA, nullptr), "csrmv_analysis");
+        if(d)
+            d->analysed = 1;
+    }
+    void csrmv_solve(double alpha, const csr_matrix<double>& A, const vector<double>& x,
+                     double beta, vector<double>& y, csrmv_algorithm, const csrmv_descr*)
+    {
+        double* yp = beta == 0.0 ? y.device_write() : y.device_readwrite();
+        ok(lab_spmv(alpha, A.device(), x.device_read(), beta, yp, nullptr), "csrmv_solve");
+    }
+
+    void create_csrgeam_descr(csrgeam_descr** d)
+    {
+        *d = new csrgeam_descr();
+    }
+    void destroy_csrgeam_descr(csrgeam_descr* d)
+    {
+        delete d;
+    }
+    void csrgeam_nnz(const csr_matrix<double>& A, const csr_matrix<double>& B,
+                     csr_matrix<double>& C, csrgeam_algorithm, csrgeam_descr*)
+    {
+        // pattern and values are produced together by csrgeam_solve
+        lab_csr out = nullptr;
+        if(ok(lab_spgeam(1.0, A.device(), 1.0, B.device(), &out, nullptr), "csrgeam_nnz"))
+            C.adopt(out, true);
+    }
+    void csrgeam_solve(double alpha, const csr_matrix<double>& A, double beta,
+                       const csr_matrix<double>& B, csr_matrix<double>& C, csrgeam_algorithm,
+                       const csrgeam_descr*)
+    {
+        lab_csr out = nullptr;
+        if(ok(lab_spgeam(alpha, A.device(), beta, B.device(), &out, nullptr), "csrgeam_solve"))
+            C.adopt(out, true);
+    }
+
+    void create_csrgemm_descr(csrgemm_descr** d)
+    {
+        *d = new csrgemm_descr();
+    }
+    void destroy_csrgemm_descr(csrgemm_descr* d)
+    {
+        delete d;
+    }
+    void csrgemm_nnz(const csr_matrix<double>& A, const csr_matrix<double>& B,
+                     const csr_matrix<double>&, csr_matrix<double>& C, csrgemm_algorithm,
+                     csrgemm_descr*)
+    {
+        lab_csr out = nullptr;
+        if(ok(lab_spgemm(A.device(), B.device(), &out, nullptr), "csrgemm_nnz"))
+            C.adopt(out, true);
+    }
+    void csrgemm_solve(double alpha, const csr_matrix<double>& A, const csr_matrix<double>& B,
+                       double, const csr_matrix<double>&, csr_matrix<double>& C, csrgemm_algorithm,
+                       const csrgemm_descr*)
+    {
+        lab_csr out = nullptr;
+        if(!ok(lab_spgemm(A.device(), B.device(), &out, nullptr), "csrgemm_solve"))
+            return;
+        if(alpha != 1.0)
+        {
+            lab_csr scaled = nullptr;
+            if(ok(lab_spgeam(alpha, out, 0.0, out, &scaled, nullptr), "csrgemm_solve scale"))
+            {
+                lab_csr_destroy(out);
+                out = scaled;
+            }
+        }
+        C.adopt(out, true);
+    }
+
+    template <typename T>
+    void exclusive_scan(vector<T>& x)
+    {
+        if(sizeof(T) == 8)
+            ok(lab_exclusive_scan_i64((int64_t)x.get_size(),
+                                      reinterpret_cast<int64_t*>(x.device_readwrite()), nullptr),
+               "exclusive_scan");
+        else
+            ok(lab_exclusive_scan_i32((int64_t)x.get_size(),
+                                      reinterpret_cast<int32_t*>(x.device_readwrite()), nullptr),
+               "exclusive_scan");
+    }
+    template void exclusive_scan<int>(vector<int>&);
+    template void exclusive_scan<int64_t>(vector<int64_t>&);
+
+    bool is_device_available()
+    {
+        return lab_init(-1) == LAB_OK;
+    }
+
+    void synchronize()
+    {
+        lab_synchronize(nullptr);
+    }
+
+    // ============================================================ iter_control
+    // iter_control.cpp:38-91
+    bool iter_control::residual_converges(double residual_norm,
+                                          double initial_residual_norm) const
+    {
+        if(std::isnan(residual_norm))
+        {
+            std::cout << "Error: NaN detected in residual norm" << std::endl;
+            return false;
+        }
+        if(std::isnan(initial_residual_norm))
+        {
+            std::cout << "Error: NaN detected in initial residual norm" << std::endl;
+            return false;
+        }
+        if(residual_norm <= abs_tol)
+            return true;
+        if(residual_norm / initial_residual_norm <= rel_tol)
+            return true;
+        return false;
+    }
+
+    bool iter_control::exceed_max_iter(int iter) const
+    {
+        return iter > max_iter;
+    }
+
+    bool iter_control::exceed_max_cycle(int cycle) const
+    {
+        return cycle > max_cycle;
+    }
+
+    static lab_iter_control to_lab(const iter_control& c)
+    {
+        lab_iter_control l;
+        l.rel_tol   = c.rel_tol;
+        l.abs_tol   = c.abs_tol;
+        l.max_iter  = c.max_iter;
+        l.max_cycle = c.max_cycle;
+        return l;
+    }
+
+    // ============================================================ AMG
+    hierarchy::hierarchy()
+        : on_host(true)
+    {
+    }
+
+    bool hierarchy::is_on_host() const
+    {
+        return on_host;
+    }
+
+    void hierarchy::move_to_device()
+    {
+        on_host = false;
+    }
+
+    void hierarchy::move_to_host()
+    {
+        on_host = true;
+    }
+
+    void hierarchy::adopt(lab_hierarchy hh)
+    {
+        // drop every borrowed level before the previous device hierarchy goes
+        for(auto& M : A_cs)
+            M.reset();
+        for(auto& M : prolongations)
+            M.reset();
+        for(auto& M : restrictions)
+            M.reset();
+        device = std::shared_ptr<lab_hier_s>(hh, [](lab_hier_s* p) { lab_hierarchy_destroy(p); });
+        int L  = 0;
+        lab_hierarchy_levels(hh, &L);
+        total_levels = L;
+        for(int l = 0; l <= L; l++)
+        {
+            lab_csr A = nullptr, P = nullptr, R = nullptr;
+            if(l < L)
+                lab_hierarchy_level(hh, l, &A, &P, &R);
+            else
+                lab_hierarchy_level(hh, l, &A, nullptr, nullptr);
+            A_cs[l].adopt(A, false);
+            if(l < L)
+            {
+                prolongations[l].adopt(P, false);
+                restrictions[l].adopt(R, false);
+            }
+        }
+    }
+
+    static void setup(lab_amg_kind kind, const csr_matrix<double>& A, int max_level,
+                      hierarchy& h)
+    {
+        lab_hierarchy hh = nullptr;
+        if(ok(lab_amg_setup(kind, A.device(), max_level, &hh, nullptr), "amg setup"))
+            h.adopt(hh);
+    }
+
+    void saamg_setup(const csr_matrix<double>& A, int max_level, hierarchy& h)
+    {
+        setup(LAB_AMG_SA, A, max_level, h);
+    }
+    void uaamg_setup(const csr_matrix<double>& A, int max_level, hierarchy& h)
+    {
+        setup(LAB_AMG_UA, A, max_level, h);
+    }
+    void rsamg_setup(const csr_matrix<double>& A, int max_level, hierarchy& h)
+    {
+        setup(LAB_AMG_RS, A, max_level, h);
+    }
+
+    static lab_amg_options make_options(int n1, int n2, cycle c, smoother s, double omega)
+    {
+        lab_amg_options o;
+        lab_amg_options_default(&o);
+        o.n1       = n1;
+        o.n2       = n2;
+        o.cycle    = (int)c;
+        o.smoother = (int)s;
+        o.omega    = omega;
+        return o;
+    }
+
+    int amg_solve(const hierarchy& h, vector<double>& x, const vector<double>& b, int n1, int n2,
+                  cycle c, smoother s, iter_control control)
+    {
+        if(!h.device)
+        {
+            std::cerr << "Error: amg_solve called before an AMG setup" << std::endl;
+            return -1;
+        }
+        lab_amg_options  o   = make_options(n1, n2, c, s, 1.0);
+        lab_iter_control ctl = to_lab(control);
+        lab_solve_info   info{};
+        lab_status st = lab_amg_solve(h.device.get(), &o, b.device_read(), x.device_readwrite(),
+                                      &ctl, &info, nullptr);
+        ok(st, "amg_solve");
+        return info.iterations;
+    }
+
+    void compute_strong_connections(const csr_matrix<double>& A, double eps,
+                                    vector<int>& connections)
+    {
+        if(connections.get_size() < (size_t)A.get_nnz())
+            connections.resize(A.get_nnz());
+        ok(lab_strength(A.device(), eps, connections.device_write(), nullptr),
+           "compute_strong_connections");
+    }
+
+    void compute_classical_strong_connections(const csr_matrix<double>& A, double theta,
+                                              csr_matrix<double>& S, vector<int>& connections)
+    {
+        if(connections.get_size() < (size_t)A.get_nnz())
+            connections.resize(A.get_nnz());
+        lab_csr out = nullptr;
+        if(ok(lab_classical_strength(A.device(), theta, connections.device_readwrite(), &out,
+                                     nullptr),
+              "compute_classical_strong_connections"))
+            S.adopt(out, true);
+    }
+
+    bool compute_aggregates_using_pmis(const csr_matrix<double>& A,
+                                       const vector<int>&        connections,
+                                       vector<int64_t>&          aggregates,
+                                       vector<int64_t>&          aggregate_root_nodes)
+    {
+        if(aggregates.get_size() < (size_t)A.get_m())
+            aggregates.resize(A.get_m());
+        if(aggregate_root_nodes.get_size() < (size_t)A.get_m())
+            aggregate_root_nodes.resize(A.get_m());
+        return ok(lab_pmis_aggregate_roots(A.device(), connections.device_read(),
+                                           aggregates.device_write(),
+                                           aggregate_root_nodes.device_write(), nullptr, nullptr),
+                  "compute_aggregates_using_pmis");
+    }
+
+    void compute_cfpoint_first_pass(const csr_matrix<double>& S, const csr_matrix<double>&,
+                                    vector<uint32_t>& cfpoints)
+    {
+        if(cfpoints.get_size() < (size_t)S.get_m())
+            cfpoints.resize(S.get_m());
+        ok(lab_cfpoints_passes(S.device(), cfpoints.device_write(), 1, 0, nullptr),
+           "compute_cfpoint_first_pass");
+    }
+
+    void compute_cfpoint_second_pass(const csr_matrix<double>& S, vector<uint32_t>& cfpoints)
+    {
+        ok(lab_cfpoints_passes(S.device(), cfpoints.device_readwrite(), 0, 1, nullptr),
+           "compute_cfpoint_second_pass");
+    }
+
+    void galarkin_triple_product(const csr_matrix<double>& R, const csr_matrix<double>& A,
+                                 const csr_matrix<double>& P, csr_matrix<double>& A_coarse)
+    {
+        csr_matrix<double> AP;
+        A.multiply_by_matrix(AP, P);
+        R.multiply_by_matrix(A_coarse, AP);
+    }
+
+    // ============================================================ preconditioners
+    jacobi_precond::jacobi_precond() {}
+    jacobi_precond::~jacobi_precond()
+    {
+        if(M)
+            lab_precond_destroy(M);
+    }
+    void jacobi_precond::build(const csr_matrix<double>& A)
+    {
+        if(M)
+            lab_precond_destroy(M);
+        M = nullptr;
+        ok(lab_precond_create_jacobi(A.device(), &M, nullptr), "jacobi_precond::build");
+    }
+    void jacobi_precond::solve(const vector<double>& rhs, vector<double>& x) const
+    {
+        ok(lab_precond_apply(M, rhs.device_read(), x.device_write(), nullptr),
+           "jacobi_precond::solve");
+    }
+    void jacobi_precond::move_to_device()
+    {
+        on_host = false;
+    }
+    void jacobi_precond::move_to_host()
+    {
+        on_host = true;
+    }
+    bool jacobi_precond::is_on_host() const
+    {
+        return on_host;
+    }
+
+    amg_precond::amg_precond(int n1, int n2, cycle c, smoother s, double omega)
+        : opts(make_options(n1, n2, c, s, omega))
+    {
+    }
+    amg_precond::~amg_precond()
+    {
+        if(M)
+            lab_precond_destroy(M);
+    }
+    void amg_precond::set_setup(lab_amg_kind k, int ml)
+    {
+        kind      = k;
+        max_level = ml;
+    }
+    void amg_precond::set_precision(lab_precision p)
+    {
+        opts.precision = p;
+    }
+    void amg_precond::set_coarse_solver(lab_coarse c)
+    {
+        opts.coarse = c;
+    }
+    void amg_precond::attach(const hierarchy& hier)
+    {
+        h = &hier;
+    }
+    void amg_precond::build(const csr_matrix<double>& A)
+    {
+        if(!h)
+        {
+            setup((lab_amg_kind)kind, A, max_level, own);
+            h = &own;
+        }
+        if(M)
+            lab_precond_destroy(M);
+        M = nullptr;
+        if(!h->device)
+        {
+            std::cerr << "Error: amg_precond::build: no hierarchy" << std::endl;
+            return;
+        }
+        ok(lab_precond_create_amg(h->device.get(), &opts, &M, nullptr), "amg_precond::build");
+    }
+    void amg_precond::solve(const vector<double>& rhs, vector<double>& x) const
+    {
+        ok(lab_precond_apply(M, rhs.device_read(), x.device_write(), nullptr), "amg_precond::solve");
+    }
+    void amg_precond::move_to_device()
+    {
+        on_host = false;
+    }
+    void amg_precond::move_to_host()
+    {
+        on_host = true;
+    }
+    bool amg_precond::is_on_host() const
+    {
+        return on_host;
+    }
+
+    // ============================================================ CG
+    cg_solver::cg_solver()
+        : restart_iter(-1)
+        , on_host(false)
+    {
+    }
+    cg_solver::~cg_solver() {}
+
+    void cg_solver::build(const csr_matrix<double>& A)
+    {
+        p.resize(A.get_m());
+        z.resize(A.get_m());
+        res.resize(A.get_m());
+    }
+
+    int cg_solver::solve_nonprecond(const csr_matrix<double>& A, vector<double>& x,
+                                    const vector<double>& b, iter_control control)
+    {
+        lab_iter_control ctl = to_lab(control);
+        lab_status       st  = lab_pcg_solve(A.device(), nullptr, b.device_read(),
+                                      x.device_readwrite(), &ctl, &info, nullptr);
+        ok(st, "cg_solver::solve_nonprecond");
+        return info.iterations;
+    }
+
+    int cg_solver::solve_precond(const csr_matrix<double>& A, vector<double>& x,
+                                 const vector<double>& b, const preconditioner* precond,
+                                 iter_control control)
+    {
+        lab_iter_control ctl = to_lab(control);
+        if(lab_precond M = precond->device_handle())
+        {
+            lab_status st = lab_pcg_solve(A.device(), M, b.device_read(), x.device_readwrite(),
+                                          &ctl, &info, nullptr);
+            ok(st, "cg_solver::solve_precond");
+            return info.iterations;
+        }
+        // A user-defined preconditioner: the reference loop (cg.cpp:136-223) on
+        // device vectors, calling the preconditioner through its virtual solve().
+        compute_residual(A, x, b, res);
+        double initial_res_norm = norm_inf(res);
+        precond->solve(res, z);
+        p.copy_from(z);
+        double gamma = dot_product(z, res);
+        int    iter  = 0;
+        info         = lab_solve_info{};
+        while(!control.exceed_max_iter(iter))
+        {
+            A.multiply_by_vector(z, p);
+            double alpha = gamma / dot_product(z, p);
+            axpy(alpha, p, x);
+            axpy(-1.0 * alpha, z, res);
+            double res_norm = norm_inf(res);
+            info.final_residual = res_norm;
+            if(control.residual_converges(res_norm, initial_res_norm))
+            {
+                info.converged = 1;
+                break;
+            }
+            precond->solve(res, z);
+            double old_gamma = gamma;
+            gamma            = dot_product(z, res);
+            double beta      = gamma / old_gamma;
+            axpby(1.0, z, beta, p);
+            iter++;
+        }
+        info.iterations       = iter;
+        info.initial_residual = initial_res_norm;
+        info.status           = info.converged ? LAB_OK : LAB_NOT_CONVERGED;
+        return iter;
+    }
+
+    int cg_solver::solve(const csr_matrix<double>& A, vector<double>& x, const vector<double>& b,
+                         const preconditioner* precond, iter_control control)
+    {
+        if(precond == nullptr)
+            return solve_nonprecond(A, x, b, control);
+        return solve_precond(A, x, b, precond, control);
+    }
+
+    void cg_solver::move_to_host()
+    {
+        on_host = true;
+    }
+    void cg_solver::move_to_device()
+    {
+        on_host = false;
+    }
+    bool cg_solver::is_on_host() const
+    {
+        return on_host;
+    }
+
+    // ============================================================ GMRES
+    gmres_solver::gmres_solver()
+        : restart(-1)
+    {
+    }
+    gmres_solver::~gmres_solver() {}
+
+    void gmres_solver::build(const csr_matrix<double>& A, int r)
+    {
+        restart = std::min(r, A.get_m() - 1);
+    }
+
+    int gmres_solver::solve_nonprecond(const csr_matrix<double>& A, vector<double>& x,
+                                       const vector<double>& b, iter_control control)
+    {
+        lab_iter_control ctl = to_lab(control);
+        ok(lab_gmres_solve(A.device(), nullptr, restart, b.device_read(), x.device_readwrite(),
+                           &ctl, &info, nullptr),
+           "gmres_solver::solve");
+        return info.iterations;
+    }
+
+    int gmres_solver::solve_precond(const csr_matrix<double>& A, vector<double>& x,
+                                    const vector<double>& b, const preconditioner* precond,
+                                    iter_control control)
+    {
+        lab_iter_control ctl = to_lab(control);
+        lab_precond      M   = precond ? precond->device_handle() : nullptr;
+        if(precond && !M)
+            std::cerr << "Error: gmres_solver needs a device preconditioner (jacobi_precond or "
+                         "amg_precond); solving without one"
+                      << std::endl;
+        ok(lab_gmres_solve(A.device(), M, restart, b.device_read(), x.device_readwrite(), &ctl,
+                           &info, nullptr),
+           "gmres_solver::solve");
+        return info.iterations;
+    }
+
+    int gmres_solver::solve(const csr_matrix<double>& A, vector<double>& x,
+                            const vector<double>& b, const preconditioner* precond,
+                            iter_control control)
+    {
+        if(precond == nullptr)
+            return solve_nonprecond(A, x, b, control);
+        return solve_precond(A, x, b, precond, control);
+    }
+}

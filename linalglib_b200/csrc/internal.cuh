@@ -1,0 +1,212 @@
+// Internal declarations shared by the liblinalg_b200 translation units.
+#pragma once
+
+#include "lab.h"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+namespace lab
+{
+    // ------------------------------------------------------------ errors
+    void       set_error(const char* fmt, ...);
+    lab_status cuda_status(cudaError_t e, const char* what, const char* file, int line);
+
+#define LAB_CUDA(call)                                                            \
+    do                                                                            \
+    {                                                                             \
+        cudaError_t e_ = (call);                                                  \
+        if(e_ != cudaSuccess)                                                     \
+            return ::lab::cuda_status(e_, #call, __FILE__, __LINE__);             \
+    } while(0)
+
+#define LAB_TRY(x)                                                                \
+    do                                                                            \
+    {                                                                             \
+        lab_status s_ = (x);                                                      \
+        if(s_ != LAB_OK)                                                          \
+            return s_;                                                            \
+    } while(0)
+
+#define LAB_ARG(cond, msg)                                                        \
+    do                                                                            \
+    {                                                                             \
+        if(!(cond))                                                               \
+        {                                                                         \
+            ::lab::set_error("bad argument: %s (%s)", msg, #cond);                \
+            return LAB_BAD_ARG;                                                   \
+        }                                                                         \
+    } while(0)
+
+    // Kernel launches go through this macro so the library can count them.
+    extern std::atomic<int64_t> g_launches;
+#define LAB_LAUNCH(kernel, grid, block, smem, stream, ...)                        \
+    do                                                                            \
+    {                                                                             \
+        kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);               \
+        ::lab::g_launches.fetch_add(1, std::memory_order_relaxed);                \
+        cudaError_t le_ = cudaGetLastError();                                     \
+        if(le_ != cudaSuccess)                                                    \
+            return ::lab::cuda_status(le_, #kernel, __FILE__, __LINE__);          \
+    } while(0)
+
+    // ------------------------------------------------------------ device / memory
+    lab_status ensure_init();
+    int        num_sms();
+    inline cudaStream_t to_stream(lab_stream s)
+    {
+        return reinterpret_cast<cudaStream_t>(s);
+    }
+
+    // Stream-ordered allocation from the device's default memory pool (the pool
+    // keeps freed blocks, so setup temporaries cost no driver round trips).
+    // Every allocation is padded by 64 bytes so vectorised loads that round a
+    // range out to a 16-byte boundary stay inside it.
+    lab_status dmalloc(void** p, size_t bytes, cudaStream_t s);
+    void       dfree(void* p, cudaStream_t s);
+
+    template <class T>
+    inline lab_status dalloc(T** p, size_t n, cudaStream_t s)
+    {
+        return dmalloc(reinterpret_cast<void**>(p), n * sizeof(T), s);
+    }
+
+    // RAII device buffer for temporaries.
+    template <class T>
+    struct dbuf
+    {
+        T*           p = nullptr;
+        size_t       n = 0;
+        cudaStream_t s = 0;
+        dbuf()         = default;
+        dbuf(const dbuf&) = delete;
+        dbuf& operator=(const dbuf&) = delete;
+        ~dbuf()
+        {
+            release();
+        }
+        lab_status alloc(size_t count, cudaStream_t st)
+        {
+            release();
+            s = st;
+            n = count;
+            return dalloc(&p, count > 0 ? count : 1, st);
+        }
+        void release()
+        {
+            if(p)
+                dfree(p, s);
+            p = nullptr;
+            n = 0;
+        }
+        T* get() const
+        {
+            return p;
+        }
+    };
+
+    // Pinned host staging for scalar read-backs.
+    lab_status pinned_scratch(void** p, size_t bytes);
+
+    // ------------------------------------------------------------ CSR
+    struct spmv_plan
+    {
+        int    analysed = 0;
+        int    alg      = LAB_SPMV_ROWSEQ; // lab_spmv_alg
+        int    lanes    = 1;               // lanes per row for LAB_SPMV_VECTOR
+        int    forced   = 0;
+        int    max_row  = 0;
+        double avg_row  = 0.0;
+        // LAB_SPMV_ROWSEQ: row blocks of bounded nnz
+        int  rows_per_block = 0;
+        int  nblocks        = 0;
+        int* block_row      = nullptr; // device int32[nblocks+1] (row starts), null = uniform
+        // LAB_SPMV_MERGE: merge-path split points
+        int  merge_items_per_block = 0;
+        int* merge_coords          = nullptr; // device int32[2*(nblocks+1)]
+    };
+
+    struct csr_values_lp
+    {
+        float*          f32  = nullptr;
+        __nv_bfloat16*  bf16 = nullptr;
+        float*          invd32 = nullptr;
+    };
+
+    // Unique ids for cached solver state (graphs are keyed by object identity,
+    // not by address, so a freed-and-reused address never matches).
+    uint64_t next_uid();
+    // Drop solver caches keyed by an object that is being destroyed.
+    void solver_cache_forget(const void* key);
+
+    struct lab_csr_impl
+    {
+        uint64_t  uid = next_uid();
+        int64_t   m = 0, n = 0, nnz = 0;
+        int32_t*  row_ptr = nullptr;
+        int32_t*  col_ind = nullptr;
+        double*   val     = nullptr;
+        spmv_plan plan;
+        // cached diagonal data for smoothers (built on demand)
+        double* diag    = nullptr;
+        double* invdiag = nullptr;
+        csr_values_lp lp;
+    };
+
+    lab_status csr_alloc(lab_csr_impl** A, int64_t m, int64_t n, int64_t nnz, cudaStream_t s);
+    void       csr_release(lab_csr_impl* A);
+    lab_status csr_ensure_invdiag(lab_csr_impl* A, cudaStream_t s);
+    lab_status csr_ensure_lowp(lab_csr_impl* A, int precision, int use_bf16, cudaStream_t s);
+    lab_status spmv_analyse(lab_csr_impl* A, cudaStream_t s);
+
+    // ------------------------------------------------------------ shared device helpers
+    lab_status scan_i32(int32_t* x, int64_t n, cudaStream_t s); // in-place exclusive
+    lab_status scan_i64(int64_t* x, int64_t n, cudaStream_t s);
+    // Exclusive scan of n counts into row_ptr[0..n] (row_ptr[n] = total); total to host.
+    lab_status counts_to_rowptr(const int32_t* counts, int32_t* row_ptr, int64_t n,
+                                int64_t* total, cudaStream_t s);
+    lab_status max_i64(const int64_t* x, int64_t n, int64_t* result_host, cudaStream_t s);
+    lab_status copy_d2h_sync(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
+    // Fixed-shape reduction grid shared by every deterministic reduction.
+    constexpr int kRedBlocks  = 1184; // 8 x 148 SMs
+    constexpr int kRedThreads = 256;
+
+    template <class T>
+    __host__ __device__ inline T ceil_div(T a, T b)
+    {
+        return (a + b - 1) / b;
+    }
+
+    __device__ __forceinline__ double warp_sum(double v)
+    {
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+    }
+
+    // max that propagates NaN (fmax drops it, which would let a NaN residual
+    // norm read as small)
+    __device__ __forceinline__ double nanmax(double a, double b)
+    {
+        return (a != a || b != b) ? __longlong_as_double(0x7ff8000000000000ll) : fmax(a, b);
+    }
+
+    __device__ __forceinline__ double warp_max(double v)
+    {
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            v = nanmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        return v;
+    }
+}
+
+struct lab_csr_s : lab::lab_csr_impl
+{
+};

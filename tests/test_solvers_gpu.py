@@ -1,0 +1,209 @@
+"""Cycles and Krylov solvers on the GPU vs the oracle and the compiled reference.
+
+Acceptance follows the reference's check_solution (clients/common/utility.cpp:426-476):
+the relative inf-norm residual reaches the requested tolerance; in addition the
+iteration counts must match the CPU oracle (+-1 for rounding of the device
+reductions) and the solutions must agree to well inside the tolerance.
+"""
+import numpy as np
+import pytest
+import torch
+
+from linalglib_b200 import _lib as L
+from linalglib_b200 import problems as P
+
+from helpers import inf_rel_residual
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "poisson2d_64": lambda: P.poisson2d(64),
+    "poisson3d_20": lambda: P.poisson3d(20),
+    "laplacian3d_14": lambda: P.graph_laplacian3d(14, seed=2),
+    "diffusion27_10": lambda: P.diffusion27(10, seed=0),
+}
+
+
+def _setup(gpu, A, kind=L.AMG_SA):
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    return dA, gpu.Hierarchy(dA, kind=kind)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("omega", [1.0, 2.0 / 3.0])
+def test_vcycle_matches_oracle(gpu, oracle, name, omega):
+    A = CASES[name]()
+    dA, H = _setup(gpu, A)
+    Ho = oracle.amg_setup(A)
+    r = np.random.default_rng(1).uniform(-1, 1, A[0].size - 1)
+    z = H.cycle(gpu.vec(r), options=gpu.amg_options(omega=omega, coarse=L.COARSE_DIRECT)).cpu().numpy()
+    zo = Ho.vcycle(r, omega=omega, coarse=1)
+    assert np.max(np.abs(z - zo)) <= 1e-12 * np.max(np.abs(zo))
+
+
+def test_vcycle_coarse_gs_matches_reference(gpu, reference):
+    """max_level 2 leaves a 495-row coarsest level: the reference's 1000 GS sweeps."""
+    A = P.poisson2d(128)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    H = gpu.Hierarchy(dA, kind=L.AMG_SA, max_level=2)
+    Hr = reference.amg_setup(A, kind=0, max_level=2)
+    r = np.random.default_rng(2).uniform(-1, 1, A[0].size - 1)
+    z = H.cycle(gpu.vec(r), options=gpu.amg_options(coarse=L.COARSE_GS)).cpu().numpy()
+    zr = Hr.vcycle(r)
+    assert np.max(np.abs(z - zr)) <= 1e-12 * np.max(np.abs(zr))
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("kind", [L.AMG_SA, L.AMG_UA])
+@pytest.mark.parametrize("omega", [1.0, 2.0 / 3.0])
+def test_amg_pcg_matches_oracle(gpu, oracle, name, kind, omega):
+    A = CASES[name]()
+    b, xt = P.rhs_from_solution(*A[:3], seed=0)
+    dA, H = _setup(gpu, A, kind)
+    M = gpu.Preconditioner.amg(H, gpu.amg_options(omega=omega))
+    ctl = gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=500)
+    x, info = gpu.pcg(dA, gpu.vec(b), M=M, control=ctl)
+    x = x.cpu().numpy()
+    Ho = oracle.amg_setup(A, kind=kind)
+    xo, ito, relo = Ho.pcg(b, omega=omega, coarse=1, rel_tol=1e-8, abs_tol=0.0, max_iter=500)
+    assert info.converged == 1 and info.status == L.LAB_OK
+    assert abs(info.iterations - ito) <= 1, (info.iterations, ito)
+    # the reference's criterion: ||r||_inf / ||r0||_inf <= rtol with x0 = 0 (r0 = b)
+    assert inf_rel_residual(A, x, b) <= 1e-8 * 1.0001
+    assert np.max(np.abs(x - xo)) <= 1e-6 * np.max(np.abs(xo))
+
+
+def test_amg_pcg_matches_reference(gpu, reference):
+    A = P.poisson2d(128)
+    b, xt = P.rhs_from_solution(*A[:3], seed=0)
+    dA, H = _setup(gpu, A)
+    M = gpu.Preconditioner.amg(H)
+    x, info = gpu.pcg(dA, gpu.vec(b), M=M,
+                      control=gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=1000))
+    Hr = reference.amg_setup(A, kind=0)
+    xr, itr = Hr.pcg(b, rel_tol=1e-8, abs_tol=1e-300)
+    assert itr == 37  # the reference's count on this problem
+    assert abs(info.iterations - itr) <= 1
+    x = x.cpu().numpy()
+    assert np.max(np.abs(x - xr)) <= 1e-7 * np.max(np.abs(xr))
+    assert np.max(np.abs(x - xt)) <= 1e-6
+
+
+def test_pcg_host_buffers(gpu):
+    A = P.poisson3d(16)
+    b, _ = P.rhs_from_solution(*A[:3], seed=5)
+    dA, H = _setup(gpu, A)
+    M = gpu.Preconditioner.amg(H)
+    ctl = gpu.iter_control(rel_tol=1e-10, abs_tol=0.0)
+    xd, infod = gpu.pcg(dA, gpu.vec(b), M=M, control=ctl)
+    xh = np.zeros_like(b)
+    xh, infoh = gpu.pcg_host(dA, b.copy(), xh, M=M, control=ctl)
+    assert infod.iterations == infoh.iterations
+    assert np.array_equal(xd.cpu().numpy(), xh)
+
+
+@pytest.mark.parametrize("name", ["poisson2d_64", "laplacian3d_14"])
+def test_jacobi_pcg_matches_oracle(gpu, oracle, name):
+    A = CASES[name]()
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    M = gpu.Preconditioner.jacobi(dA)
+    x, info = gpu.pcg(dA, gpu.vec(b), M=M,
+                      control=gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=3000))
+    xo, ito = oracle.cg(A, b, jacobi=True, rel_tol=1e-8, abs_tol=0.0, max_iter=3000)
+    assert info.converged == 1
+    assert abs(info.iterations - ito) <= 2, (info.iterations, ito)
+    assert np.max(np.abs(x.cpu().numpy() - xo)) <= 1e-6 * np.max(np.abs(xo))
+
+
+def test_plain_cg_restart_quirk(gpu, oracle):
+    """No preconditioner: the reference restarts every iteration (cg.cpp:89)."""
+    A = P.poisson2d(24)
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    x, info = gpu.pcg(dA, gpu.vec(b), M=None,
+                      control=gpu.iter_control(rel_tol=1e-6, abs_tol=0.0, max_iter=40))
+    xo, ito = oracle.cg(A, b, jacobi=False, rel_tol=1e-6, abs_tol=0.0, max_iter=40)
+    assert info.iterations == ito
+    assert np.max(np.abs(x.cpu().numpy() - xo)) <= 1e-9 * np.max(np.abs(xo))
+
+
+@pytest.mark.parametrize("name", ["poisson2d_64", "poisson3d_20"])
+def test_amg_solve_stationary(gpu, oracle, reference, name):
+    A = CASES[name]()
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    dA, H = _setup(gpu, A)
+    x, info = H.solve(gpu.vec(b), options=gpu.amg_options(n1=1, n2=1),
+                      control=gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_cycle=300))
+    Ho = oracle.amg_setup(A)
+    xo, ito = Ho.amg_solve(b, n1=1, n2=1, coarse=1, rel_tol=1e-8, abs_tol=0.0, max_cycle=300)
+    assert info.converged == 1
+    assert abs(info.iterations - ito) <= 1
+    assert np.max(np.abs(x.cpu().numpy() - xo)) <= 1e-6 * np.max(np.abs(xo))
+
+
+@pytest.mark.parametrize("cycle", [L.CYCLE_W, L.CYCLE_F])
+def test_wf_cycles_match_reference(gpu, reference, cycle):
+    A = P.poisson2d(48)
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    dA, H = _setup(gpu, A)
+    x, info = H.solve(gpu.vec(b), options=gpu.amg_options(cycle=cycle),
+                      control=gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_cycle=300))
+    Hr = reference.amg_setup(A, kind=0)
+    xr, itr = Hr.amg_solve(b, n1=1, n2=1, cycle=cycle, rel_tol=1e-8, abs_tol=1e-300, max_cycle=300)
+    assert info.converged == 1
+    assert abs(info.iterations - itr) <= 1, (info.iterations, itr)
+    assert np.max(np.abs(x.cpu().numpy() - xr)) <= 1e-6 * np.max(np.abs(xr))
+
+
+@pytest.mark.parametrize("smoother", [L.SMOOTH_GS, L.SMOOTH_SGS, L.SMOOTH_SOR, L.SMOOTH_SSOR])
+def test_multicolour_smoothers_converge(gpu, smoother):
+    A = P.poisson3d(18)
+    b, xt = P.rhs_from_solution(*A[:3], seed=0)
+    dA, H = _setup(gpu, A)
+    M = gpu.Preconditioner.amg(H, gpu.amg_options(smoother=smoother))
+    x, info = gpu.pcg(dA, gpu.vec(b), M=M, control=gpu.iter_control(rel_tol=1e-10, abs_tol=0.0))
+    assert info.converged == 1 and info.iterations < 60
+    assert inf_rel_residual(A, x.cpu().numpy(), b) <= 1e-10 * 1.0001
+
+
+def test_gmres_matches_reference(gpu, reference):
+    A = P.graph_laplacian3d(10, seed=1)
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    x, info = gpu.gmres(dA, gpu.vec(b), restart=20,
+                        control=gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=200))
+    xr, itr = reference.gmres(A, b, restart=20, rel_tol=1e-8, abs_tol=1e-300, max_iter=200)
+    assert info.converged == 1
+    assert abs(info.iterations - itr) <= 1
+    assert np.max(np.abs(x.cpu().numpy() - xr)) <= 1e-6 * np.max(np.abs(xr))
+
+
+def test_gmres_amg_preconditioned(gpu):
+    A = P.diffusion27(10, seed=3)
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    dA, H = _setup(gpu, A)
+    M = gpu.Preconditioner.amg(H)
+    x, info = gpu.gmres(dA, gpu.vec(b), M=M, restart=30,
+                        control=gpu.iter_control(rel_tol=1e-10, abs_tol=0.0, max_iter=100))
+    assert info.converged == 1
+    assert inf_rel_residual(A, x.cpu().numpy(), b) <= 1e-8
+
+
+def test_nan_rhs_reports_nan(gpu):
+    A = P.poisson2d(16)
+    b = np.ones(256)
+    b[7] = np.nan
+    dA, H = _setup(gpu, A)
+    M = gpu.Preconditioner.amg(H)
+    x, info = gpu.pcg(dA, gpu.vec(b), M=M, control=gpu.iter_control(max_iter=50))
+    assert info.status == L.LAB_NAN and info.converged == 0
+
+
+def test_zero_rhs_converges_immediately(gpu):
+    A = P.poisson2d(16)
+    dA, H = _setup(gpu, A)
+    M = gpu.Preconditioner.amg(H)
+    x, info = gpu.pcg(dA, gpu.vec(np.zeros(256)), M=M)
+    assert info.converged == 1 and info.iterations == 0
+    assert torch.count_nonzero(x) == 0
