@@ -1,0 +1,436 @@
+#!/usr/bin/env python3
+"""Benchmark: SA-AMG-preconditioned CG to a 1e-8 relative residual on the 3D
+7-point Poisson operator on a 128^3 grid (2,097,152 rows, 14,581,760 nonzeros),
+FP64, one GPU per process.
+
+A step is one complete time-to-solution: SA-AMG setup from the level-0 matrix
+(strength, PMIS aggregation, smoothed prolongation, transpose, two SpGEMMs per
+level), then PCG with one V-cycle (1+1 Jacobi sweeps, omega 1, the reference
+smoother) per iteration until ||b - A x||_inf / ||b||_inf <= 1e-8.
+
+  value  -- solves per second with A and b resident in HBM (whole job: all ranks)
+  e2e    -- the same through the C ABI with HOST buffers: each step uploads A and
+            b from pinned memory (lab_csr_create + lab_pcg_solve_host) and reads
+            x back, copies inside the timed region
+  roofline -- the dominant kernel of the step (see profiles/), timed with CUDA
+            events on the launching stream
+  cpu_baseline -- the reference LinAlgLib host path compiled from its sources
+            (oracle/_ref) on this machine's cores, one full solve of the same system
+
+Multi-GPU: the single system does not shard (one GPU per system); N ranks solve N
+independent replicas ("replicas only"), value = N / (max over ranks of the time).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import os
+
+if "OMP_NUM_THREADS" not in os.environ:  # the CPU reference uses every host core
+    os.environ["OMP_NUM_THREADS"] = str(os.cpu_count() or 1)
+
+import argparse
+import ctypes
+import json
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "AMG-PCG time-to-1e-8 (mixed vs FP64 on B200); SpMV GB/s vs ~8 TB/s HBM"
+UNIT = "solves/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128, help="grid side of the 3D Poisson system")
+    ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="full", choices=["full", "profile"],
+                    help="profile: only the warm-up and timed device-resident steps (the "
+                         "command the ncu launch lists in profiles/ are taken from)")
+    return ap.parse_args()
+
+
+def problem(n):
+    from linalglib_b200 import problems as P
+    A = P.poisson3d(n)
+    b, xt = P.rhs_from_solution(*A, seed=0)
+    return A, b, xt
+
+
+def spmv_bytes(m, n, nnz, vb=8):
+    # the reference's effective-bandwidth formula (test_functions_multiply_by_vector.cpp:122-124)
+    return vb * (nnz + m + n) + 4 * (m + 1 + nnz)
+
+
+# ------------------------------------------------------------------ distributed
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, need_gpu=True):
+        import torch
+        if need_gpu:
+            torch.cuda.set_device(self.local)
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl" if need_gpu else "gloo",
+                                    timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi samples of this rank's GPU during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU baseline
+def cpu_reference_solve(A, b, rtol):
+    """One full solve on the compiled reference: (setup_s, solve_s, iters)."""
+    from oracle.oracle import load_reference
+    ref = load_reference()
+    if ref is None:
+        return None
+    t0 = time.perf_counter()
+    h = ref.amg_setup(A, kind=0, max_level=20)
+    t1 = time.perf_counter()
+    x, it = h.pcg(b, rel_tol=rtol, abs_tol=1e-300, max_iter=1000)
+    t2 = time.perf_counter()
+    del h
+    return t1 - t0, t2 - t1, it
+
+
+def cpu_port_solve(A, b, rtol):
+    from oracle.oracle import Oracle
+    O = Oracle()
+    t0 = time.perf_counter()
+    h = O.amg_setup(A, kind=0)
+    t1 = time.perf_counter()
+    x, it, _ = h.pcg(b, rel_tol=rtol, abs_tol=0.0, coarse=0)
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1, it
+
+
+def cpu_baseline(A, b, rtol, n):
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    r = cpu_reference_solve(A, b, rtol)
+    kind = "reference"
+    if r is None:
+        r = cpu_port_solve(A, b, rtol)
+        kind, cores = "port", 1
+    ts, tv, it = r
+    return {"value": 1.0 / (ts + tv), "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"one full solve of the {n}^3 system: setup {ts:.2f} s + PCG {tv:.2f} s "
+                      f"({it} iterations, AMG adapter adds 2 residual SpMVs per V-cycle)"}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args, d):
+    if d.rank != 0:
+        return 0
+    A, b, _ = problem(args.n)
+    warm, steps = min(args.warmup, 1), max(1, min(args.steps, 3))
+    for _ in range(warm):
+        if cpu_reference_solve(A, b, args.rtol) is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "oracle/_ref/liblinalg_ref.so not built (reference sources absent)"}))
+            return 0
+    times, parts = [], []
+    for _ in range(steps):
+        ts, tv, it = cpu_reference_solve(A, b, args.rtol)
+        times.append(ts + tv)
+        parts.append((ts, tv, it))
+    total = sum(times)
+    value = steps / total
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * total / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (3D 7-point Poisson, x_true ~ U[-1,1] seed 0, b = A x_true)",
+        "config": {"workload": f"SA-AMG-PCG, 3D 7-point Poisson {args.n}^3, rtol {args.rtol:g}",
+                   "rows": int(A[0].size - 1), "nnz": int(A[2].size),
+                   "parallelism": "host OpenMP, rank 0 only"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{steps} full solves (setup + PCG) of the {args.n}^3 system"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "setup_s": [p[0] for p in parts], "solve_s": [p[1] for p in parts],
+        "iterations": parts[-1][2],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def dominant_kernel_roofline(core, dA, m, nnz, torch):
+    """Standalone CUDA-event timing of the dominant kernel class (level-0 CSR pass:
+    SpMV on the 128^3 operator, the same row engine as the smoother kernels)."""
+    x = torch.empty(m, dtype=torch.float64, device="cuda").uniform_(-1, 1)
+    y = torch.zeros(m, dtype=torch.float64, device="cuda")
+    flush = torch.empty(160 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    for _ in range(5):
+        dA.spmv(x, y)
+    times = []
+    for _ in range(30):
+        flush.fill_(0.0)  # evict L2 (126 MB) between launches
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dA.spmv(x, y)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) * 1e-3)
+    t = statistics.median(times)
+    algo = spmv_bytes(m, m, nnz)
+    achieved = algo / t / 1e9
+    peak, which = 6547.2, "fallback"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, which = float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        peak, which = 6650.0, "fallback"
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "spmv_poisson3d_128.md")
+    if os.path.exists(prof):
+        mt = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(prof).read())
+        if mt:
+            traffic = float(mt.group(1))
+    return {"bound": "hbm", "kernel": "k_rowseq<op_spmv> on A_0 (level-0 CSR pass)",
+            "achieved": achieved, "peak": peak, "peak_source": which, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": algo,
+            "launch_us": t * 1e6}
+
+
+def run_ours(args, d):
+    import torch
+
+    d.init(need_gpu=True)
+    import linalglib_b200.core as core
+    from linalglib_b200 import _lib as L
+    core.init()
+    A, b, xt = problem(args.n)
+    m, nnz = A[0].size - 1, A[2].size
+    stream = torch.cuda.current_stream()
+    dA = core.CsrMatrix.from_arrays(*A)
+    dA.analyse()
+    bd = core.vec(b)
+    opts = core.amg_options(n1=1, n2=1, omega=1.0)
+    ctl = core.iter_control(rel_tol=args.rtol, abs_tol=0.0, max_iter=1000)
+    keep = []
+
+    def step(x):
+        H = core.Hierarchy(dA, kind=L.AMG_SA, max_level=20)
+        M = core.Preconditioner.amg(H, opts)
+        x.zero_()
+        x, info = core.pcg(dA, bd, x=x, M=M, control=ctl)
+        keep.append((M, H))  # released after the timed region
+        return H, info
+
+    xs = [torch.zeros(m, dtype=torch.float64, device="cuda") for _ in range(2)]
+    for i in range(args.warmup):
+        step(xs[i % 2])
+    torch.cuda.synchronize()
+    keep.clear()
+
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    d.barrier()
+    torch.cuda.synchronize()
+    l0 = core.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    setups, solves, iters, conv = [], [], [], []
+    for i in range(args.steps):
+        H, info = step(xs[i % 2])
+        setups.append(H.setup_ms())
+        solves.append(info.solve_ms)
+        iters.append(info.iterations)
+        conv.append(info.converged)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    d.barrier()
+    launches = core.launch_count() - l0
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    clk = clocks.stop()
+    t_max = d.max(elapsed)
+    keep.clear()
+    x_last = xs[(args.steps - 1) % 2].cpu().numpy()
+    err = float(np.max(np.abs(x_last - xt)))
+    if args.mode == "profile":
+        if d.rank == 0:
+            print(json.dumps({"mode": "profile", "ms_per_step": 1e3 * t_max / args.steps,
+                              "setup_ms": setups, "solve_ms": solves, "iterations": iters[-1],
+                              "gpu_launches": int(launches)}), flush=True)
+        d.close()
+        return 0
+
+    # ---------------- e2e: host buffers through the C ABI
+    import ctypes as C
+    pin = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+           for k, a in (("rp", A[0]), ("ci", A[1]), ("v", A[2]), ("b", b))}
+    xh = torch.zeros(m, dtype=torch.float64).pin_memory()
+    lib = L.lib()
+    sh = core.stream_handle()
+
+    def e2e_step():
+        hA = C.c_void_p()
+        L.check(lib.lab_csr_create(C.byref(hA), m, m, nnz, C.c_void_p(pin["rp"].data_ptr()),
+                                   C.c_void_p(pin["ci"].data_ptr()),
+                                   C.c_void_p(pin["v"].data_ptr()), L.MEM_HOST, sh))
+        hH = C.c_void_p()
+        L.check(lib.lab_amg_setup(L.AMG_SA, hA, 20, C.byref(hH), sh))
+        hM = C.c_void_p()
+        L.check(lib.lab_precond_create_amg(hH, C.byref(opts), C.byref(hM), sh))
+        xh.zero_()
+        info = L.SolveInfo()
+        L.check(lib.lab_pcg_solve_host(hA, hM, C.c_void_p(pin["b"].data_ptr()),
+                                       C.c_void_p(xh.data_ptr()), C.byref(ctl), C.byref(info), sh))
+        return hA, hH, hM
+
+    def e2e_free(hs):
+        hA, hH, hM = hs
+        lib.lab_precond_destroy(hM)
+        lib.lab_hierarchy_destroy(hH)
+        lib.lab_csr_destroy(hA)
+
+    e2e_free(e2e_step())
+    torch.cuda.synchronize()
+    d.barrier()
+    held = []
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        held.append(e2e_step())
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_t = d.max(f0.elapsed_time(f1) * 1e-3)
+    for hs in held:
+        e2e_free(hs)
+    h2d = 4 * (m + 1) + 4 * nnz + 8 * nnz + 8 * m + 8 * m  # A, b, x0
+    d2h = 8 * m
+
+    roof = dominant_kernel_roofline(core, dA, m, nnz, torch)
+
+    if d.rank == 0:
+        cpu = None
+        if args.gpus == 1 and d.world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(A, b, args.rtol, args.n)
+        value = d.world * args.steps / t_max
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (3D 7-point Poisson, x_true ~ U[-1,1] seed 0, b = A x_true)",
+            "config": {"workload": f"SA-AMG-PCG, 3D 7-point Poisson {args.n}^3, rtol {args.rtol:g}",
+                       "rows": int(m), "nnz": int(nnz),
+                       "parallelism": f"replicas x{d.world} (one independent system per GPU)",
+                       "l2": "inputs larger than L2 (A_0 alone is 217 MB)",
+                       "smoother": "1+1 Jacobi, omega 1 (reference)", "coarse": "dense direct"},
+            "e2e": {"value": d.world * args.steps / e2e_t, "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": int(launches),
+            "setup_ms": setups, "solve_ms": solves, "iterations": iters[-1],
+            "converged": all(conv), "max_abs_err_vs_x_true": err,
+        }
+        print(json.dumps(line), flush=True)
+    d.close()
+    return 0
+
+
+def main():
+    args = parse()
+    d = Dist()
+    if args.impl == "reference":
+        return run_reference(args, d)
+    return run_ours(args, d)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,989 @@
+// Multigrid cycles on the device: fused smoother / residual / restriction /
+// prolongation kernels, multicolour Gauss-Seidel, coarsest-level solves, and
+// the V / W / F recursion (amg.cpp:144-513), in FP64 or in reduced precision
+// (FP32 arithmetic over FP32 or BF16 stored values) for the mixed-precision
+// preconditioner.
+#include "cycle.cuh"
+
+#include <cuda_bf16.h>
+#include <type_traits>
+
+namespace lab
+{
+    // ================================================================ ops
+    // Pre-smoothing from a zero guess fused with the residual:
+    //   x = omega D^-1 b   (first Jacobi sweep from x = 0)
+    //   r = b - A x        (x recomputed from b and D^-1 at every gather)
+    template <class VT, class T>
+    struct op_pre0
+    {
+        using val_t                   = VT;
+        using acc_t                   = T;
+        static constexpr bool kFma    = true;
+        static constexpr bool kReduce = false;
+        const T* __restrict__ b;
+        const T* __restrict__ invd;
+        T omega;
+        T* __restrict__ x;
+        T* __restrict__ r;
+        __device__ __forceinline__ T gather(int c) const
+        {
+            return omega * (__ldg(invd + c) * __ldg(b + c));
+        }
+        __device__ __forceinline__ double finish(int i, T s) const
+        {
+            x[i] = gather(i);
+            r[i] = b[i] - s;
+            return 0.0;
+        }
+    };
+
+    // Weighted Jacobi sweep y = x + omega D^-1 (b - A x); with DOT returns y_i dv_i.
+    template <class VT, class T, bool DOT>
+    struct op_jacobi
+    {
+        using val_t                   = VT;
+        using acc_t                   = T;
+        static constexpr bool kFma    = true;
+        static constexpr bool kReduce = DOT;
+        const T* __restrict__ x;
+        const T* __restrict__ b;
+        const T* __restrict__ invd;
+        T omega;
+        T* __restrict__ y;
+        const T* __restrict__ dv;
+        __device__ __forceinline__ T gather(int c) const
+        {
+            return __ldg(x + c);
+        }
+        __device__ __forceinline__ double finish(int i, T s) const
+        {
+            T yi = x[i] + omega * (invd[i] * (b[i] - s));
+            y[i] = yi;
+            return DOT ? (double)yi * (double)dv[i] : 0.0;
+        }
+    };
+
+    template <class VT, class T>
+    struct op_res
+    {
+        using val_t                   = VT;
+        using acc_t                   = T;
+        static constexpr bool kFma    = true;
+        static constexpr bool kReduce = false;
+        const T* __restrict__ x;
+        const T* __restrict__ b;
+        T* __restrict__ r;
+        __device__ __forceinline__ T gather(int c) const
+        {
+            return __ldg(x + c);
+        }
+        __device__ __forceinline__ double finish(int i, T s) const
+        {
+            r[i] = b[i] - s;
+            return 0.0;
+        }
+    };
+
+    // y = x + P e (x may alias y: in-place correction for GS-type smoothers)
+    template <class VT, class T, bool DOT>
+    struct op_prolong
+    {
+        using val_t                   = VT;
+        using acc_t                   = T;
+        static constexpr bool kFma    = true;
+        static constexpr bool kReduce = DOT;
+        const T* __restrict__ e;
+        const T* x;
+        T*       y;
+        const T* __restrict__ dv;
+        __device__ __forceinline__ T gather(int c) const
+        {
+            return __ldg(e + c);
+        }
+        __device__ __forceinline__ double finish(int i, T s) const
+        {
+            T yi = x[i] + s;
+            y[i] = yi;
+            return DOT ? (double)yi * (double)dv[i] : 0.0;
+        }
+    };
+
+    // y = R r
+    template <class VT, class T>
+    struct op_restrict
+    {
+        using val_t                   = VT;
+        using acc_t                   = T;
+        static constexpr bool kFma    = true;
+        static constexpr bool kReduce = false;
+        const T* __restrict__ r;
+        T* __restrict__ y;
+        __device__ __forceinline__ T gather(int c) const
+        {
+            return __ldg(r + c);
+        }
+        __device__ __forceinline__ double finish(int i, T s) const
+        {
+            y[i] = s;
+            return 0.0;
+        }
+    };
+
+    // ================================================================ small kernels
+    template <class T>
+    __global__ void k_zero(T* x, int64_t n, const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+            i += (int64_t)gridDim.x * blockDim.x)
+            x[i] = T(0);
+    }
+
+    template <class T>
+    __global__ void k_copy(T* __restrict__ y, const T* __restrict__ x, int64_t n, const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+            i += (int64_t)gridDim.x * blockDim.x)
+            y[i] = x[i];
+    }
+
+    __global__ void k_copy_d(double* __restrict__ y, const double* __restrict__ x, int64_t n,
+                             const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+            i += (int64_t)gridDim.x * blockDim.x)
+            y[i] = x[i];
+    }
+
+    __global__ void k_d2f(const double* __restrict__ x, float* __restrict__ y, int64_t n,
+                          const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+            i += (int64_t)gridDim.x * blockDim.x)
+            y[i] = (float)x[i];
+    }
+
+    // z = (double) x with (z, r) accumulated for the PCG beta.
+    __global__ void __launch_bounds__(256)
+        k_f2d_dot(const float* __restrict__ x, const double* __restrict__ r, double* __restrict__ z,
+                  int64_t n, double* partial, unsigned int* counter, double* out, const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        double acc = 0.0;
+        for(int64_t i = blockIdx.x * 256ll + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256)
+        {
+            double zi = (double)x[i];
+            z[i]      = zi;
+            acc += zi * r[i];
+        }
+        if(out)
+            reduce_finish_sum<256>(acc, partial, counter, out);
+    }
+
+    // x += (double) e
+    __global__ void k_add_f2d(const float* __restrict__ e, double* __restrict__ x, int64_t n)
+    {
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+            i += (int64_t)gridDim.x * blockDim.x)
+            x[i] += (double)e[i];
+    }
+
+    // Coarsest 1x1 level: x = b / a (amg.cpp:211-216).
+    template <class T>
+    __global__ void k_coarse1(const double* a, const T* b, T* x, const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        x[0] = (T)__ddiv_rn((double)b[0], a[0]);
+    }
+
+    // x = Ainv b with the FP64 dense inverse (one warp per row, FP64 accumulation).
+    template <class T>
+    __global__ void k_coarse_dense(const double* __restrict__ Ainv, const T* __restrict__ b,
+                                   T* __restrict__ x, int n, const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        int row  = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+        int lane = threadIdx.x & 31;
+        if(row >= n)
+            return;
+        double s = 0.0;
+        for(int k = lane; k < n; k += 32)
+            s = fma(Ainv[(size_t)row * n + k], (double)b[k], s);
+        s = warp_sum(s);
+        if(lane == 0)
+            x[row] = (T)s;
+    }
+
+    // The reference's coarsest solve: `sweeps` lexicographic Gauss-Seidel sweeps
+    // (amg.cpp:238-264, 362-388, 485-511), one thread, same operation order.
+    template <class T>
+    __global__ void k_coarse_gs(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                const double* __restrict__ v, int n, const T* __restrict__ b,
+                                T* __restrict__ x, int sweeps, const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        if(threadIdx.x != 0 || blockIdx.x != 0)
+            return;
+        for(int it = 0; it < sweeps; it++)
+            for(int j = 0; j < n; j++)
+            {
+                double sigma = 0.0, ajj = 0.0;
+                for(int k = rp[j]; k < rp[j + 1]; k++)
+                {
+                    int c = ci[k];
+                    if(c != j)
+                        sigma = __dadd_rn(sigma, __dmul_rn(v[k], (double)x[c]));
+                    else
+                        ajj = v[k];
+                }
+                x[j] = (T)__ddiv_rn(__dsub_rn((double)b[j], sigma), ajj);
+            }
+    }
+
+    // Dense inverse by Gauss-Jordan with partial pivoting, one CTA (n <= 1024).
+    __global__ void __launch_bounds__(1024)
+        k_gauss_jordan(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                       const double* __restrict__ v, int n, double* M, double* I, int* singular)
+    {
+        const int t  = threadIdx.x;
+        const int NT = blockDim.x;
+        for(size_t k = t; k < (size_t)n * n; k += NT)
+        {
+            M[k] = 0.0;
+            I[k] = 0.0;
+        }
+        __syncthreads();
+        for(int i = t; i < n; i += NT)
+        {
+            I[(size_t)i * n + i] = 1.0;
+            for(int j = rp[i]; j < rp[i + 1]; j++)
+                M[(size_t)i * n + ci[j]] += v[j];
+        }
+        __syncthreads();
+        __shared__ int    s_piv;
+        __shared__ double s_pv;
+        for(int c = 0; c < n; c++)
+        {
+            if(t == 0)
+            {
+                int    p  = c;
+                double pv = fabs(M[(size_t)c * n + c]);
+                for(int r = c + 1; r < n; r++)
+                {
+                    double a = fabs(M[(size_t)r * n + c]);
+                    if(a > pv)
+                    {
+                        pv = a;
+                        p  = r;
+                    }
+                }
+                s_piv = p;
+                s_pv  = pv;
+            }
+            __syncthreads();
+            if(s_pv == 0.0)
+            {
+                if(t == 0)
+                    *singular = 1;
+                return;
+            }
+            int p = s_piv;
+            if(p != c)
+                for(int k = t; k < n; k += NT)
+                {
+                    double a             = M[(size_t)c * n + k];
+                    M[(size_t)c * n + k] = M[(size_t)p * n + k];
+                    M[(size_t)p * n + k] = a;
+                    a                    = I[(size_t)c * n + k];
+                    I[(size_t)c * n + k] = I[(size_t)p * n + k];
+                    I[(size_t)p * n + k] = a;
+                }
+            __syncthreads();
+            const double inv = 1.0 / M[(size_t)c * n + c];
+            __syncthreads();
+            for(int k = t; k < n; k += NT)
+            {
+                M[(size_t)c * n + k] *= inv;
+                I[(size_t)c * n + k] *= inv;
+            }
+            __syncthreads();
+            for(size_t q = t; q < (size_t)n * n; q += NT)
+            {
+                int r = (int)(q / n), k = (int)(q % n);
+                if(r == c || k == c)
+                    continue;
+                double f = M[(size_t)r * n + c];
+                M[q] -= f * M[(size_t)c * n + k];
+                I[q] -= f * I[(size_t)c * n + k];
+            }
+            __syncthreads();
+            for(int r = t; r < n; r += NT)
+                if(r != c)
+                {
+                    double f             = M[(size_t)r * n + c];
+                    I[(size_t)r * n + c] -= f * I[(size_t)c * n + c];
+                    M[(size_t)r * n + c] = 0.0;
+                }
+            __syncthreads();
+        }
+    }
+
+    // ---------------------------------------------------------------- multicolour GS
+    __device__ __forceinline__ unsigned int colour_hash(unsigned int x)
+    {
+        x ^= 0x9e3779b9u;
+        x = ((x >> 16) ^ x) * 0x45d9f3bu;
+        x = ((x >> 16) ^ x) * 0x45d9f3bu;
+        return (x >> 16) ^ x;
+    }
+
+    // Jones-Plassmann-Luby: an uncoloured row takes colour c when its (hash, index)
+    // beats every uncoloured neighbour in the symmetrised pattern.
+    __global__ void k_jpl_round(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                int64_t m, int32_t* colour, int c, int* remaining)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m || colour[i] >= 0)
+            return;
+        unsigned hi = colour_hash((unsigned)i);
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+        {
+            int k = ci[j];
+            if(k == i)
+                continue;
+            int ck = colour[k];
+            if(ck >= 0 && ck != c)
+                continue;
+            unsigned hk = colour_hash((unsigned)k);
+            if(hk > hi || (hk == hi && k > i))
+            {
+                atomicAdd(remaining, 1);
+                return;
+            }
+        }
+        colour[i] = c;
+    }
+
+    __global__ void k_colour_count(const int32_t* colour, int64_t m, int32_t* cnt)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i < m)
+            atomicAdd(&cnt[colour[i]], 1);
+    }
+
+    __global__ void k_colour_scatter(const int32_t* colour, int64_t m, int32_t* cursor,
+                                     int32_t* perm)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i < m)
+            perm[atomicAdd(&cursor[colour[i]], 1)] = (int32_t)i;
+    }
+
+    // One colour of a GS / SOR sweep: x_i += omega (b_i - (A x)_i) / a_ii for the
+    // rows of that colour (mutually independent, so updated in place).
+    template <int LANES, class VT, class T>
+    __global__ void k_gs_colour(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                const VT* __restrict__ v, const T* __restrict__ invd,
+                                const int32_t* __restrict__ rows, int nrows,
+                                const T* __restrict__ b, T* x, T omega, const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        int64_t t    = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        int64_t q    = t / LANES;
+        int     lane = (int)(t % LANES);
+        int     i    = q < nrows ? rows[q] : -1;
+        T       s    = T(0);
+        if(i >= 0)
+            for(int j = rp[i] + lane; j < rp[i + 1]; j += LANES)
+                s = acc_step<true>(to_acc(v[j], T(0)), x[ci[j]], s);
+#pragma unroll
+        for(int o = LANES / 2; o > 0; o >>= 1)
+            s += __shfl_xor_sync(0xffffffffu, s, o, LANES);
+        if(i >= 0 && lane == 0)
+            x[i] = x[i] + omega * (invd[i] * (b[i] - s));
+    }
+
+    // ================================================================ precision plumbing
+    __global__ void k_vals_f32(const double* __restrict__ v, int64_t n, float* __restrict__ f)
+    {
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+            i += (int64_t)gridDim.x * blockDim.x)
+            f[i] = (float)v[i];
+    }
+
+    __global__ void k_vals_bf16(const double* __restrict__ v, int64_t n,
+                                __nv_bfloat16* __restrict__ f)
+    {
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+            i += (int64_t)gridDim.x * blockDim.x)
+            f[i] = __double2bfloat16(v[i]);
+    }
+
+    // FP32 (or BF16) value copies of a matrix and its FP32 inverse diagonal.
+    lab_status csr_ensure_lowp(lab_csr_impl* A, int precision, int use_bf16, cudaStream_t s)
+    {
+        if(precision == LAB_PREC_FP64)
+            return LAB_OK;
+        const int64_t nz = std::max<int64_t>(A->nnz, 1);
+        unsigned      g  = grid_for(A->nnz);
+        if(use_bf16 && !A->lp.bf16)
+        {
+            LAB_TRY(dalloc(&A->lp.bf16, (size_t)nz, s));
+            if(A->nnz)
+                LAB_LAUNCH(k_vals_bf16, g, 256, 0, s, (const double*)A->val, A->nnz, A->lp.bf16);
+        }
+        if(!use_bf16 && !A->lp.f32)
+        {
+            LAB_TRY(dalloc(&A->lp.f32, (size_t)nz, s));
+            if(A->nnz)
+                LAB_LAUNCH(k_vals_f32, g, 256, 0, s, (const double*)A->val, A->nnz, A->lp.f32);
+        }
+        if(A->m == A->n && !A->lp.invd32)
+        {
+            LAB_TRY(csr_ensure_invdiag(A, s));
+            LAB_TRY(dalloc(&A->lp.invd32, (size_t)A->m + 1, s));
+            if(A->m)
+                LAB_LAUNCH(k_vals_f32, grid_for(A->m), 256, 0, s, (const double*)A->invdiag, A->m,
+                           A->lp.invd32);
+        }
+        return LAB_OK;
+    }
+
+    unsigned grid_for(int64_t n)
+    {
+        return (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div<int64_t>(n, 256),
+                                                                (int64_t)num_sms() * 8));
+    }
+
+    unsigned red_grid(int64_t n)
+    {
+        return (unsigned)std::max<int64_t>(1, std::min<int64_t>(kRedBlocks, ceil_div<int64_t>(n, 256)));
+    }
+
+    // Per-precision views of a level's vectors and operator data.
+    template <class T>
+    struct lv;
+    template <>
+    struct lv<double>
+    {
+        static double* x(level_ws& w) { return w.x; }
+        static double* b(level_ws& w) { return w.b; }
+        static double* r(level_ws& w) { return w.r; }
+        static double* t(level_ws& w) { return w.t; }
+        static const double* invd(const lab_csr_impl* A) { return A->invdiag; }
+    };
+    template <>
+    struct lv<float>
+    {
+        static float* x(level_ws& w) { return w.xf; }
+        static float* b(level_ws& w) { return w.bf; }
+        static float* r(level_ws& w) { return w.rf; }
+        static float* t(level_ws& w) { return w.tf; }
+        static const float* invd(const lab_csr_impl* A) { return A->lp.invd32; }
+    };
+
+    // BF16 value storage on the two finest levels (LAB_PREC_FP32_BF16).
+    static inline bool level_bf16(const lab_amg_options* o, int l)
+    {
+        return o->precision == LAB_PREC_FP32_BF16 && l < 2;
+    }
+
+    // Call f(values) with the value array the cycle of precision T reads.
+    template <class T, class F>
+    static lab_status with_vals(const lab_csr_impl* M, bool bf16, F&& f)
+    {
+        if constexpr(std::is_same<T, double>::value)
+            return f(static_cast<const double*>(M->val));
+        else
+        {
+            if(bf16)
+                return f(static_cast<const __nv_bfloat16*>(M->lp.bf16));
+            return f(static_cast<const float*>(M->lp.f32));
+        }
+    }
+
+    template <class P>
+    using vt_of = typename std::remove_const<typename std::remove_pointer<P>::type>::type;
+
+    // ================================================================ setup of the cycle
+    static lab_status build_colouring(lab_csr_impl* A, level_ws& w, cudaStream_t s)
+    {
+        if(w.colour)
+            return LAB_OK;
+        const int64_t m = A->m;
+        lab_csr_impl* T = nullptr;
+        LAB_TRY(transpose(A, &T, s));
+        lab_csr_impl* G  = nullptr;
+        lab_status    st = spgeam(1.0, A, 1.0, T, &G, s); // symmetrised pattern A + A^T
+        csr_release(T);
+        LAB_TRY(st);
+        dbuf<int32_t> colour, cnt, cursor;
+        dbuf<int>     rem;
+        st = colour.alloc((size_t)m + 1, s);
+        if(st == LAB_OK)
+            st = rem.alloc(1, s);
+        int ncol = 0;
+        if(st == LAB_OK)
+        {
+            cudaMemsetAsync(colour.get(), 0xff, sizeof(int32_t) * m, s);
+            // every round colours at least the highest-priority uncoloured row
+            for(int64_t c = 0; c <= m; c++)
+            {
+                cudaMemsetAsync(rem.get(), 0, sizeof(int), s);
+                k_jpl_round<<<(unsigned)ceil_div<int64_t>(m, 256), 256, 0, s>>>(
+                    G->row_ptr, G->col_ind, m, colour.get(), (int)c, rem.get());
+                g_launches.fetch_add(1);
+                int h = 0;
+                st    = copy_d2h_sync(&h, rem.get(), sizeof(int), s);
+                if(st != LAB_OK)
+                    break;
+                ncol = (int)c + 1;
+                if(h == 0)
+                    break;
+            }
+        }
+        csr_release(G);
+        LAB_TRY(st);
+        LAB_TRY(cnt.alloc((size_t)ncol + 1, s));
+        LAB_TRY(cursor.alloc((size_t)ncol + 1, s));
+        LAB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int32_t) * (ncol + 1), s));
+        LAB_LAUNCH(k_colour_count, (unsigned)ceil_div<int64_t>(m, 256), 256, 0, s, colour.get(), m,
+                   cnt.get());
+        LAB_TRY(counts_to_rowptr(cnt.get(), cursor.get(), ncol, nullptr, s));
+        w.colour_ptr_h = new int32_t[ncol + 1];
+        LAB_TRY(copy_d2h_sync(w.colour_ptr_h, cursor.get(), sizeof(int32_t) * (ncol + 1), s));
+        LAB_TRY(dalloc(&w.colour, (size_t)m + 1, s));
+        LAB_LAUNCH(k_colour_scatter, (unsigned)ceil_div<int64_t>(m, 256), 256, 0, s, colour.get(),
+                   m, cursor.get(), w.colour);
+        w.ncolours = ncol;
+        return LAB_OK;
+    }
+
+    static lab_status build_coarse(hierarchy_impl* h, int coarse_mode, cudaStream_t s)
+    {
+        lab_csr_impl* A = h->A[h->levels];
+        const int     n = (int)A->m;
+        if(n <= 1 || coarse_mode != LAB_COARSE_DIRECT || h->coarse_inv || h->coarse_singular)
+            return LAB_OK;
+        if(n > 1024)
+        {
+            h->coarse_singular = 2; // too large for the dense path: GS sweeps are used
+            return LAB_OK;
+        }
+        dbuf<double> M;
+        dbuf<int>    sing;
+        LAB_TRY(M.alloc((size_t)n * n, s));
+        LAB_TRY(sing.alloc(1, s));
+        LAB_TRY(dalloc(&h->coarse_inv, (size_t)n * n, s));
+        LAB_CUDA(cudaMemsetAsync(sing.get(), 0, sizeof(int), s));
+        LAB_LAUNCH(k_gauss_jordan, 1, 1024, 0, s, A->row_ptr, A->col_ind, A->val, n, M.get(),
+                   h->coarse_inv, sing.get());
+        int hs = 0;
+        LAB_TRY(copy_d2h_sync(&hs, sing.get(), sizeof(int), s));
+        if(hs)
+        {
+            h->coarse_singular = 1;
+            dfree(h->coarse_inv, s);
+            h->coarse_inv = nullptr;
+        }
+        h->coarse_n = n;
+        return LAB_OK;
+    }
+
+    lab_status cycle_prepare(hierarchy_impl* h, const lab_amg_options* o, cudaStream_t s)
+    {
+        const int  L     = h->levels;
+        const bool lowp  = o->precision != LAB_PREC_FP64;
+        for(int l = 0; l <= L; l++)
+        {
+            lab_csr_impl* A = h->A[l];
+            level_ws&     w = h->ws[l];
+            const size_t  m = (size_t)A->m + 1;
+            LAB_TRY(spmv_analyse(A, s));
+            LAB_TRY(csr_ensure_invdiag(A, s));
+            if(l < L)
+            {
+                LAB_TRY(spmv_analyse(h->P[l], s));
+                LAB_TRY(spmv_analyse(h->R[l], s));
+            }
+            if(!w.x)
+            {
+                LAB_TRY(dalloc(&w.x, m, s));
+                LAB_TRY(dalloc(&w.b, m, s));
+                LAB_TRY(dalloc(&w.r, m, s));
+                LAB_TRY(dalloc(&w.t, m, s));
+            }
+            if(lowp)
+            {
+                const bool bf = level_bf16(o, l);
+                LAB_TRY(csr_ensure_lowp(A, o->precision, bf, s));
+                if(l < L)
+                {
+                    LAB_TRY(csr_ensure_lowp(h->P[l], o->precision, bf, s));
+                    LAB_TRY(csr_ensure_lowp(h->R[l], o->precision, bf, s));
+                }
+                if(!w.xf)
+                {
+                    LAB_TRY(dalloc(&w.xf, m, s));
+                    LAB_TRY(dalloc(&w.bf, m, s));
+                    LAB_TRY(dalloc(&w.rf, m, s));
+                    LAB_TRY(dalloc(&w.tf, m, s));
+                }
+            }
+            if(o->smoother != LAB_SMOOTH_JACOBI && l < L)
+                LAB_TRY(build_colouring(A, w, s));
+        }
+        LAB_TRY(build_coarse(h, o->coarse, s));
+        h->ws_ready = 1;
+        return LAB_OK;
+    }
+
+    // ================================================================ reductions
+    template <int OP>
+    __global__ void __launch_bounds__(256)
+        k_red_dev(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                  double* partial, unsigned int* counter, double* out, const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        double acc = 0.0;
+        for(int64_t i = blockIdx.x * 256ll + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256)
+            acc = OP == 0 ? acc + x[i] * y[i] : nanmax(acc, fabs(x[i]));
+        if(OP == 0)
+            reduce_finish_sum<256>(acc, partial, counter, out);
+        else
+            reduce_finish_max<256>(acc, partial, counter, out);
+    }
+
+    lab_status dot_device(int64_t n, const double* x, const double* y, red_buf r, cudaStream_t s)
+    {
+        LAB_LAUNCH(k_red_dev<0>, red_grid(n), 256, 0, s, n, x, y, r.partial, r.counter, r.out,
+                   r.skip);
+        return LAB_OK;
+    }
+
+    lab_status norm_inf_device(int64_t n, const double* x, red_buf r, cudaStream_t s)
+    {
+        LAB_LAUNCH(k_red_dev<1>, red_grid(n), 256, 0, s, n, x, (const double*)nullptr, r.partial,
+                   r.counter, r.out, r.skip);
+        return LAB_OK;
+    }
+
+    // ================================================================ smoothing
+    // One sweep reading xin; the new iterate is written to xout (Jacobi) or
+    // xin in place (GS family); *result tells which.
+    template <class T>
+    static lab_status smooth(const lab_csr_impl* A, int l, level_ws& w, const T* b, T* xin, T* xout,
+                             T** result, const cyc_ctx& c, red_buf dot = red_buf(),
+                             const T* dv = nullptr)
+    {
+        const lab_amg_options* o = c.o;
+        red_buf                rb;
+        rb.skip       = c.skip;
+        dot.skip      = c.skip;
+        const T* invd = lv<T>::invd(A);
+        const bool bf = level_bf16(o, l);
+        if(o->smoother == LAB_SMOOTH_JACOBI)
+        {
+            *result = xout;
+            return with_vals<T>(A, bf, [&](auto* vals) -> lab_status {
+                using VT = vt_of<decltype(vals)>;
+                if(dv)
+                {
+                    op_jacobi<VT, T, true> op{xin, b, invd, (T)o->omega, xout, dv};
+                    return launch_rowop(A, vals, op, c.s, dot);
+                }
+                op_jacobi<VT, T, false> op{xin, b, invd, (T)o->omega, xout, nullptr};
+                return launch_rowop(A, vals, op, c.s, rb);
+            });
+        }
+        if(!w.colour_ptr_h)
+        {
+            set_error("multicolour smoother without a colouring of level %d", l);
+            return LAB_BAD_ARG;
+        }
+        // GS family.  The reference maps SGS to plain GS (amg.cpp:130-132) and uses
+        // omega 0.5 for SOR / SSOR (amg.cpp:133-137); SSOR sweeps forward then back.
+        const T    omega = (o->smoother == LAB_SMOOTH_SOR || o->smoother == LAB_SMOOTH_SSOR)
+                               ? (T)o->omega_sor
+                               : T(1);
+        const bool sym   = o->smoother == LAB_SMOOTH_SSOR;
+        const int  lanes = A->plan.alg == LAB_SPMV_ROWSEQ ? 1 : std::min(A->plan.lanes, 32);
+        auto pass = [&](int col) -> lab_status {
+            return with_vals<T>(A, bf, [&](auto* vals) -> lab_status {
+                using VT = vt_of<decltype(vals)>;
+                int r0 = w.colour_ptr_h[col], r1 = w.colour_ptr_h[col + 1];
+                int nr = r1 - r0;
+                if(nr == 0)
+                    return LAB_OK;
+                unsigned g = (unsigned)ceil_div<int64_t>((int64_t)nr * lanes, 256);
+#define LAB_GS(LN)                                                                              \
+    LAB_LAUNCH((k_gs_colour<LN, VT, T>), g, 256, 0, c.s, A->row_ptr, A->col_ind, vals, invd,    \
+               (const int32_t*)(w.colour + r0), nr, b, xin, omega, c.skip)
+                switch(lanes)
+                {
+                case 1:
+                    LAB_GS(1);
+                    break;
+                case 2:
+                    LAB_GS(2);
+                    break;
+                case 4:
+                    LAB_GS(4);
+                    break;
+                case 8:
+                    LAB_GS(8);
+                    break;
+                case 16:
+                    LAB_GS(16);
+                    break;
+                default:
+                    LAB_GS(32);
+                    break;
+                }
+#undef LAB_GS
+                return LAB_OK;
+            });
+        };
+        for(int col = 0; col < w.ncolours; col++)
+            LAB_TRY(pass(col));
+        if(sym)
+            for(int col = w.ncolours - 1; col >= 0; col--)
+                LAB_TRY(pass(col));
+        *result = xin;
+        if(dv)
+        {
+            if constexpr(std::is_same<T, double>::value)
+                LAB_TRY(dot_device(A->m, xin, dv, dot, c.s));
+        }
+        return LAB_OK;
+    }
+
+    // ================================================================ coarsest level
+    template <class T>
+    static lab_status coarse_solve(hierarchy_impl* h, const T* b, T* x, bool zero_guess,
+                                   int sweeps, const cyc_ctx& c)
+    {
+        lab_csr_impl* A = h->A[h->levels];
+        const int     n = (int)A->m;
+        if(n == 0)
+            return LAB_OK;
+        if(n == 1)
+        {
+            LAB_LAUNCH(k_coarse1<T>, 1, 1, 0, c.s, (const double*)A->val, b, x, c.skip);
+            return LAB_OK;
+        }
+        if(c.o->coarse == LAB_COARSE_DIRECT && h->coarse_inv)
+        {
+            unsigned g = (unsigned)ceil_div(n, 8);
+            LAB_LAUNCH(k_coarse_dense<T>, g, 256, 0, c.s, (const double*)h->coarse_inv, b, x, n,
+                       c.skip);
+            return LAB_OK;
+        }
+        if(zero_guess)
+            LAB_LAUNCH(k_zero<T>, grid_for(n), 256, 0, c.s, x, (int64_t)n, c.skip);
+        LAB_LAUNCH(k_coarse_gs<T>, 1, 1, 0, c.s, A->row_ptr, A->col_ind, A->val, n, b, x, sweeps,
+                   c.skip);
+        return LAB_OK;
+    }
+
+    // ================================================================ the recursion
+    // cycle(l): x <- cycle(x; b) on level l.  kind 0 = V (amg.cpp:144-267),
+    // 1 = W (269-390), 2 = F (392-513).  zero_guess: x enters as 0 (not read).
+    // With `dv` (level 0 of the FP64 preconditioner) the kernel writing the final
+    // x also accumulates (x, dv) into dot.out.
+    template <class T>
+    static lab_status cycle(hierarchy_impl* h, int l, int kind, T* x, const T* b, bool zero_guess,
+                            const cyc_ctx& c, red_buf dot = red_buf(), const T* dv = nullptr)
+    {
+        const lab_amg_options* o = c.o;
+        red_buf                rb;
+        rb.skip  = c.skip;
+        dot.skip = c.skip;
+        if(l == h->levels)
+        {
+            LAB_TRY(coarse_solve<T>(h, b, x, zero_guess, kind == 0 ? 1000 : 100, c));
+            if constexpr(std::is_same<T, double>::value)
+                if(dv)
+                    LAB_TRY(dot_device(h->A[l]->m, x, dv, dot, c.s));
+            return LAB_OK;
+        }
+        lab_csr_impl* A   = h->A[l];
+        lab_csr_impl* P   = h->P[l];
+        lab_csr_impl* R   = h->R[l];
+        level_ws&     w   = h->ws[l];
+        level_ws&     wc  = h->ws[l + 1];
+        const int64_t m   = A->m;
+        const int     n1  = o->n1, n2 = o->n2;
+        const bool    jac = o->smoother == LAB_SMOOTH_JACOBI;
+        const bool    bf  = level_bf16(o, l);
+        T*            wr  = lv<T>::r(w);
+        T*            cx  = lv<T>::x(wc);
+        T*            cb  = lv<T>::b(wc);
+        const T*      invd = lv<T>::invd(A);
+
+        // Jacobi alternates between x and the level's scratch vector; start in the
+        // buffer that makes the last write land in x (GS sweeps and the correction
+        // work in place).
+        T*        cur    = x;
+        T*        oth    = lv<T>::t(w);
+        const int visits = kind == 0 ? 1 : 2;
+        if(jac)
+        {
+            int flips = (zero_guess && n1 >= 1) ? (n1 - 1) + visits * (1 + n2)
+                                                : n1 + visits * (1 + n2);
+            if(zero_guess && (flips & 1))
+            {
+                cur = lv<T>::t(w);
+                oth = x;
+            }
+        }
+        auto flip = [&](T* res) {
+            if(res != cur)
+            {
+                oth = cur;
+                cur = res;
+            }
+        };
+        auto residual = [&]() -> lab_status {
+            return with_vals<T>(A, bf, [&](auto* vals) -> lab_status {
+                op_res<vt_of<decltype(vals)>, T> op{cur, b, wr};
+                return launch_rowop(A, vals, op, c.s, rb);
+            });
+        };
+
+        // ---- pre-smoothing + residual
+        if(zero_guess && n1 >= 1 && jac)
+        {
+            LAB_TRY(with_vals<T>(A, bf, [&](auto* vals) -> lab_status {
+                op_pre0<vt_of<decltype(vals)>, T> op{b, invd, (T)o->omega, cur, wr};
+                return launch_rowop(A, vals, op, c.s, rb);
+            }));
+            for(int k = 1; k < n1; k++)
+            {
+                T* res = nullptr;
+                LAB_TRY(smooth<T>(A, l, w, b, cur, oth, &res, c));
+                flip(res);
+            }
+            if(n1 > 1)
+                LAB_TRY(residual());
+        }
+        else
+        {
+            if(zero_guess)
+                LAB_LAUNCH(k_zero<T>, grid_for(m), 256, 0, c.s, cur, m, c.skip);
+            for(int k = 0; k < n1; k++)
+            {
+                T* res = nullptr;
+                LAB_TRY(smooth<T>(A, l, w, b, cur, oth, &res, c));
+                flip(res);
+            }
+            LAB_TRY(residual());
+        }
+
+        // ---- restrict, recurse, correct
+        auto coarse_correct = [&](bool cz, int ckind, bool last) -> lab_status {
+            LAB_TRY(with_vals<T>(R, bf, [&](auto* vals) -> lab_status {
+                op_restrict<vt_of<decltype(vals)>, T> op{wr, cb};
+                return launch_rowop(R, vals, op, c.s, rb);
+            }));
+            LAB_TRY(cycle<T>(h, l + 1, ckind, cx, cb, cz, c));
+            const bool fuse = last && dv && n2 == 0 && kind == 0;
+            T*         dst  = jac ? oth : cur;
+            LAB_TRY(with_vals<T>(P, bf, [&](auto* vals) -> lab_status {
+                using VT = vt_of<decltype(vals)>;
+                if(fuse)
+                {
+                    op_prolong<VT, T, true> op{cx, cur, dst, dv};
+                    return launch_rowop(P, vals, op, c.s, dot);
+                }
+                op_prolong<VT, T, false> op{cx, cur, dst, nullptr};
+                return launch_rowop(P, vals, op, c.s, rb);
+            }));
+            flip(dst);
+            return LAB_OK;
+        };
+        auto post = [&](int sweeps, bool last) -> lab_status {
+            for(int k = 0; k < sweeps; k++)
+            {
+                T*   res      = nullptr;
+                bool fuse_dot = last && dv && k == sweeps - 1;
+                LAB_TRY(smooth<T>(A, l, w, b, cur, oth, &res, c, fuse_dot ? dot : red_buf(),
+                                  fuse_dot ? dv : nullptr));
+                flip(res);
+            }
+            return LAB_OK;
+        };
+
+        if(kind == 0)
+        {
+            LAB_TRY(coarse_correct(true, 0, true));
+            LAB_TRY(post(n2, true));
+        }
+        else
+        {
+            // W: second visit recurses with W again; F: with V (amg.cpp:463).
+            // The second coarse solve starts from the first one's result.
+            LAB_TRY(coarse_correct(true, kind, false));
+            LAB_TRY(post(n2, false));
+            LAB_TRY(residual());
+            LAB_TRY(coarse_correct(false, kind == 1 ? 1 : 0, false));
+            LAB_TRY(post(n2, true)); // n3 = n2 (amg.cpp:537)
+            if constexpr(std::is_same<T, double>::value)
+                if(dv && n2 == 0)
+                    LAB_TRY(dot_device(m, cur, dv, dot, c.s));
+        }
+        if(cur != x)
+            LAB_LAUNCH(k_copy<T>, grid_for(m), 256, 0, c.s, x, (const T*)cur, m, c.skip);
+        return LAB_OK;
+    }
+
+    // ================================================================ entry points
+    lab_status cycle_precond(hierarchy_impl* h, const cyc_ctx& c, const double* r, double* z,
+                             red_buf dot)
+    {
+        if(c.o->precision == LAB_PREC_FP64)
+        {
+            if(dot.out)
+                return cycle<double>(h, 0, c.o->cycle, z, r, true, c, dot, r);
+            return cycle<double>(h, 0, c.o->cycle, z, r, true, c);
+        }
+        // Reduced precision: r -> fp32, FP32 cycle, z = fp64(x) with (z, r) fused.
+        level_ws&     w = h->ws[0];
+        const int64_t m = h->A[0]->m;
+        LAB_LAUNCH(k_d2f, grid_for(m), 256, 0, c.s, r, w.bf, m, c.skip);
+        LAB_TRY(cycle<float>(h, 0, c.o->cycle, w.xf, (const float*)w.bf, true, c));
+        LAB_LAUNCH(k_f2d_dot, red_grid(m), 256, 0, c.s, (const float*)w.xf, r, z, m, dot.partial,
+                   dot.counter, dot.out, c.skip);
+        return LAB_OK;
+    }
+
+    lab_status cycle_iterate(hierarchy_impl* h, const cyc_ctx& c, const double* b, double* x)
+    {
+        if(c.o->precision == LAB_PREC_FP64)
+            return cycle<double>(h, 0, c.o->cycle, x, b, false, c);
+        // correction form: x += cycle(0; b - A x) with the FP64 residual
+        level_ws&     w = h->ws[0];
+        lab_csr_impl* A = h->A[0];
+        const int64_t m = A->m;
+        op_residual   opr{x, b, w.r};
+        LAB_TRY(launch_rowop(A, A->val, opr, c.s));
+        LAB_LAUNCH(k_d2f, grid_for(m), 256, 0, c.s, (const double*)w.r, w.bf, m, c.skip);
+        LAB_TRY(cycle<float>(h, 0, c.o->cycle, w.xf, (const float*)w.bf, true, c));
+        LAB_LAUNCH(k_add_f2d, grid_for(m), 256, 0, c.s, (const float*)w.xf, x, m);
+        return LAB_OK;
+    }
+}

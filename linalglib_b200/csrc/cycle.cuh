@@ -1,0 +1,38 @@
+// Multigrid cycles (cycle.cu) as used by the solvers (solve.cu).
+#pragma once
+
+#include "amg.cuh"
+#include "spmv_engine.cuh"
+
+namespace lab
+{
+    struct cyc_ctx
+    {
+        const lab_amg_options* o;
+        cudaStream_t           s;
+        const int*             skip; // early-exit flag (PCG graph), may be null
+    };
+
+    // Allocate every per-level vector, analyse every operator, build the
+    // reduced-precision copies / colourings / coarse inverse the options need.
+    // Synchronises; never called inside a graph capture.
+    lab_status cycle_prepare(hierarchy_impl* h, const lab_amg_options* o, cudaStream_t s);
+
+    // z = cycle(0; r) on level 0 (FP64 interface whatever the cycle precision).
+    // With dot.out set, also (z, r) -> dot.out.  Enqueue only (capturable).
+    lab_status cycle_precond(hierarchy_impl* h, const cyc_ctx& c, const double* r, double* z,
+                             red_buf dot);
+
+    // x <- cycle(x; b) on level 0 (stationary iteration step).  FP64 cycles run in
+    // place; reduced-precision cycles run in correction form x += cycle(0; b - A x).
+    lab_status cycle_iterate(hierarchy_impl* h, const cyc_ctx& c, const double* b, double* x);
+
+    // deterministic device reductions into r.out (grid <= kRedBlocks)
+    lab_status dot_device(int64_t n, const double* x, const double* y, red_buf r, cudaStream_t s);
+    lab_status norm_inf_device(int64_t n, const double* x, red_buf r, cudaStream_t s);
+    unsigned   red_grid(int64_t n);
+    unsigned   grid_for(int64_t n);
+
+    __global__ void k_copy_d(double* __restrict__ y, const double* __restrict__ x, int64_t n,
+                             const int* skip);
+}

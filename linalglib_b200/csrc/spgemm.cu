@@ -289,6 +289,209 @@ namespace lab
         return LAB_OK;
     }
 
+    // ------------------------------------------------------------ hash-accumulator SpGEMM
+    // For rows with many products but few distinct columns (the Galerkin products
+    // R*(A*P) and A*P on coarse levels: up to ~12k products, <= ~300 columns).
+    // One warp per row.  The warp walks the A row in order; for each entry the
+    // lanes take the distinct columns of the matching B row, so no two lanes ever
+    // touch the same table key within a step, and a __syncwarp separates steps:
+    // every column's contributions are added in A-row order, the first one
+    // assigned, exactly as host_csrgemm.cpp:119-139.  Only the distinct columns
+    // are then sorted.
+    constexpr int kHashWarps = 4;
+    constexpr int kHashSym   = 2048; // symbolic table slots per warp (keys only)
+    constexpr int kHashNum   = 1024; // numeric table slots per warp
+    constexpr int kHashNumMaxCnt = kHashNum / 2;
+
+    __device__ __forceinline__ unsigned hash_slot(int c, unsigned mask)
+    {
+        return ((unsigned)c * 2654435761u >> 7) & mask;
+    }
+
+    // mode 0: symbolic (counts[row], or the row goes to the overflow list)
+    template <int MODE>
+    __global__ void __launch_bounds__(32 * kHashWarps)
+        k_hash_gemm(csr_ref A, csr_ref B, const int32_t* __restrict__ rows, int nrows,
+                    int32_t* counts, const int32_t* __restrict__ out_rp, int32_t* out_ci,
+                    double* out_v, int32_t* ovf_rows, int* n_ovf)
+    {
+        extern __shared__ __align__(16) unsigned char hsm[];
+        const int      wid  = threadIdx.x >> 5;
+        const int      lane = threadIdx.x & 31;
+        constexpr int  H    = MODE == 0 ? kHashSym : kHashNum;
+        const size_t   per  = MODE == 0 ? (size_t)H * 4 : (size_t)H * 4 + (size_t)H * 8 + (size_t)(H / 2) * 8;
+        unsigned char* base = hsm + per * wid;
+        int*           skey = reinterpret_cast<int*>(base);
+        double*        sval = reinterpret_cast<double*>(base + (size_t)H * 4);
+        uint64_t*      sk   = reinterpret_cast<uint64_t*>(base + (size_t)H * 12);
+        __shared__ int s_claims[kHashWarps];
+
+        for(int r = blockIdx.x * kHashWarps + wid; r < nrows; r += gridDim.x * kHashWarps)
+        {
+            const int row = rows[r];
+            int       cnt = 0;
+            unsigned  Hr  = H;
+            if(MODE == 1)
+            {
+                cnt = out_rp[row + 1] - out_rp[row];
+                Hr  = (unsigned)max(32, pow2_ceil(2 * cnt));
+            }
+            const unsigned mask = Hr - 1;
+            for(unsigned q = lane; q < Hr; q += 32)
+                skey[q] = -1;
+            if(lane == 0)
+                s_claims[wid] = 0;
+            __syncwarp();
+            bool ovf = false;
+            for(int j = A.rp[row]; j < A.rp[row + 1] && !ovf; j++)
+            {
+                const int    k  = A.ci[j];
+                const double a  = A.v[j];
+                const int    b0 = B.rp[k], b1 = B.rp[k + 1];
+                for(int p = b0 + lane; p < b1; p += 32)
+                {
+                    const int c    = B.ci[p];
+                    unsigned  slot = hash_slot(c, mask);
+                    for(unsigned probe = 0; probe < Hr; probe++)
+                    {
+                        int old = atomicCAS(&skey[slot], -1, c);
+                        if(old == -1)
+                        {
+                            if(MODE == 1)
+                                sval[slot] = __dmul_rn(a, B.v[p]);
+                            else
+                                atomicAdd(&s_claims[wid], 1);
+                            break;
+                        }
+                        if(old == c)
+                        {
+                            if(MODE == 1)
+                                sval[slot] = __dadd_rn(sval[slot], __dmul_rn(a, B.v[p]));
+                            break;
+                        }
+                        slot = (slot + 1) & mask;
+                    }
+                }
+                __syncwarp();
+                if(MODE == 0 && s_claims[wid] > (int)(3 * H / 4))
+                    ovf = true; // too many distinct columns for this table
+                __syncwarp();
+            }
+            if(MODE == 0)
+            {
+                if(lane == 0)
+                {
+                    if(ovf)
+                        ovf_rows[atomicAdd(n_ovf, 1)] = row;
+                    else
+                        counts[row] = s_claims[wid];
+                }
+            }
+            else
+            {
+                // compact the filled slots, sort by column, write
+                int n = 0;
+                for(unsigned q0 = 0; q0 < Hr; q0 += 32)
+                {
+                    unsigned q    = q0 + lane;
+                    bool     full = skey[q] >= 0;
+                    unsigned bal  = __ballot_sync(0xffffffffu, full);
+                    if(full)
+                        sk[n + __popc(bal & ((1u << lane) - 1u))] = make_key(skey[q], (int)q);
+                    n += __popc(bal);
+                }
+                __syncwarp();
+                bitonic_sort<grp_warp>(sk, n);
+                const int32_t o = out_rp[row];
+                for(int i = lane; i < n; i += 32)
+                {
+                    out_ci[o + i] = key_col(sk[i]);
+                    out_v[o + i]  = sval[key_pos(sk[i])];
+                }
+            }
+            __syncwarp();
+        }
+    }
+
+    // Split row ids by item count: rows with ub <= 256 to `small`, others to `big`.
+    __global__ void k_split_rows(const int32_t* __restrict__ upper, int64_t m, int32_t* small,
+                                 int32_t* big, int* cnt)
+    {
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+            i += (int64_t)gridDim.x * blockDim.x)
+        {
+            if(upper[i] <= kEscWarpCap)
+                small[atomicAdd(&cnt[0], 1)] = (int32_t)i;
+            else
+                big[atomicAdd(&cnt[1], 1)] = (int32_t)i;
+        }
+    }
+
+    // Numeric routing of the big rows: exact count <= kHashNumMaxCnt -> hash, else sort.
+    __global__ void k_split_numeric(const int32_t* __restrict__ big, int nbig,
+                                    const int32_t* __restrict__ rp, int32_t* hash_rows,
+                                    int32_t* sort_rows, int* cnt)
+    {
+        for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nbig; i += gridDim.x * blockDim.x)
+        {
+            int row = big[i];
+            if(rp[row + 1] - rp[row] <= kHashNumMaxCnt)
+                hash_rows[atomicAdd(&cnt[0], 1)] = row;
+            else
+                sort_rows[atomicAdd(&cnt[1], 1)] = row;
+        }
+    }
+
+    __global__ void k_gsizes(const int32_t* __restrict__ rows, int n, const int32_t* __restrict__ upper,
+                             int64_t* sizes)
+    {
+        int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i < n)
+            sizes[i] = pow2_ceil(upper[rows[i]]);
+        if(i == n)
+            sizes[n] = 0;
+    }
+
+    // An explicit list of rows processed by the global-memory sort tier.
+    static lab_status tiers_for_rows(const int32_t* rows, int n, const int32_t* upper,
+                                     esc_tiers& t, cudaStream_t s)
+    {
+        t.nw = t.nb = 0;
+        t.ng = n;
+        if(n == 0)
+            return LAB_OK;
+        LAB_TRY(t.rows.alloc((size_t)n, s));
+        LAB_CUDA(cudaMemcpyAsync(t.rows.get(), rows, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+        LAB_TRY(t.g_offsets.alloc((size_t)n + 1, s));
+        LAB_LAUNCH(k_gsizes, (unsigned)ceil_div(n + 1, 256), 256, 0, s, (const int32_t*)t.rows.get(),
+                   n, upper, t.g_offsets.get());
+        LAB_TRY(scan_i64(t.g_offsets.get(), n + 1, s));
+        LAB_TRY(copy_d2h_sync(&t.g_total, t.g_offsets.get() + n, sizeof(int64_t), s));
+        LAB_TRY(t.g_keys.alloc((size_t)t.g_total, s));
+        LAB_TRY(t.g_vals.alloc((size_t)t.g_total, s));
+        return LAB_OK;
+    }
+
+    template <int MODE>
+    static lab_status launch_hash(csr_ref Ar, csr_ref Br, const int32_t* rows, int n,
+                                  int32_t* counts, const int32_t* out_rp, int32_t* out_ci,
+                                  double* out_v, int32_t* ovf_rows, int* n_ovf, cudaStream_t s)
+    {
+        if(n == 0)
+            return LAB_OK;
+        const size_t per  = MODE == 0 ? (size_t)kHashSym * 4
+                                      : (size_t)kHashNum * 12 + (size_t)(kHashNum / 2) * 8;
+        const size_t smem = per * kHashWarps;
+        static const cudaError_t attr = cudaFuncSetAttribute(
+            k_hash_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        LAB_CUDA(attr);
+        unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(n, kHashWarps),
+                                                    (int64_t)num_sms() * 8);
+        LAB_LAUNCH(k_hash_gemm<MODE>, grid, 32 * kHashWarps, smem, s, Ar, Br, rows, n, counts,
+                   out_rp, out_ci, out_v, ovf_rows, n_ovf);
+        return LAB_OK;
+    }
+
     lab_status spgemm(const lab_csr_impl* A, const lab_csr_impl* B, lab_csr_impl** C,
                       cudaStream_t s)
     {
@@ -314,8 +517,97 @@ namespace lab
             set_error("spgemm: a row has more than 2^30 intermediate products");
             return LAB_NOT_SUPPORTED;
         }
-        exp_gemm e{Ar, Br};
-        return esc_build(e, upper.get(), A->m, B->n, C, s);
+        exp_gemm      e{Ar, Br};
+        const int64_t m = A->m;
+        if(m == 0)
+            return esc_build(e, upper.get(), m, B->n, C, s);
+
+        // ---- tiers: <= 256 products: warp sort; more: warp hash; hash overflow: global sort
+        dbuf<int32_t> small, big, counts, ovf_rows, rp;
+        dbuf<int>     cnt;
+        LAB_TRY(small.alloc((size_t)m, s));
+        LAB_TRY(big.alloc((size_t)m, s));
+        LAB_TRY(counts.alloc((size_t)m + 1, s));
+        LAB_TRY(ovf_rows.alloc((size_t)m, s));
+        LAB_TRY(cnt.alloc(8, s));
+        LAB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * 8, s));
+        LAB_CUDA(cudaMemsetAsync(counts.get(), 0, sizeof(int32_t) * (m + 1), s));
+        unsigned g = (unsigned)std::min<int64_t>(ceil_div<int64_t>(m, 256), 4096);
+        LAB_LAUNCH(k_split_rows, g, 256, 0, s, (const int32_t*)upper.get(), m, small.get(),
+                   big.get(), cnt.get());
+        int hc[2];
+        LAB_TRY(copy_d2h_sync(hc, cnt.get(), sizeof(int) * 2, s));
+        const int nsmall = hc[0], nbig = hc[1];
+
+        esc_tiers ts;
+        ts.nw = nsmall;
+        if(nsmall)
+        {
+            LAB_TRY(ts.rows.alloc((size_t)nsmall, s));
+            LAB_CUDA(cudaMemcpyAsync(ts.rows.get(), small.get(), sizeof(int32_t) * nsmall,
+                                     cudaMemcpyDeviceToDevice, s));
+        }
+        LAB_TRY((esc_run<exp_gemm, 0>(e, m, ts, counts.get(), nullptr, nullptr, s)));
+        LAB_TRY(launch_hash<0>(Ar, Br, big.get(), nbig, counts.get(), nullptr, nullptr, nullptr,
+                               ovf_rows.get(), cnt.get() + 2, s));
+        int novf = 0;
+        LAB_TRY(copy_d2h_sync(&novf, cnt.get() + 2, sizeof(int), s));
+        if(novf)
+        {
+            esc_tiers tg;
+            LAB_TRY(tiers_for_rows(ovf_rows.get(), novf, upper.get(), tg, s));
+            LAB_TRY((esc_run<exp_gemm, 0>(e, m, tg, counts.get(), nullptr, nullptr, s)));
+        }
+
+        // ---- row pointer and allocation
+        LAB_TRY(rp.alloc((size_t)m + 1, s));
+        int64_t nnz = 0;
+        LAB_TRY(counts_to_rowptr(counts.get(), rp.get(), m, &nnz, s));
+        lab_csr_impl* out = nullptr;
+        LAB_TRY(csr_alloc(&out, m, B->n, nnz, s));
+        lab_status st = LAB_OK;
+        if(cudaMemcpyAsync(out->row_ptr, rp.get(), sizeof(int32_t) * (m + 1),
+                           cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            st = LAB_CUDA_ERROR;
+
+        // ---- numeric
+        exp_gemm e2 = e;
+        e2.out_rp   = out->row_ptr;
+        if(st == LAB_OK)
+            st = esc_run<exp_gemm, 1>(e2, m, ts, nullptr, out->col_ind, out->val, s);
+        dbuf<int32_t> hrows, srows;
+        if(st == LAB_OK && nbig)
+        {
+            st = hrows.alloc((size_t)nbig, s);
+            if(st == LAB_OK)
+                st = srows.alloc((size_t)nbig, s);
+            if(st == LAB_OK)
+            {
+                cudaMemsetAsync(cnt.get() + 4, 0, sizeof(int) * 2, s);
+                k_split_numeric<<<(unsigned)ceil_div(nbig, 256), 256, 0, s>>>(
+                    big.get(), nbig, out->row_ptr, hrows.get(), srows.get(), cnt.get() + 4);
+                g_launches.fetch_add(1);
+                int hn[2] = {0, 0};
+                st = copy_d2h_sync(hn, cnt.get() + 4, sizeof(int) * 2, s);
+                if(st == LAB_OK)
+                    st = launch_hash<1>(Ar, Br, hrows.get(), hn[0], nullptr, out->row_ptr,
+                                        out->col_ind, out->val, nullptr, nullptr, s);
+                if(st == LAB_OK && hn[1])
+                {
+                    esc_tiers tg;
+                    st = tiers_for_rows(srows.get(), hn[1], upper.get(), tg, s);
+                    if(st == LAB_OK)
+                        st = esc_run<exp_gemm, 1>(e2, m, tg, nullptr, out->col_ind, out->val, s);
+                }
+            }
+        }
+        if(st != LAB_OK)
+        {
+            csr_release(out);
+            return st;
+        }
+        *C = out;
+        return LAB_OK;
     }
 
     lab_status spgeam(double alpha, const lab_csr_impl* A, double beta, const lab_csr_impl* B,

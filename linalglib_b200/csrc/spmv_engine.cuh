@@ -86,7 +86,10 @@ namespace lab
         return ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16 + (size_t)(cap + 8) * 4;
     }
 
-    template <class Op, int NT>
+    // MAXR > 0: every row has at most MAXR entries (from the analysis); the row is
+    // read into registers with all its gathers issued before the fma chain, which
+    // keeps MAXR loads in flight per thread.  The accumulation order is unchanged.
+    template <class Op, int NT, int MAXR>
     __global__ void __launch_bounds__(NT)
         k_rowseq(csr_view<typename Op::val_t> A, Op op, int cap, red_buf red)
     {
@@ -124,7 +127,22 @@ namespace lab
         {
             const int a = A.rp[row], b = A.rp[row + 1];
             AT        s = AT(0);
-            if(staged)
+            if(staged && MAXR > 0)
+            {
+                AT vv[MAXR > 0 ? MAXR : 1], xv[MAXR > 0 ? MAXR : 1];
+#pragma unroll
+                for(int k = 0; k < MAXR; k++)
+                    if(a + k < b)
+                    {
+                        vv[k] = to_acc(sv[a + k - j0v], AT(0));
+                        xv[k] = op.gather(sc[a + k - j0c]);
+                    }
+#pragma unroll
+                for(int k = 0; k < MAXR; k++)
+                    if(a + k < b)
+                        s = acc_step<Op::kFma>(vv[k], xv[k], s);
+            }
+            else if(staged)
             {
                 for(int j = a; j < b; j++)
                     s = acc_step<Op::kFma>(to_acc(sv[j - j0v], AT(0)), op.gather(sc[j - j0c]), s);
@@ -153,6 +171,7 @@ namespace lab
         if(row < A.m)
         {
             const int a = A.rp[row], b = A.rp[row + 1];
+#pragma unroll 4
             for(int j = a + lane; j < b; j += W)
                 s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), op.gather(A.ci[j]), s);
         }
@@ -199,11 +218,24 @@ namespace lab
                 smem = rowseq_smem<VT>(0);
             }
             // Raise the dynamic shared-memory cap once per instantiation.
-            static const cudaError_t attr = cudaFuncSetAttribute(
-                k_rowseq<Op, kRowseqNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            LAB_CUDA(attr);
-            LAB_LAUNCH((k_rowseq<Op, kRowseqNT>), (unsigned)rowop_grid(A), kRowseqNT, smem, s, V,
-                       op, cap, red);
+            static const cudaError_t attr8 = cudaFuncSetAttribute(
+                k_rowseq<Op, kRowseqNT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            static const cudaError_t attr16 = cudaFuncSetAttribute(
+                k_rowseq<Op, kRowseqNT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                200 * 1024);
+            static const cudaError_t attr0 = cudaFuncSetAttribute(
+                k_rowseq<Op, kRowseqNT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            LAB_CUDA(attr8);
+            LAB_CUDA(attr16);
+            LAB_CUDA(attr0);
+            const unsigned grid = (unsigned)rowop_grid(A);
+            if(p.max_row <= 8)
+                LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 8>), grid, kRowseqNT, smem, s, V, op, cap, red);
+            else if(p.max_row <= 16)
+                LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 16>), grid, kRowseqNT, smem, s, V, op, cap,
+                           red);
+            else
+                LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 0>), grid, kRowseqNT, smem, s, V, op, cap, red);
             return LAB_OK;
         }
         unsigned grid = (unsigned)rowop_grid(A);

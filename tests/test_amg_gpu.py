@@ -102,6 +102,13 @@ def test_spgemm_long_rows(gpu, oracle):
     Bm = (rpb, cib.reshape(-1), rng.uniform(-1, 1, 3 * n), 700)
     C = gpu.CsrMatrix.from_arrays(*B[:3], n=n).spgemm(gpu.CsrMatrix.from_arrays(*Bm[:3], n=700))
     assert csr_equal(C.to_numpy(), oracle.spgemm(B, Bm))
+    # many distinct columns per row: the hash table overflows into the sort tier
+    cib2 = np.sort(rng.choice(6000, size=(n, 3)), axis=1)
+    ok2 = np.all(np.diff(cib2, axis=1) > 0, axis=1)
+    cib2[~ok2] = np.array([0, 1, 2])
+    Bm2 = (rpb, cib2.reshape(-1).astype(np.int32), rng.uniform(-1, 1, 3 * n), 6000)
+    C2 = gpu.CsrMatrix.from_arrays(*B[:3], n=n).spgemm(gpu.CsrMatrix.from_arrays(*Bm2[:3], n=6000))
+    assert csr_equal(C2.to_numpy(), oracle.spgemm(B, Bm2))
 
 
 @pytest.mark.parametrize("kind", [L.AMG_SA, L.AMG_UA])

@@ -66,6 +66,13 @@ def test_amg_pcg_matches_oracle(gpu, oracle, name, kind, omega):
     x = x.cpu().numpy()
     Ho = oracle.amg_setup(A, kind=kind)
     xo, ito, relo = Ho.pcg(b, omega=omega, coarse=1, rel_tol=1e-8, abs_tol=0.0, max_iter=500)
+    if ito > 500:
+        # The unweighted Jacobi V-cycle of the reference (omega = 1) does not give a
+        # convergent PCG on the anisotropic 27-point operator; neither does the oracle
+        # nor the reference (501 = max_iter + 1).  Same outcome required here.
+        assert info.converged == 0 and info.status == L.LAB_NOT_CONVERGED
+        assert info.iterations == ito
+        return
     assert info.converged == 1 and info.status == L.LAB_OK
     assert abs(info.iterations - ito) <= 1, (info.iterations, ito)
     # the reference's criterion: ||r||_inf / ||r0||_inf <= rtol with x0 = 0 (r0 = b)
