@@ -333,6 +333,51 @@ LAB_API lab_status lab_gmres_solve(lab_csr A, lab_precond M, int restart, const 
                                    double* x, const lab_iter_control* c, lab_solve_info* info,
                                    lab_stream s);
 
+/* ------------------------------------------------------------------ batching
+ * Many independent systems in one solve (no reference counterpart).
+ *
+ * lab_csr_block_diag stacks nblocks matrices into one block-diagonal matrix
+ * (offsets[k] = first row of block k, host int64[nblocks + 1] written on return).
+ * One AMG setup on it builds every system's hierarchy at once: strength,
+ * aggregation, prolongation and Galerkin products never couple blocks. */
+LAB_API lab_status lab_csr_block_diag(const lab_csr* blocks, int nblocks, lab_csr* out,
+                                      int64_t* offsets, lab_stream s);
+/* Batched PCG: system k owns rows [offsets[k], offsets[k+1]) of A (host
+ * int64[nsys + 1]) and b / x.  Each system has its own alpha, beta, stopping
+ * test (the reference's, per system) and iteration count; a converged system
+ * stops updating (per-system convergence mask) while the others continue.
+ * iterations / converged: host int[nsys] (may be NULL).  info summarises the
+ * batch (iterations = max over systems, converged = all converged). */
+LAB_API lab_status lab_batched_pcg_solve(lab_csr A, lab_precond M, int nsys,
+                                         const int64_t* offsets, const double* b, double* x,
+                                         const lab_iter_control* c, int* iterations,
+                                         int* converged, lab_solve_info* info, lab_stream s);
+/* Block PCG for nrhs right-hand sides of one matrix: B and X are n x nrhs
+ * column-major (leading dimension n).  Every column has its own scalars and
+ * stopping test; the products with A use SpMM (one pass over A per block of 8
+ * columns). */
+LAB_API lab_status lab_multi_rhs_pcg_solve(lab_csr A, lab_precond M, int nrhs, const double* B,
+                                           double* X, const lab_iter_control* c, int* iterations,
+                                           int* converged, lab_solve_info* info, lab_stream s);
+
+/* ------------------------------------------------------------------ adjoint
+ * Differentiation of x = A^{-1} b for a loss L(x) (no reference counterpart:
+ * LinAlgLib has no derivatives).  The forward iterates are not stored; the
+ * adjoint is a second solve.
+ *
+ * lambda = A^{-T} g with g = dL/dx, which is dL/db.  symmetric != 0: A^T = A and
+ * the solve is PCG with M (a symmetric preconditioner: the AMG cycle with equal
+ * pre-/post-smoothing, or Jacobi).  symmetric == 0: A^T is formed and solved
+ * with GMRES(restart 50) preconditioned by M when M was built from A^T, else
+ * unpreconditioned (M = NULL). */
+LAB_API lab_status lab_adjoint_solve(lab_csr A, lab_precond M, int symmetric, const double* g,
+                                     double* lambda, const lab_iter_control* c,
+                                     lab_solve_info* info, lab_stream s);
+/* dL/dA restricted to A's sparsity pattern: grad[j] = -lambda[i] * x[col[j]] for
+ * every stored entry j of row i (grad has A's nnz layout). */
+LAB_API lab_status lab_adjoint_grad_A(lab_csr A, const double* lambda, const double* x,
+                                      double* grad, lab_stream s);
+
 /* Same solve, host buffers: b and x are HOST pointers, copied in and out inside
  * the call (the end-to-end form the C++ API uses for host-resident vectors). */
 LAB_API lab_status lab_pcg_solve_host(lab_csr A, lab_precond M, const double* b_host,

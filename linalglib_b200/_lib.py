@@ -108,6 +108,15 @@ _SIGS = {
     "lab_pcg_solve": [_p, _p, _p, _p, C.POINTER(IterControl), C.POINTER(SolveInfo), _p],
     "lab_pcg_solve_host": [_p, _p, _p, _p, C.POINTER(IterControl), C.POINTER(SolveInfo), _p],
     "lab_gmres_solve": [_p, _p, _i, _p, _p, C.POINTER(IterControl), C.POINTER(SolveInfo), _p],
+    "lab_adjoint_solve": [_p, _p, _i, _p, _p, C.POINTER(IterControl), C.POINTER(SolveInfo), _p],
+    "lab_adjoint_grad_A": [_p, _p, _p, _p, _p],
+    "lab_pmis_aggregate_roots": [_p, _p, _p, _p, C.POINTER(_i), _p],
+    "lab_cfpoints_passes": [_p, _p, _i, _i, _p],
+    "lab_csr_block_diag": [_p, _i, C.POINTER(_p), _p, _p],
+    "lab_batched_pcg_solve": [_p, _p, _i, _p, _p, _p, C.POINTER(IterControl), _p, _p,
+                              C.POINTER(SolveInfo), _p],
+    "lab_multi_rhs_pcg_solve": [_p, _p, _i, _p, _p, C.POINTER(IterControl), _p, _p,
+                                C.POINTER(SolveInfo), _p],
 }
 
 _lib = None

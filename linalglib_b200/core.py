@@ -343,3 +343,61 @@ def gmres(A: CsrMatrix, b, x=None, M: Preconditioner | None = None, restart=30, 
     call("lab_gmres_solve", A.h, M.h if M is not None else None, restart, ptr(b), ptr(x),
          C.byref(control), C.byref(info), stream_handle())
     return x, info
+
+
+def adjoint_solve(A: CsrMatrix, g, M: Preconditioner | None = None, symmetric=True,
+                  control=None, lam=None):
+    """lambda = A^{-T} g (= dL/db for g = dL/dx)."""
+    control = control or iter_control()
+    if lam is None:
+        lam = torch.zeros_like(g)
+    info = SolveInfo()
+    call("lab_adjoint_solve", A.h, M.h if M is not None else None, int(bool(symmetric)), ptr(g),
+         ptr(lam), C.byref(control), C.byref(info), stream_handle())
+    return lam, info
+
+
+def adjoint_grad_A(A: CsrMatrix, lam, x):
+    """dL/dA on A's pattern: grad[j] = -lam[i] * x[col[j]]."""
+    grad = torch.empty(A.nnz, dtype=torch.float64, device="cuda")
+    call("lab_adjoint_grad_A", A.h, ptr(lam), ptr(x), ptr(grad), stream_handle())
+    return grad
+
+
+# ---------------------------------------------------------------- batching
+def block_diag(blocks):
+    """Stack CsrMatrix blocks block-diagonally; returns (matrix, offsets)."""
+    arr = (C.c_void_p * len(blocks))(*[b.h.value for b in blocks])
+    offs = (C.c_int64 * (len(blocks) + 1))()
+    h = C.c_void_p()
+    call("lab_csr_block_diag", arr, len(blocks), C.byref(h), offs, stream_handle())
+    return CsrMatrix(h), np.array(offs[:], dtype=np.int64)
+
+
+def batched_pcg(A: CsrMatrix, offsets, b, M: Preconditioner, x=None, control=None):
+    """Independent systems stacked in A (rows offsets[k]:offsets[k+1])."""
+    control = control or iter_control()
+    if x is None:
+        x = torch.zeros_like(b)
+    nsys = len(offsets) - 1
+    offs = (C.c_int64 * (nsys + 1))(*[int(o) for o in offsets])
+    iters = (C.c_int * nsys)()
+    conv = (C.c_int * nsys)()
+    info = SolveInfo()
+    call("lab_batched_pcg_solve", A.h, M.h, nsys, offs, ptr(b), ptr(x), C.byref(control), iters,
+         conv, C.byref(info), stream_handle())
+    return x, np.array(iters[:]), np.array(conv[:]), info
+
+
+def multi_rhs_pcg(A: CsrMatrix, B, M: Preconditioner, X=None, control=None):
+    """B: (nrhs, n) tensor (row k = right-hand side k, i.e. column-major n x nrhs)."""
+    control = control or iter_control()
+    if X is None:
+        X = torch.zeros_like(B)
+    k = B.shape[0]
+    iters = (C.c_int * k)()
+    conv = (C.c_int * k)()
+    info = SolveInfo()
+    call("lab_multi_rhs_pcg_solve", A.h, M.h, k, ptr(B), ptr(X), C.byref(control), iters, conv,
+         C.byref(info), stream_handle())
+    return X, np.array(iters[:]), np.array(conv[:]), info

@@ -163,6 +163,8 @@ namespace lab
     lab_status csr_ensure_invdiag(lab_csr_impl* A, cudaStream_t s);
     lab_status csr_ensure_lowp(lab_csr_impl* A, int precision, int use_bf16, cudaStream_t s);
     lab_status spmv_analyse(lab_csr_impl* A, cudaStream_t s);
+    lab_status spmm_columns(const lab_csr_impl* A, int k, const double* X, int64_t ldx, double* Y,
+                            int64_t ldy, cudaStream_t s, const int* skip);
 
     // ------------------------------------------------------------ shared device helpers
     lab_status scan_i32(int32_t* x, int64_t n, cudaStream_t s); // in-place exclusive

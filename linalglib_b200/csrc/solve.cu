@@ -53,6 +53,20 @@ namespace lab
         return cycle_precond(M->h, c, r, z, dot);
     }
 
+    // dL/dA_ij = -lambda_i x_j on the pattern of A (thread per row; the row's
+    // entries are contiguous, so the writes and the col_ind reads coalesce).
+    __global__ void k_adjoint_grad(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                   int64_t m, const double* __restrict__ lambda,
+                                   const double* __restrict__ x, double* __restrict__ grad)
+    {
+        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        const double li = -lambda[i];
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+            grad[j] = li * __ldg(x + ci[j]);
+    }
+
     // ================================================================ PCG
     enum
     {
@@ -408,6 +422,90 @@ namespace lab
     // Unpreconditioned CG as the reference runs it (cg.cpp:60-134): with
     // restart_iter = -1, `iter % restart_iter == 0` holds for every iter > 0, so
     // each iteration restarts from the true residual (steepest descent).
+    // Mixed precision: FP64 iterative refinement around PCG with the
+    // reduced-precision cycle.  Each outer step recomputes the true residual
+    // r = b - A x in FP64, applies the reference's stopping test to it, solves
+    // A e = r by PCG (FP64 vectors, scalars and dots; FP32 / BF16 cycle) to a
+    // relative 1e-6 (or just what is still needed), and corrects x += e.  The
+    // restart bounds the drift a reduced-precision preconditioner induces in the
+    // CG recurrences.
+    static lab_status pcg_refine(lab_csr_impl* A, precond_impl* M, const double* b, double* x,
+                                 const lab_iter_control* ctl, lab_solve_info* info,
+                                 cudaStream_t s)
+    {
+        const int64_t m = A->m;
+        dbuf<double>  r, e, sc;
+        dbuf<unsigned int> cnt;
+        LAB_TRY(r.alloc((size_t)m + 1, s));
+        LAB_TRY(e.alloc((size_t)m + 1, s));
+        LAB_TRY(sc.alloc((size_t)kRedBlocks + 4, s));
+        LAB_TRY(cnt.alloc(2, s));
+        LAB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(unsigned int) * 2, s));
+        red_buf rb{sc.get() + 4, cnt.get(), sc.get(), nullptr};
+        cudaEvent_t t0, t1;
+        cudaEventCreate(&t0);
+        cudaEventCreate(&t1);
+        cudaEventRecord(t0, s);
+        double r0 = 0.0, rn = 0.0;
+        int    total = 0, conv = 0;
+        bool   nan   = false;
+        lab_status st = LAB_OK;
+        for(int outer = 0; outer < 50; outer++)
+        {
+            op_residual opr{x, b, r.get()};
+            if((st = launch_rowop(A, A->val, opr, s)) != LAB_OK)
+                break;
+            if((st = norm_inf_device(m, r.get(), rb, s)) != LAB_OK)
+                break;
+            if((st = copy_d2h_sync(&rn, sc.get(), sizeof(double), s)) != LAB_OK)
+                break;
+            if(outer == 0)
+                r0 = rn;
+            nan = std::isnan(rn) || std::isnan(r0);
+            if(nan)
+                break;
+            if(rn <= ctl->abs_tol || rn / r0 <= ctl->rel_tol || rn == 0.0)
+            {
+                conv = 1;
+                break;
+            }
+            if(total > ctl->max_iter)
+                break;
+            lab_iter_control inner = *ctl;
+            inner.abs_tol          = 0.0;
+            inner.rel_tol          = std::max(1e-6, 0.5 * ctl->rel_tol * r0 / rn);
+            inner.max_iter         = ctl->max_iter - total;
+            lab_solve_info ii{};
+            cudaMemsetAsync(e.get(), 0, sizeof(double) * m, s);
+            st = pcg_solve(A, M, r.get(), e.get(), &inner, &ii, s);
+            if(st != LAB_OK && st != LAB_NOT_CONVERGED)
+                break;
+            st = LAB_OK;
+            total += ii.iterations + (ii.converged ? 0 : 1);
+            if((st = lab_axpy(m, 1.0, e.get(), x, s)) != LAB_OK)
+                break;
+        }
+        cudaEventRecord(t1, s);
+        cudaEventSynchronize(t1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        if(st != LAB_OK)
+            return st;
+        lab_status status = conv ? LAB_OK : (nan ? LAB_NAN : LAB_NOT_CONVERGED);
+        if(info)
+        {
+            info->iterations       = total;
+            info->converged        = conv;
+            info->initial_residual = r0;
+            info->final_residual   = rn;
+            info->solve_ms         = ms;
+            info->status           = status;
+        }
+        return status;
+    }
+
     static lab_status cg_plain(lab_csr_impl* A, const double* b, double* x,
                                const lab_iter_control* ctl, lab_solve_info* info, cudaStream_t s)
     {
@@ -802,6 +900,440 @@ namespace lab
     }
 }
 
+namespace lab
+{
+    // ================================================================ segmented PCG
+    // Batched systems and multi-RHS solves share one machinery: the vectors are
+    // split into `nseg` segments (a system's rows, or one right-hand side), each
+    // with its own scalars and stopping test.  Every segmented kernel runs on a
+    // (K, nseg) grid: K CTAs per segment, each over a fixed contiguous chunk, the
+    // last CTA of a segment (per-segment ticket) reducing the K partials in order
+    // -- deterministic, and a converged segment is skipped (convergence mask).
+    constexpr int kSegK = 8;
+    enum
+    {
+        G_GAMMA = 0,
+        G_PQ    = 1,
+        G_RN    = 2,
+        G_R0    = 3,
+        G_GNEW  = 4,
+        G_N     = 8
+    };
+    enum
+    {
+        GF_DONE   = 0,
+        GF_ITER   = 1,
+        GF_CONV   = 2,
+        GF_STATUS = 3,
+        GF_N      = 4
+    };
+    // global flags: [0] = all done, [1] = active segments, [2] = max_iter
+    struct seg_ws
+    {
+        int           nseg   = 0;
+        int64_t       total  = 0;
+        int64_t*      off    = nullptr; // device [nseg + 1]
+        double *      r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
+        double*       sc      = nullptr; // [nseg][G_N]
+        int*          sf      = nullptr; // [nseg][GF_N]
+        int*          gflags  = nullptr; // [4]
+        double*       partial = nullptr; // [4 slots][nseg][kSegK]
+        unsigned int* tickets = nullptr; // [4 slots][nseg]
+        double        rtol = 0, atol = 0;
+        void release()
+        {
+            void* ps[] = {off, r, z, p, q, sc, sf, gflags, partial, tickets};
+            for(void* x : ps)
+                if(x)
+                    cudaFree(x);
+        }
+    };
+
+    __device__ __forceinline__ void seg_range(const int64_t* off, int s, int k, int64_t& a,
+                                              int64_t& b)
+    {
+        const int64_t s0 = off[s], s1 = off[s + 1];
+        const int64_t ch = (s1 - s0 + kSegK - 1) / kSegK;
+        a                = s0 + k * ch;
+        b                = min(s1, a + ch);
+    }
+
+    // Per-segment ticket: true in every thread of the segment's last CTA.
+    __device__ __forceinline__ bool seg_ticket(unsigned int* t)
+    {
+        __shared__ bool last;
+        __syncthreads();
+        if(threadIdx.x == 0)
+        {
+            __threadfence();
+            last = atomicAdd(t, 1u) == kSegK - 1;
+        }
+        __syncthreads();
+        return last;
+    }
+
+    // (x, y) per segment -> sc[s][slot]; OP 1: max |x|
+    template <int OP>
+    __global__ void __launch_bounds__(256)
+        k_seg_reduce(const int64_t* off, const double* __restrict__ x, const double* __restrict__ y,
+                     double* sc, int slot, const int* sf, const int* gflags, double* partial,
+                     unsigned int* tickets, int skip_done)
+    {
+        const int s = blockIdx.y, k = blockIdx.x, nseg = gridDim.y;
+        if(gflags[0] || (skip_done && sf[s * GF_N + GF_DONE]))
+            return;
+        int64_t a, b;
+        seg_range(off, s, k, a, b);
+        double acc = 0.0;
+        for(int64_t i = a + threadIdx.x; i < b; i += 256)
+            acc = OP == 0 ? acc + x[i] * y[i] : nanmax(acc, fabs(x[i]));
+        double bs = OP == 0 ? block_sum<256>(acc) : block_max<256>(acc);
+        if(threadIdx.x == 0)
+            partial[(size_t)s * kSegK + k] = bs;
+        (void)nseg;
+        if(seg_ticket(&tickets[s]))
+        {
+            if(threadIdx.x == 0)
+            {
+                double t = 0.0;
+                for(int j = 0; j < kSegK; j++)
+                {
+                    double v = __ldcg(partial + (size_t)s * kSegK + j);
+                    t        = OP == 0 ? t + v : nanmax(t, v);
+                }
+                sc[s * G_N + slot] = t;
+                tickets[s]         = 0;
+            }
+        }
+    }
+
+    __device__ __forceinline__ void seg_retire(int* sf, int s, int* gflags, int status, int conv)
+    {
+        sf[s * GF_N + GF_DONE]   = 1;
+        sf[s * GF_N + GF_CONV]   = conv;
+        sf[s * GF_N + GF_STATUS] = status;
+        if(atomicSub(&gflags[1], 1) == 1)
+            gflags[0] = 1;
+    }
+
+    // x += alpha p; r -= alpha q; ||r||_inf; stopping test, per segment.
+    __global__ void __launch_bounds__(256)
+        k_seg_update(const int64_t* off, double* __restrict__ x, double* __restrict__ r,
+                     const double* __restrict__ p, const double* __restrict__ q, double* sc,
+                     int* sf, int* gflags, double* partial, unsigned int* tickets, double rtol,
+                     double atol)
+    {
+        const int s = blockIdx.y, k = blockIdx.x;
+        if(gflags[0] || sf[s * GF_N + GF_DONE])
+            return;
+        const double alpha = sc[s * G_N + G_GAMMA] / sc[s * G_N + G_PQ];
+        const double na    = -1.0 * alpha;
+        int64_t      a, b;
+        seg_range(off, s, k, a, b);
+        double acc = 0.0;
+        for(int64_t i = a + threadIdx.x; i < b; i += 256)
+        {
+            x[i]      = alpha == 1.0 ? __dadd_rn(p[i], x[i]) : __dadd_rn(__dmul_rn(alpha, p[i]), x[i]);
+            double ri = na == 1.0 ? __dadd_rn(q[i], r[i]) : __dadd_rn(__dmul_rn(na, q[i]), r[i]);
+            r[i]      = ri;
+            acc       = nanmax(acc, fabs(ri));
+        }
+        double bs = block_max<256>(acc);
+        if(threadIdx.x == 0)
+            partial[(size_t)s * kSegK + k] = bs;
+        if(seg_ticket(&tickets[s]))
+        {
+            if(threadIdx.x == 0)
+            {
+                double t = 0.0;
+                for(int j = 0; j < kSegK; j++)
+                    t = nanmax(t, __ldcg(partial + (size_t)s * kSegK + j));
+                tickets[s]          = 0;
+                sc[s * G_N + G_RN]  = t;
+                double r0           = sc[s * G_N + G_R0];
+                bool   nan          = isnan(t) || isnan(r0);
+                if(!nan && (t <= atol || t / r0 <= rtol))
+                    seg_retire(sf, s, gflags, LAB_OK, 1);
+                else if(nan)
+                    seg_retire(sf, s, gflags, LAB_NAN, 0);
+            }
+        }
+    }
+
+    // p = z + beta p, gamma <- gnew, iteration count, max_iter test, per segment.
+    __global__ void __launch_bounds__(256)
+        k_seg_pupdate(const int64_t* off, double* __restrict__ p, const double* __restrict__ z,
+                      double* sc, int* sf, int* gflags, unsigned int* tickets)
+    {
+        const int s = blockIdx.y, k = blockIdx.x;
+        if(gflags[0] || sf[s * GF_N + GF_DONE])
+            return;
+        const double beta = sc[s * G_N + G_GNEW] / sc[s * G_N + G_GAMMA];
+        int64_t      a, b;
+        seg_range(off, s, k, a, b);
+        for(int64_t i = a + threadIdx.x; i < b; i += 256)
+            p[i] = beta == 0.0 ? z[i] : __dadd_rn(z[i], __dmul_rn(beta, p[i]));
+        if(seg_ticket(&tickets[s]))
+        {
+            if(threadIdx.x == 0)
+            {
+                tickets[s]            = 0;
+                sc[s * G_N + G_GAMMA] = sc[s * G_N + G_GNEW];
+                int it                = sf[s * GF_N + GF_ITER] + 1;
+                sf[s * GF_N + GF_ITER] = it;
+                if(it > gflags[2])
+                    seg_retire(sf, s, gflags, LAB_NOT_CONVERGED, 0);
+            }
+        }
+    }
+
+    __global__ void k_seg_init(double* sc, int* sf, int* gflags, int nseg, int max_iter)
+    {
+        int active = 0;
+        for(int s = 0; s < nseg; s++)
+        {
+            sc[s * G_N + G_GAMMA]    = sc[s * G_N + G_GNEW];
+            sc[s * G_N + G_RN]       = sc[s * G_N + G_R0];
+            sf[s * GF_N + GF_ITER]   = 0;
+            bool zero                = sc[s * G_N + G_R0] == 0.0;
+            sf[s * GF_N + GF_DONE]   = zero;
+            sf[s * GF_N + GF_CONV]   = zero;
+            sf[s * GF_N + GF_STATUS] = zero ? LAB_OK : LAB_NOT_CONVERGED;
+            active += !zero;
+        }
+        gflags[1] = active;
+        gflags[2] = max_iter;
+        gflags[0] = active == 0;
+    }
+
+    // Operator products for the two segmentations.
+    struct seg_ops
+    {
+        lab_csr_impl* A     = nullptr;
+        precond_impl* M     = nullptr;
+        int           multi = 0; // 0: stacked systems, 1: nseg columns of one matrix
+        int64_t       n     = 0; // rows of A (multi-RHS column length)
+    };
+
+    static lab_status seg_apply_A(const seg_ops& o, seg_ws& w, const double* in, double* out,
+                                  cudaStream_t s, const int* skip)
+    {
+        if(!o.multi)
+        {
+            op_spmv op{in, out, 1.0, 0.0};
+            red_buf rb;
+            rb.skip = skip;
+            return launch_rowop(o.A, o.A->val, op, s, rb);
+        }
+        lab_csr_impl* A = o.A;
+        for(int c = 0; c < w.nseg; c += 8)
+        {
+            int k = std::min(8, w.nseg - c);
+            LAB_TRY(spmm_columns(A, k, in + (int64_t)c * o.n, o.n, out + (int64_t)c * o.n, o.n,
+                                 s, skip));
+        }
+        return LAB_OK;
+    }
+
+    static lab_status seg_apply_M(const seg_ops& o, seg_ws& w, const double* r, double* z,
+                                  cudaStream_t s, const int* skip)
+    {
+        if(!o.multi)
+            return precond_apply(o.M, r, z, s, skip, red_buf());
+        for(int c = 0; c < w.nseg; c++)
+            LAB_TRY(precond_apply(o.M, r + (int64_t)c * o.n, z + (int64_t)c * o.n, s, skip,
+                                  red_buf()));
+        return LAB_OK;
+    }
+
+    static lab_status seg_solve(const seg_ops& o, int nseg, const int64_t* offsets_h,
+                                const double* b, double* x, const lab_iter_control* ctl,
+                                int* iters_h, int* conv_h, lab_solve_info* info, cudaStream_t s)
+    {
+        seg_ws w;
+        w.nseg  = nseg;
+        w.total = offsets_h[nseg];
+        lab_status st = LAB_OK;
+        auto       al = [&](auto** p, size_t n) {
+            if(st == LAB_OK)
+                st = dalloc(p, n, s);
+        };
+        al(&w.off, (size_t)nseg + 1);
+        al(&w.r, (size_t)w.total + 1);
+        al(&w.z, (size_t)w.total + 1);
+        al(&w.p, (size_t)w.total + 1);
+        al(&w.q, (size_t)w.total + 1);
+        al(&w.sc, (size_t)nseg * G_N);
+        al(&w.sf, (size_t)nseg * GF_N);
+        al(&w.gflags, 4);
+        al(&w.partial, (size_t)4 * nseg * kSegK);
+        al(&w.tickets, (size_t)4 * nseg);
+        if(st != LAB_OK)
+        {
+            w.release();
+            return st;
+        }
+        cudaMemcpyAsync(w.off, offsets_h, sizeof(int64_t) * (nseg + 1), cudaMemcpyHostToDevice, s);
+        cudaMemsetAsync(w.tickets, 0, sizeof(unsigned int) * 4 * nseg, s);
+        cudaMemsetAsync(w.gflags, 0, sizeof(int) * 4, s);
+        cudaMemsetAsync(w.sf, 0, sizeof(int) * nseg * GF_N, s);
+        const dim3 grid(kSegK, nseg);
+        const int* skip = w.gflags;
+        auto       red  = [&](int slotbuf) { return w.partial + (size_t)slotbuf * nseg * kSegK; };
+        auto       tik  = [&](int slotbuf) { return w.tickets + (size_t)slotbuf * nseg; };
+
+        cudaEvent_t t0, t1;
+        cudaEventCreate(&t0);
+        cudaEventCreate(&t1);
+        cudaEventRecord(t0, s);
+        cudaGraphExec_t gexec = nullptr;
+        cudaStream_t    cap   = nullptr;
+        int*            hf    = nullptr;
+        cudaEvent_t     ev[2] = {nullptr, nullptr};
+        do
+        {
+            // r = b - A x, r0 = ||r||, z = M r, gamma = (z, r), p = z
+            if(!o.multi)
+            {
+                op_residual opr{x, b, w.r};
+                st = launch_rowop(o.A, o.A->val, opr, s);
+            }
+            else
+            {
+                st = seg_apply_A(o, w, x, w.q, s, nullptr);
+                if(st == LAB_OK)
+                {
+                    cudaMemcpyAsync(w.r, b, sizeof(double) * w.total, cudaMemcpyDeviceToDevice, s);
+                    st = lab_axpy(w.total, -1.0, w.q, w.r, s); // r = b - A x
+                }
+            }
+            if(st != LAB_OK)
+                break;
+            k_seg_reduce<1><<<grid, 256, 0, s>>>(w.off, w.r, nullptr, w.sc, G_R0, w.sf, w.gflags,
+                                                 red(0), tik(0), 0);
+            st = seg_apply_M(o, w, w.r, w.z, s, nullptr);
+            if(st != LAB_OK)
+                break;
+            k_seg_reduce<0><<<grid, 256, 0, s>>>(w.off, w.z, w.r, w.sc, G_GNEW, w.sf, w.gflags,
+                                                 red(1), tik(1), 0);
+            cudaMemcpyAsync(w.p, w.z, sizeof(double) * w.total, cudaMemcpyDeviceToDevice, s);
+            k_seg_init<<<1, 1, 0, s>>>(w.sc, w.sf, w.gflags, nseg, ctl->max_iter);
+            g_launches.fetch_add(4);
+
+            // one iteration as a graph (captured on a private stream)
+            if(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
+            {
+                st = LAB_CUDA_ERROR;
+                break;
+            }
+            cudaGraph_t g = nullptr;
+            if(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            {
+                st = LAB_CUDA_ERROR;
+                break;
+            }
+            st = seg_apply_A(o, w, w.p, w.q, cap, skip);
+            k_seg_reduce<0><<<grid, 256, 0, cap>>>(w.off, w.p, w.q, w.sc, G_PQ, w.sf, w.gflags,
+                                                   red(2), tik(2), 1);
+            k_seg_update<<<grid, 256, 0, cap>>>(w.off, x, w.r, w.p, w.q, w.sc, w.sf, w.gflags,
+                                                red(3), tik(3), ctl->rel_tol, ctl->abs_tol);
+            if(st == LAB_OK)
+                st = seg_apply_M(o, w, w.r, w.z, cap, skip);
+            k_seg_reduce<0><<<grid, 256, 0, cap>>>(w.off, w.z, w.r, w.sc, G_GNEW, w.sf, w.gflags,
+                                                   red(1), tik(1), 1);
+            k_seg_pupdate<<<grid, 256, 0, cap>>>(w.off, w.p, w.z, w.sc, w.sf, w.gflags, tik(0));
+            cudaError_t ce = cudaStreamEndCapture(cap, &g);
+            if(st != LAB_OK || ce != cudaSuccess)
+            {
+                if(g)
+                    cudaGraphDestroy(g);
+                if(st == LAB_OK)
+                    st = cuda_status(ce, "batched PCG capture", __FILE__, __LINE__);
+                break;
+            }
+            size_t nodes = 0;
+            cudaGraphGetNodes(g, nullptr, &nodes);
+            ce = cudaGraphInstantiate(&gexec, g, 0);
+            cudaGraphDestroy(g);
+            if(ce != cudaSuccess)
+            {
+                st = cuda_status(ce, "batched PCG instantiate", __FILE__, __LINE__);
+                break;
+            }
+            g_launches.fetch_sub(4); // capture-time launches of the 4 segmented kernels
+            if(cudaMallocHost(&hf, sizeof(int) * 8) != cudaSuccess)
+            {
+                st = LAB_OOM;
+                break;
+            }
+            cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+            cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+            for(int it = 0; it <= ctl->max_iter; it++)
+            {
+                if(cudaGraphLaunch(gexec, s) != cudaSuccess)
+                {
+                    st = LAB_CUDA_ERROR;
+                    break;
+                }
+                g_launches.fetch_add((int64_t)nodes);
+                int slot = it & 1;
+                cudaMemcpyAsync(hf + slot * 4, w.gflags, sizeof(int) * 4, cudaMemcpyDeviceToHost,
+                                s);
+                cudaEventRecord(ev[slot], s);
+                if(it >= 1)
+                {
+                    cudaEventSynchronize(ev[(it - 1) & 1]);
+                    if(hf[((it - 1) & 1) * 4])
+                        break;
+                }
+            }
+        } while(0);
+        cudaEventRecord(t1, s);
+        cudaStreamSynchronize(s);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        std::vector<int> sf((size_t)nseg * GF_N);
+        if(st == LAB_OK)
+            st = copy_d2h_sync(sf.data(), w.sf, sizeof(int) * sf.size(), s);
+        if(gexec)
+            cudaGraphExecDestroy(gexec);
+        if(cap)
+            cudaStreamDestroy(cap);
+        if(hf)
+            cudaFreeHost(hf);
+        for(auto& e : ev)
+            if(e)
+                cudaEventDestroy(e);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        w.release();
+        if(st != LAB_OK)
+            return st;
+        int maxit = 0, allconv = 1, nan = 0;
+        for(int k = 0; k < nseg; k++)
+        {
+            if(iters_h)
+                iters_h[k] = sf[k * GF_N + GF_ITER];
+            if(conv_h)
+                conv_h[k] = sf[k * GF_N + GF_CONV];
+            maxit = std::max(maxit, sf[k * GF_N + GF_ITER]);
+            allconv &= sf[k * GF_N + GF_CONV];
+            nan |= sf[k * GF_N + GF_STATUS] == LAB_NAN;
+        }
+        lab_status status = allconv ? LAB_OK : (nan ? LAB_NAN : LAB_NOT_CONVERGED);
+        if(info)
+        {
+            info->iterations       = maxit;
+            info->converged        = allconv;
+            info->initial_residual = 0.0;
+            info->final_residual   = 0.0;
+            info->solve_ms         = ms;
+            info->status           = status;
+        }
+        return status;
+    }
+}
+
 using namespace lab;
 
 struct lab_precond_s : precond_impl
@@ -935,6 +1467,8 @@ LAB_API lab_status lab_pcg_solve(lab_csr A, lab_precond M, const double* b, doub
     LAB_TRY(ensure_init());
     if(!M)
         return cg_plain(A, b, x, c, info, to_stream(s));
+    if(M->kind == 0 && M->o.precision != LAB_PREC_FP64)
+        return pcg_refine(A, M, b, x, c, info, to_stream(s));
     return pcg_solve(A, M, b, x, c, info, to_stream(s));
 }
 
@@ -949,8 +1483,10 @@ LAB_API lab_status lab_pcg_solve_host(lab_csr A, lab_precond M, const double* bh
     LAB_TRY(x.alloc((size_t)A->m + 1, s));
     LAB_CUDA(cudaMemcpyAsync(b.get(), bh, sizeof(double) * A->m, cudaMemcpyHostToDevice, s));
     LAB_CUDA(cudaMemcpyAsync(x.get(), xh, sizeof(double) * A->m, cudaMemcpyHostToDevice, s));
-    lab_status st = M ? pcg_solve(A, M, b.get(), x.get(), c, info, s)
-                      : cg_plain(A, b.get(), x.get(), c, info, s);
+    lab_status st = !M ? cg_plain(A, b.get(), x.get(), c, info, s)
+                       : (M->kind == 0 && M->o.precision != LAB_PREC_FP64)
+                             ? pcg_refine(A, M, b.get(), x.get(), c, info, s)
+                             : pcg_solve(A, M, b.get(), x.get(), c, info, s);
     if(st != LAB_OK && st != LAB_NOT_CONVERGED && st != LAB_NAN)
         return st;
     LAB_CUDA(cudaMemcpyAsync(xh, x.get(), sizeof(double) * A->m, cudaMemcpyDeviceToHost, s));
@@ -967,6 +1503,145 @@ LAB_API lab_status lab_gmres_solve(lab_csr A, lab_precond M, int restart, const 
     LAB_ARG(restart >= 1, "restart must be >= 1");
     LAB_TRY(ensure_init());
     return gmres_solve(A, M, restart, b, x, c, info, to_stream(s));
+}
+
+__global__ void k_block_copy(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                             const double* __restrict__ v, int64_t m, int64_t nnz, int32_t row_off,
+                             int32_t col_off, int32_t nz_off, int32_t* orp, int32_t* oci,
+                             double* ov)
+{
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz + m;
+        i += (int64_t)gridDim.x * blockDim.x)
+    {
+        if(i < nnz)
+        {
+            oci[nz_off + i] = ci[i] + col_off;
+            ov[nz_off + i]  = v[i];
+        }
+        else
+        {
+            int64_t r        = i - nnz;
+            orp[row_off + r] = rp[r] + nz_off;
+        }
+    }
+}
+
+LAB_API lab_status lab_csr_block_diag(const lab_csr* blocks, int nblocks, lab_csr* out,
+                                      int64_t* offsets, lab_stream ls)
+{
+    LAB_ARG(blocks && out && offsets && nblocks > 0, "null argument");
+    LAB_TRY(ensure_init());
+    cudaStream_t s = to_stream(ls);
+    int64_t      m = 0, n = 0, nnz = 0;
+    for(int k = 0; k < nblocks; k++)
+    {
+        LAB_ARG(blocks[k], "null block");
+        offsets[k] = m;
+        m += blocks[k]->m;
+        n += blocks[k]->n;
+        nnz += blocks[k]->nnz;
+    }
+    offsets[nblocks] = m;
+    LAB_ARG(m < INT32_MAX && nnz < INT32_MAX, "stacked matrix exceeds int32 indices");
+    lab_csr_impl* C = nullptr;
+    LAB_TRY(csr_alloc(&C, m, n, nnz, s));
+    int64_t r0 = 0, c0 = 0, z0 = 0;
+    for(int k = 0; k < nblocks; k++)
+    {
+        const lab_csr_impl* B = blocks[k];
+        unsigned            g = grid_for(B->m + B->nnz);
+        k_block_copy<<<g, 256, 0, s>>>(B->row_ptr, B->col_ind, B->val, B->m, B->nnz, (int32_t)r0,
+                                       (int32_t)c0, (int32_t)z0, C->row_ptr, C->col_ind, C->val);
+        g_launches.fetch_add(1);
+        r0 += B->m;
+        c0 += B->n;
+        z0 += B->nnz;
+    }
+    int32_t last = (int32_t)nnz;
+    cudaMemcpyAsync(C->row_ptr + m, &last, sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if(e != cudaSuccess)
+    {
+        csr_release(C);
+        return cuda_status(e, "lab_csr_block_diag", __FILE__, __LINE__);
+    }
+    *out = static_cast<lab_csr>(C);
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_batched_pcg_solve(lab_csr A, lab_precond M, int nsys,
+                                         const int64_t* offsets, const double* b, double* x,
+                                         const lab_iter_control* c, int* iterations,
+                                         int* converged, lab_solve_info* info, lab_stream ls)
+{
+    LAB_ARG(A && M && offsets && b && x && c && nsys > 0, "null argument");
+    LAB_ARG(offsets[0] == 0 && offsets[nsys] == A->m, "offsets must cover the rows of A");
+    for(int k = 0; k < nsys; k++)
+        LAB_ARG(offsets[k + 1] >= offsets[k], "offsets must be non-decreasing");
+    LAB_TRY(ensure_init());
+    cudaStream_t s = to_stream(ls);
+    LAB_TRY(spmv_analyse(A, s));
+    if(M->kind == 0)
+        LAB_TRY(cycle_prepare(M->h, &M->o, s));
+    seg_ops o;
+    o.A = A;
+    o.M = M;
+    return seg_solve(o, nsys, offsets, b, x, c, iterations, converged, info, s);
+}
+
+LAB_API lab_status lab_multi_rhs_pcg_solve(lab_csr A, lab_precond M, int nrhs, const double* B,
+                                           double* X, const lab_iter_control* c, int* iterations,
+                                           int* converged, lab_solve_info* info, lab_stream ls)
+{
+    LAB_ARG(A && M && B && X && c && nrhs > 0, "null argument");
+    LAB_ARG(A->m == A->n, "square matrix required");
+    LAB_TRY(ensure_init());
+    cudaStream_t s = to_stream(ls);
+    LAB_TRY(spmv_analyse(A, s));
+    if(M->kind == 0)
+        LAB_TRY(cycle_prepare(M->h, &M->o, s));
+    std::vector<int64_t> off((size_t)nrhs + 1);
+    for(int k = 0; k <= nrhs; k++)
+        off[k] = (int64_t)k * A->m;
+    seg_ops o;
+    o.A     = A;
+    o.M     = M;
+    o.multi = 1;
+    o.n     = A->m;
+    return seg_solve(o, nrhs, off.data(), B, X, c, iterations, converged, info, s);
+}
+
+LAB_API lab_status lab_adjoint_solve(lab_csr A, lab_precond M, int symmetric, const double* g,
+                                     double* lambda, const lab_iter_control* c,
+                                     lab_solve_info* info, lab_stream ls)
+{
+    LAB_ARG(A && g && lambda && c, "null argument");
+    LAB_ARG(A->m == A->n, "adjoint needs a square matrix");
+    LAB_TRY(ensure_init());
+    cudaStream_t s = to_stream(ls);
+    if(symmetric)
+    {
+        if(!M)
+            return cg_plain(A, g, lambda, c, info, s);
+        return pcg_solve(A, M, g, lambda, c, info, s);
+    }
+    lab_csr_impl* T = nullptr;
+    LAB_TRY(transpose(A, &T, s));
+    lab_status st = gmres_solve(T, M, 50, g, lambda, c, info, s);
+    csr_release(T);
+    return st;
+}
+
+LAB_API lab_status lab_adjoint_grad_A(lab_csr A, const double* lambda, const double* x,
+                                      double* grad, lab_stream s)
+{
+    LAB_ARG(A && lambda && x && (grad || A->nnz == 0), "null argument");
+    LAB_TRY(ensure_init());
+    if(A->m == 0)
+        return LAB_OK;
+    LAB_LAUNCH(k_adjoint_grad, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, to_stream(s),
+               (const int32_t*)A->row_ptr, (const int32_t*)A->col_ind, A->m, lambda, x, grad);
+    return LAB_OK;
 }
 
 } // extern "C"

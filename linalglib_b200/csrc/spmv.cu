@@ -73,8 +73,10 @@ namespace lab
         k_spmm(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                const double* __restrict__ v, int32_t m, const double* __restrict__ X,
                int64_t ldx, double* __restrict__ Y, int64_t ldy, double alpha, double beta,
-               int lanes)
+               int lanes, const int* skip = nullptr)
     {
+        if(skip && *skip)
+            return;
         int64_t t    = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
         int     lane = (int)(t % lanes);
         int64_t row  = t / lanes;
@@ -106,6 +108,31 @@ namespace lab
                 *y = beta == 0.0 ? alpha * s[k] : fma(alpha, s[k], beta * *y);
             }
         }
+    }
+}
+
+namespace lab
+{
+    // Y[:, 0:k] = A X[:, 0:k] for k <= 8 columns in one pass over A (enqueue only).
+    lab_status spmm_columns(const lab_csr_impl* A, int k, const double* X, int64_t ldx, double* Y,
+                            int64_t ldy, cudaStream_t s, const int* skip)
+    {
+        if(A->m == 0 || k <= 0)
+            return LAB_OK;
+        int      lanes = A->plan.alg == LAB_SPMV_ROWSEQ ? 4 : A->plan.lanes;
+        unsigned grid  = (unsigned)ceil_div<int64_t>(A->m * (int64_t)lanes, 256);
+        int32_t  m     = (int32_t)A->m;
+        if(k == 8)
+            LAB_LAUNCH(k_spmm<8>, grid, 256, 0, s, A->row_ptr, A->col_ind, A->val, m, X, ldx, Y,
+                       ldy, 1.0, 0.0, lanes, skip);
+        else if(k == 4)
+            LAB_LAUNCH(k_spmm<4>, grid, 256, 0, s, A->row_ptr, A->col_ind, A->val, m, X, ldx, Y,
+                       ldy, 1.0, 0.0, lanes, skip);
+        else
+            for(int q = 0; q < k; q++)
+                LAB_LAUNCH(k_spmm<1>, grid, 256, 0, s, A->row_ptr, A->col_ind, A->val, m,
+                           X + q * ldx, ldx, Y + q * ldy, ldy, 1.0, 0.0, lanes, skip);
+        return LAB_OK;
     }
 }
 

@@ -158,6 +158,112 @@ namespace lab
             reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
     }
 
+    __device__ __forceinline__ void cp_async_commit()
+    {
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    template <int N>
+    __device__ __forceinline__ void cp_async_wait_group()
+    {
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+    }
+
+    // Persistent, double-buffered form of k_rowseq: each CTA walks row blocks
+    // blockIdx.x, blockIdx.x + gridDim.x, ... and prefetches block k+1 into the
+    // other shared-memory stage (cp.async groups) while it computes block k, so
+    // the DRAM stream never waits for the gathers and the fma chains.  Same
+    // per-row arithmetic as k_rowseq (bit-identical results).
+    template <class Op, int NT, int MAXR>
+    __global__ void __launch_bounds__(NT)
+        k_rowseq_pipe(csr_view<typename Op::val_t> A, Op op, int cap, red_buf red, int nblocks)
+    {
+        using VT = typename Op::val_t;
+        using AT = typename Op::acc_t;
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        constexpr int VPC    = 16 / sizeof(VT);
+        const size_t  sv_b   = ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16;
+        const size_t  sc_b   = ((size_t)(cap + 8) * 4 + 15) / 16 * 16;
+        const size_t  stage_b = sv_b + sc_b;
+        if(red.skip && *red.skip)
+            return;
+
+        auto issue = [&](int blk, int stage) {
+            const int r0  = blk * NT;
+            const int r1  = min(r0 + NT, A.m);
+            const int j0  = A.rp[r0];
+            const int j1  = A.rp[r1];
+            const int j0v = j0 & ~(VPC - 1);
+            const int j0c = j0 & ~3;
+            if((j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4)
+            {
+                VT*      sv = reinterpret_cast<VT*>(smem_raw + stage * stage_b);
+                int32_t* sc = reinterpret_cast<int32_t*>(smem_raw + stage * stage_b + sv_b);
+                const int nv = (j1 - j0v + VPC - 1) / VPC;
+                const int nc = (j1 - j0c + 3) / 4;
+                for(int k = threadIdx.x; k < nv; k += NT)
+                    cp_async16(sv + (size_t)k * VPC, A.v + j0v + (size_t)k * VPC);
+                for(int k = threadIdx.x; k < nc; k += NT)
+                    cp_async16(sc + (size_t)k * 4, A.ci + j0c + (size_t)k * 4);
+            }
+        };
+
+        double contrib = 0.0;
+        int    blk     = blockIdx.x;
+        if(blk < nblocks)
+            issue(blk, 0);
+        cp_async_commit();
+        for(int it = 0; blk < nblocks; it++, blk += gridDim.x)
+        {
+            const int nxt = blk + gridDim.x;
+            if(nxt < nblocks)
+                issue(nxt, (it + 1) & 1);
+            cp_async_commit();
+            cp_async_wait_group<1>(); // everything but the newest group has landed
+            __syncthreads();
+            const int stage = it & 1;
+            const int r0    = blk * NT;
+            const int r1    = min(r0 + NT, A.m);
+            const int j0    = A.rp[r0];
+            const int j1    = A.rp[r1];
+            const int j0v   = j0 & ~(VPC - 1);
+            const int j0c   = j0 & ~3;
+            const bool staged = (j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4;
+            const VT*      sv = reinterpret_cast<const VT*>(smem_raw + stage * stage_b);
+            const int32_t* sc = reinterpret_cast<const int32_t*>(smem_raw + stage * stage_b + sv_b);
+            const int row = r0 + threadIdx.x;
+            if(row < r1)
+            {
+                const int a = A.rp[row], b = A.rp[row + 1];
+                AT        s = AT(0);
+                if(staged)
+                {
+                    AT vv[MAXR], xv[MAXR];
+#pragma unroll
+                    for(int k = 0; k < MAXR; k++)
+                        if(a + k < b)
+                        {
+                            vv[k] = to_acc(sv[a + k - j0v], AT(0));
+                            xv[k] = op.gather(sc[a + k - j0c]);
+                        }
+#pragma unroll
+                    for(int k = 0; k < MAXR; k++)
+                        if(a + k < b)
+                            s = acc_step<Op::kFma>(vv[k], xv[k], s);
+                }
+                else
+                {
+                    for(int j = a; j < b; j++)
+                        s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), op.gather(A.ci[j]), s);
+                }
+                contrib += op.finish(row, s);
+            }
+            __syncthreads(); // this stage is refilled by the prefetch two blocks on
+        }
+        cp_async_wait_group<0>();
+        if(Op::kReduce)
+            reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
+    }
+
     template <class Op, int NT, int W>
     __global__ void __launch_bounds__(NT)
         k_vector(csr_view<typename Op::val_t> A, Op op, red_buf red)
@@ -229,13 +335,47 @@ namespace lab
             LAB_CUDA(attr16);
             LAB_CUDA(attr0);
             const unsigned grid = (unsigned)rowop_grid(A);
-            if(p.max_row <= 8)
-                LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 8>), grid, kRowseqNT, smem, s, V, op, cap, red);
-            else if(p.max_row <= 16)
-                LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 16>), grid, kRowseqNT, smem, s, V, op, cap,
-                           red);
-            else
-                LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 0>), grid, kRowseqNT, smem, s, V, op, cap, red);
+            if(p.max_row <= 16)
+            {
+                // persistent double-buffered kernel; stage capacity fixed per instantiation
+                const int  nblocks = (int)grid;
+                const bool r8      = p.max_row <= 8;
+                const int  pcap    = kRowseqNT * (r8 ? 8 : 16);
+                const size_t psmem = 2 * (((size_t)(pcap + 16) * sizeof(VT) + 15) / 16 * 16 +
+                                          ((size_t)(pcap + 8) * 4 + 15) / 16 * 16);
+                static int occ8 = -1, occ16 = -1;
+                int&       occ  = r8 ? occ8 : occ16;
+                if(occ < 0)
+                {
+                    if(r8)
+                    {
+                        LAB_CUDA(cudaFuncSetAttribute(k_rowseq_pipe<Op, kRowseqNT, 8>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)psmem));
+                        LAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                            &occ, k_rowseq_pipe<Op, kRowseqNT, 8>, kRowseqNT, psmem));
+                    }
+                    else
+                    {
+                        LAB_CUDA(cudaFuncSetAttribute(k_rowseq_pipe<Op, kRowseqNT, 16>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)psmem));
+                        LAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                            &occ, k_rowseq_pipe<Op, kRowseqNT, 16>, kRowseqNT, psmem));
+                    }
+                    occ = std::max(occ, 1);
+                }
+                const unsigned pgrid =
+                    (unsigned)std::min<int64_t>(nblocks, (int64_t)num_sms() * occ);
+                if(r8)
+                    LAB_LAUNCH((k_rowseq_pipe<Op, kRowseqNT, 8>), pgrid, kRowseqNT, psmem, s, V,
+                               op, pcap, red, nblocks);
+                else
+                    LAB_LAUNCH((k_rowseq_pipe<Op, kRowseqNT, 16>), pgrid, kRowseqNT, psmem, s, V,
+                               op, pcap, red, nblocks);
+                return LAB_OK;
+            }
+            LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 0>), grid, kRowseqNT, smem, s, V, op, cap, red);
             return LAB_OK;
         }
         unsigned grid = (unsigned)rowop_grid(A);

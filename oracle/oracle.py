@@ -383,15 +383,9 @@ class Reference:
                            rel_tol, abs_tol, max_iter)
         return x, it
 
-    def gmres(self, A, b, restart=30, hier=None, x0=None, rel_tol=1e-6, abs_tol=1e-6,
-              max_iter=1000):
-        rp, ci, v, m, n, z = self._arr(A)
-        x = np.zeros(m) if x0 is None else np.array(x0, dtype=np.float64)
-        b = np.ascontiguousarray(b, dtype=np.float64)
-        it = self.L.ref_gmres(m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(b), _ptr(x), restart,
-                              hier.h if hier is not None else None, 1, 1, rel_tol, abs_tol,
-                              max_iter)
-        return x, it
+    # No gmres(): the reference's gmres_solver::build leaves its residual vectors
+    # unsized (gmres.cpp:211-220) and its solve writes out of bounds (it crashed
+    # the test process); gmres_restated() below is the GMRES checker.
 
 
 class ReferenceHierarchy:
@@ -452,6 +446,90 @@ class ReferenceHierarchy:
         it = self.ref.L.ref_amg_solve(self.h, _ptr(b), _ptr(x), n1, n2, cycle, smoother,
                                       rel_tol, abs_tol, max_cycle)
         return x, it
+
+
+def gmres_restated(A, b, restart, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000, x0=None):
+    """Unpreconditioned restarted GMRES as the reference runs it
+    (library/src/iterative_solvers/krylov/gmres.cpp:224-368): modified Gram-Schmidt
+    Arnoldi (93-161), Givens rotations (163-199), 2-norm stopping test relative to
+    the initial residual, back substitution, restart from the true residual.
+    Returns (x, restart cycles).  The reference's own gmres_solver::build leaves
+    its residual vectors unsized (gmres.cpp:211-220), so its solve writes out of
+    bounds; this restatement is the checker instead."""
+    rp, ci, v = (np.asarray(a) for a in A[:3])
+    n = rp.size - 1
+    rows = np.repeat(np.arange(n), np.diff(rp))
+
+    def mv(x):
+        return np.bincount(rows, weights=v * x[ci], minlength=n)
+
+    restart = min(restart, n - 1)
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+
+    def conv(rn, r0):
+        if np.isnan(rn) or np.isnan(r0):
+            return False
+        return rn <= abs_tol or rn / r0 <= rel_tol
+
+    r = b - mv(x)
+    rn = np.linalg.norm(r)
+    r0 = rn
+    if conv(rn, r0):
+        return x, 0
+    it = 0
+    while not it > max_iter:
+        Q = np.zeros((restart + 1, n))
+        H = np.zeros((restart + 1, restart))
+        cs = np.zeros(restart)
+        sn = np.zeros(restart)
+        g = np.zeros(restart + 1)
+        Q[0] = r / rn
+        g[0] = rn
+        k = 1
+        while k <= restart:
+            w = mv(Q[k - 1])
+            for i in range(k):
+                H[i, k - 1] = np.dot(Q[i], w)
+                w = w - H[i, k - 1] * Q[i]
+            H[k, k - 1] = np.sqrt(np.dot(w, w))
+            Q[k] = w / H[k, k - 1]
+            for i in range(k - 1):
+                t1, t2 = H[i, k - 1], H[i + 1, k - 1]
+                H[i, k - 1] = cs[i] * t1 + sn[i] * t2
+                H[i + 1, k - 1] = -sn[i] * t1 + cs[i] * t2
+            xi, xj = H[k - 1, k - 1], H[k, k - 1]
+            if xi == 0.0:
+                cs[k - 1], sn[k - 1] = 0.0, 1.0
+            elif xj == 0.0:
+                cs[k - 1], sn[k - 1] = 1.0, 0.0
+            elif abs(xi) > abs(xj):
+                t = xj / xi
+                cs[k - 1] = 1.0 / np.sqrt(1.0 + t * t)
+                sn[k - 1] = t * cs[k - 1]
+            else:
+                t = xi / xj
+                sn[k - 1] = 1.0 / np.sqrt(1.0 + t * t)
+                cs[k - 1] = t * sn[k - 1]
+            t1, t2 = H[k - 1, k - 1], H[k, k - 1]
+            H[k - 1, k - 1] = cs[k - 1] * t1 + sn[k - 1] * t2
+            H[k, k - 1] = -sn[k - 1] * t1 + cs[k - 1] * t2
+            g[k] = -sn[k - 1] * g[k - 1]
+            g[k - 1] = cs[k - 1] * g[k - 1]
+            if conv(abs(g[k]), r0) or k == restart:
+                break
+            k += 1
+        y = g[:k].copy()
+        for i in range(k - 1, -1, -1):
+            for j in range(i + 1, k):
+                y[i] -= H[i, j] * y[j]
+            y[i] /= H[i, i]
+        x = x + Q[:k].T @ y
+        r = b - mv(x)
+        rn = np.linalg.norm(r)
+        if conv(rn, r0):
+            break
+        it += 1
+    return x, it
 
 
 def load_reference():
