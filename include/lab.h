@@ -157,6 +157,15 @@ LAB_API lab_status lab_jacobi_solve(int64_t n, const double* rhs, const double* 
 /* In-place exclusive prefix sums.  linalg_primitives.h:98 (host_primitives.cpp:76-91). */
 LAB_API lab_status lab_exclusive_scan_i64(int64_t n, int64_t* x, lab_stream s);
 LAB_API lab_status lab_exclusive_scan_i32(int64_t n, int32_t* x, lab_stream s);
+/* The int64 exclusive scan for callers that must not allocate device memory
+ * during the call: its scratch is a fixed 512 KiB array in the library's device
+ * image, so it calls no cudaMalloc / cudaFree and no allocating routine.  No
+ * counterpart in the reference (it has no allocation-free variants).
+ * Limit: n <= 134,217,728 elements; larger n returns LAB_BAD_ARG untouched.
+ * The first call on each device looks up the array's device address (make
+ * that first call before any stream capture).  All calls share the one array:
+ * calls that overlap on the GPU (other streams, other threads) race. */
+LAB_API lab_status lab_exclusive_scan_i64_noalloc(int64_t n, int64_t* x, lab_stream s);
 
 /* ------------------------------------------------------------------ sparse products */
 /* C = A*B (new matrix), rows sorted by column, each entry accumulated in A-row

@@ -83,6 +83,7 @@ _SIGS = {
     "lab_jacobi_solve": [_i64, _p, _p, _p, _p],
     "lab_exclusive_scan_i64": [_i64, _p, _p],
     "lab_exclusive_scan_i32": [_i64, _p, _p],
+    "lab_exclusive_scan_i64_noalloc": [_i64, _p, _p],
     "lab_spgemm": [_p, _p, C.POINTER(_p), _p],
     "lab_spgeam": [_d, _p, _d, _p, C.POINTER(_p), _p],
     "lab_transpose": [_p, C.POINTER(_p), _p],

@@ -462,6 +462,20 @@ namespace lab
         return LAB_OK;
     }
 
+    // In-place exclusive scan with caller-provided block-sum scratch
+    // (bsum: ceil(n / 2048) entries); launches only, allocates nothing.
+    lab_status scan_i64_into(int64_t* x, int64_t n, int64_t* bsum, cudaStream_t s)
+    {
+        if(n <= 0)
+            return LAB_OK;
+        int64_t nb = ceil_div<int64_t>(n, kScanTile);
+        LAB_LAUNCH(k_scan_tiles<int64_t>, (unsigned)nb, kScanThreads, 0, s, x, n, bsum);
+        LAB_LAUNCH(k_scan_bsums<int64_t>, 1, 1024, 0, s, bsum, nb);
+        LAB_LAUNCH(k_scan_apply<int64_t>, (unsigned)nb, kScanThreads, 0, s, x, n,
+                   (const int64_t*)bsum);
+        return LAB_OK;
+    }
+
     lab_status scan_i32(int32_t* x, int64_t n, cudaStream_t s)
     {
         return scan_impl<int32_t>(x, n, s);
