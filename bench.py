@@ -55,9 +55,11 @@ def parse():
     ap.add_argument("--n", type=int, default=128, help="grid side of the 3D Poisson system")
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="full", choices=["full", "profile"],
+    ap.add_argument("--mode", default="full", choices=["full", "profile", "spmv"],
                     help="profile: only the warm-up and timed device-resident steps (the "
-                         "command the ncu launch lists in profiles/ are taken from)")
+                         "command the ncu launch lists in profiles/ are taken from); "
+                         "spmv: only the standalone level-0 SpMV timing (5 warm-up launches, "
+                         "then 30 timed ones, each after an L2 flush)")
     return ap.parse_args()
 
 
@@ -111,7 +113,12 @@ class Dist:
 
 # ------------------------------------------------------------------ clocks
 class Clocks:
-    """nvidia-smi samples of this rank's GPU during the timed region."""
+    """nvidia-smi samples of this rank's GPU during the timed region.
+
+    The sampler is started before the warm-up (nvidia-smi's own start-up takes
+    about a second and must not overlap the timed steps); begin()/stop() bracket
+    the timed region and only samples taken inside it are kept (the nearest
+    ones if the region is shorter than the sampling period)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -121,6 +128,7 @@ class Clocks:
         self.idx = gpu_index
         self.proc = None
         self.lines = []
+        self.t0 = None
 
     def start(self):
         try:
@@ -135,20 +143,28 @@ class Clocks:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def begin(self):
+        self.t0 = time.monotonic()
 
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t1 = time.monotonic()
         time.sleep(0.3)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        t0 = self.t0 if self.t0 is not None else t1
+        inside = [ln for t, ln in self.lines if t0 <= t <= t1 + 0.25]
+        if not inside and self.lines:
+            inside = [min(self.lines, key=lambda tl: abs(tl[0] - t1))[1]]
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in inside:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -295,6 +311,13 @@ def run_ours(args, d):
     stream = torch.cuda.current_stream()
     dA = core.CsrMatrix.from_arrays(*A)
     dA.analyse()
+    if args.mode == "spmv":
+        roof = dominant_kernel_roofline(core, dA, m, nnz, torch)
+        if d.rank == 0:
+            print(json.dumps({"mode": "spmv", "rows": int(m), "nnz": int(nnz), "roofline": roof}),
+                  flush=True)
+        d.close()
+        return 0
     bd = core.vec(b)
     opts = core.amg_options(n1=1, n2=1, omega=1.0)
     ctl = core.iter_control(rel_tol=args.rtol, abs_tol=0.0, max_iter=1000)
@@ -309,13 +332,14 @@ def run_ours(args, d):
         return H, info
 
     xs = [torch.zeros(m, dtype=torch.float64, device="cuda") for _ in range(2)]
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
     for i in range(args.warmup):
         step(xs[i % 2])
     torch.cuda.synchronize()
     keep.clear()
 
-    clocks = Clocks(torch.cuda.current_device())
-    clocks.start()
+    clocks.begin()
     d.barrier()
     torch.cuda.synchronize()
     l0 = core.launch_count()

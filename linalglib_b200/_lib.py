@@ -164,6 +164,15 @@ def call(name, *args):
     return check(getattr(lib(), name)(*args), name)
 
 
+def call_solve(name, *args):
+    """Like call(), for solvers: a NaN/Inf residual or a breakdown is an outcome
+    reported in the solve info, not an exception."""
+    st = getattr(lib(), name)(*args)
+    if st in (LAB_NAN, LAB_BREAKDOWN):
+        return st
+    return check(st, name)
+
+
 def declared_symbols(header_path=None):
     """Names of the functions include/lab.h declares (for export checks)."""
     import re

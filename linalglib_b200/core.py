@@ -10,7 +10,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from ._lib import AmgOptions, IterControl, SolveInfo, call, lib
+from ._lib import AmgOptions, IterControl, SolveInfo, call, call_solve, lib
 
 _initialised = False
 
@@ -60,10 +60,11 @@ class CsrMatrix:
     @classmethod
     def from_arrays(cls, row_ptr, col_ind, val, n=None, stream=None):
         init()
-        if isinstance(row_ptr, torch.Tensor) and row_ptr.is_cuda:
-            rp = row_ptr.to(torch.int32).contiguous()
-            ci = col_ind.to(torch.int32).contiguous()
-            v = val.to(torch.float64).contiguous()
+        if any(isinstance(a, torch.Tensor) and a.is_cuda for a in (row_ptr, col_ind, val)):
+            # any device operand: all three go to the device
+            rp = torch.as_tensor(row_ptr, device="cuda").to(torch.int32).contiguous()
+            ci = torch.as_tensor(col_ind, device="cuda").to(torch.int32).contiguous()
+            v = torch.as_tensor(val, device="cuda").to(torch.float64).contiguous()
             where = L.MEM_DEVICE
             m = rp.numel() - 1
             nnz = v.numel()
@@ -278,7 +279,7 @@ class Hierarchy:
         if x is None:
             x = torch.zeros_like(b)
         info = SolveInfo()
-        call("lab_amg_solve", self.h, C.byref(options), ptr(b), ptr(x), C.byref(control),
+        call_solve("lab_amg_solve", self.h, C.byref(options), ptr(b), ptr(x), C.byref(control),
              C.byref(info), stream_handle())
         return x, info
 
@@ -321,7 +322,7 @@ def pcg(A: CsrMatrix, b, x=None, M: Preconditioner | None = None, control=None):
     if x is None:
         x = torch.zeros_like(b)
     info = SolveInfo()
-    call("lab_pcg_solve", A.h, M.h if M is not None else None, ptr(b), ptr(x),
+    call_solve("lab_pcg_solve", A.h, M.h if M is not None else None, ptr(b), ptr(x),
          C.byref(control), C.byref(info), stream_handle())
     return x, info
 
@@ -330,7 +331,7 @@ def pcg_host(A: CsrMatrix, b: np.ndarray, x: np.ndarray, M=None, control=None):
     """PCG with host (numpy) b and x: the copies happen inside the call."""
     control = control or iter_control()
     info = SolveInfo()
-    call("lab_pcg_solve_host", A.h, M.h if M is not None else None, ptr(b), ptr(x),
+    call_solve("lab_pcg_solve_host", A.h, M.h if M is not None else None, ptr(b), ptr(x),
          C.byref(control), C.byref(info), stream_handle())
     return x, info
 
@@ -340,7 +341,7 @@ def gmres(A: CsrMatrix, b, x=None, M: Preconditioner | None = None, restart=30, 
     if x is None:
         x = torch.zeros_like(b)
     info = SolveInfo()
-    call("lab_gmres_solve", A.h, M.h if M is not None else None, restart, ptr(b), ptr(x),
+    call_solve("lab_gmres_solve", A.h, M.h if M is not None else None, restart, ptr(b), ptr(x),
          C.byref(control), C.byref(info), stream_handle())
     return x, info
 
@@ -352,7 +353,7 @@ def adjoint_solve(A: CsrMatrix, g, M: Preconditioner | None = None, symmetric=Tr
     if lam is None:
         lam = torch.zeros_like(g)
     info = SolveInfo()
-    call("lab_adjoint_solve", A.h, M.h if M is not None else None, int(bool(symmetric)), ptr(g),
+    call_solve("lab_adjoint_solve", A.h, M.h if M is not None else None, int(bool(symmetric)), ptr(g),
          ptr(lam), C.byref(control), C.byref(info), stream_handle())
     return lam, info
 
@@ -384,7 +385,7 @@ def batched_pcg(A: CsrMatrix, offsets, b, M: Preconditioner, x=None, control=Non
     iters = (C.c_int * nsys)()
     conv = (C.c_int * nsys)()
     info = SolveInfo()
-    call("lab_batched_pcg_solve", A.h, M.h, nsys, offs, ptr(b), ptr(x), C.byref(control), iters,
+    call_solve("lab_batched_pcg_solve", A.h, M.h, nsys, offs, ptr(b), ptr(x), C.byref(control), iters,
          conv, C.byref(info), stream_handle())
     return x, np.array(iters[:]), np.array(conv[:]), info
 
@@ -398,6 +399,6 @@ def multi_rhs_pcg(A: CsrMatrix, B, M: Preconditioner, X=None, control=None):
     iters = (C.c_int * k)()
     conv = (C.c_int * k)()
     info = SolveInfo()
-    call("lab_multi_rhs_pcg_solve", A.h, M.h, k, ptr(B), ptr(X), C.byref(control), iters, conv,
+    call_solve("lab_multi_rhs_pcg_solve", A.h, M.h, k, ptr(B), ptr(X), C.byref(control), iters, conv,
          C.byref(info), stream_handle())
     return X, np.array(iters[:]), np.array(conv[:]), info

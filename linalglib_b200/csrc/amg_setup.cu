@@ -306,6 +306,34 @@ namespace lab
             G::sync();
             return n;
         }
+        template <bool VALS, class F>
+        __device__ void emit_seq(int row, F&& f) const
+        {
+            const int a0 = rp[row], a1 = rp[row + 1];
+            double    coef = 0.0, dval = 0.0;
+            if(VALS)
+            {
+                double dg = 0.0;
+                for(int j = a0; j < a1; j++)
+                {
+                    if(ci[j] == row)
+                        dg = __dadd_rn(dg, v[j]);
+                    else if(conn[j] == 0)
+                        dg = __dsub_rn(dg, v[j]);
+                }
+                coef = __dmul_rn(-relax, __ddiv_rn(1.0, dg));
+                dval = __dsub_rn(1.0, relax);
+            }
+            for(int j = a0; j < a1; j++)
+            {
+                const int c = ci[j];
+                if(c != row && conn[j] != 1)
+                    continue;
+                const int64_t ag = agg[c];
+                if(ag >= 0)
+                    f((int)ag, VALS ? ((c == row) ? dval : __dmul_rn(coef, v[j])) : 0.0);
+            }
+        }
         __device__ int32_t out_start(int row) const
         {
             return out_rp[row];

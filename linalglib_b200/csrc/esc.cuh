@@ -19,6 +19,7 @@
 
 namespace lab
 {
+    constexpr int kEscLaneCap = 32;
     constexpr int kEscWarpCap = 256;
     constexpr int kEscCtaCap  = 4096;
     constexpr int kEscCtaNT   = 512;
@@ -180,6 +181,63 @@ namespace lab
         }
     }
 
+    // ------------------------------------------------------------------ lane tier
+    // Rows with at most kEscLaneCap items: one lane per row.  The lane keeps the
+    // row's distinct columns as a sorted list in shared memory (entry e of lane l
+    // at [e][l], bank-conflict free) and applies the items one at a time in
+    // canonical order: a new column is inserted with its value, a repeated one
+    // is added to (rounded once per addition) -- the reference's accumulation.
+    // Exp::emit_seq(row, f) calls f(col, val) for the row's items in order.
+    constexpr int kEscLaneWarps = 4;
+
+    template <class Exp, int MODE>
+    __global__ void __launch_bounds__(32 * kEscLaneWarps)
+        k_esc_lane(Exp e, const int32_t* __restrict__ rows, int nrows, int32_t* counts,
+                   int32_t* out_col, double* out_val)
+    {
+        __shared__ int    skey[kEscLaneWarps][kEscLaneCap][32];
+        __shared__ double sval[MODE == 1 ? kEscLaneWarps : 1][MODE == 1 ? kEscLaneCap : 1][32];
+        const int         w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for(int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x)
+        {
+            const int row = rows[r];
+            int       len = 0;
+            e.template emit_seq<MODE == 1>(row, [&](int c, double v) {
+                int pos = 0;
+                while(pos < len && skey[w][pos][lane] < c)
+                    pos++;
+                if(pos < len && skey[w][pos][lane] == c)
+                {
+                    if(MODE == 1)
+                        sval[w][pos][lane] = __dadd_rn(sval[w][pos][lane], v);
+                    return;
+                }
+                for(int q = len; q > pos; q--)
+                {
+                    skey[w][q][lane] = skey[w][q - 1][lane];
+                    if(MODE == 1)
+                        sval[w][q][lane] = sval[w][q - 1][lane];
+                }
+                skey[w][pos][lane] = c;
+                if(MODE == 1)
+                    sval[w][pos][lane] = v;
+                len++;
+            });
+            if(MODE == 0)
+                counts[row] = len;
+            else
+            {
+                const int32_t o = e.out_start(row);
+                for(int q = 0; q < len; q++)
+                {
+                    out_col[o + q] = skey[w][q][lane];
+                    if(out_val)
+                        out_val[o + q] = sval[MODE == 1 ? w : 0][MODE == 1 ? q : 0][lane];
+                }
+            }
+        }
+    }
+
     // ------------------------------------------------------------------ kernels
     // Exp interface:
     //   __device__ int  upper(int row) const        item count (computed before)
@@ -281,8 +339,8 @@ namespace lab
     // Row classification by item count: tier lists (unordered within a tier).
     struct esc_tiers
     {
-        dbuf<int32_t> rows;       // [m] : W rows, then B rows, then G rows
-        int           nw = 0, nb = 0, ng = 0;
+        dbuf<int32_t> rows; // [m] : lane rows, then W rows, then B rows, then G rows
+        int           nl = 0, nw = 0, nb = 0, ng = 0;
         dbuf<int64_t> g_offsets;  // [ng] scratch offsets of G rows
         int64_t       g_total = 0;
         dbuf<uint64_t> g_keys;
@@ -295,12 +353,20 @@ namespace lab
     lab_status esc_run(const Exp& e, int64_t m, esc_tiers& t, int32_t* counts, int32_t* out_col,
                        double* out_val, cudaStream_t s)
     {
+        if(t.nl > 0)
+        {
+            unsigned grid = (unsigned)std::min<int64_t>(
+                ceil_div<int64_t>(t.nl, 32 * kEscLaneWarps), (int64_t)num_sms() * 16);
+            LAB_LAUNCH((k_esc_lane<Exp, MODE>), grid, 32 * kEscLaneWarps, 0, s, e, t.rows.get(),
+                       t.nl, counts, out_col, out_val);
+        }
+        const int32_t* wrows = t.rows.get() + t.nl;
         if(t.nw > 0)
         {
             unsigned grid = (unsigned)std::min<int64_t>(
                 ceil_div<int64_t>(t.nw, kEscWarpsPerCta), (int64_t)num_sms() * 8);
-            LAB_LAUNCH((k_esc_warp<Exp, MODE>), grid, 32 * kEscWarpsPerCta, 0, s, e, t.rows.get(),
-                       t.nw, counts, out_col, out_val);
+            LAB_LAUNCH((k_esc_warp<Exp, MODE>), grid, 32 * kEscWarpsPerCta, 0, s, e, wrows, t.nw,
+                       counts, out_col, out_val);
         }
         if(t.nb > 0)
         {
@@ -309,15 +375,15 @@ namespace lab
                 k_esc_cta<Exp, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             LAB_CUDA(attr);
             unsigned grid = (unsigned)std::min<int64_t>(t.nb, (int64_t)num_sms() * 3);
-            LAB_LAUNCH((k_esc_cta<Exp, MODE>), grid, kEscCtaNT, smem, s, e, t.rows.get() + t.nw,
-                       t.nb, counts, out_col, out_val);
+            LAB_LAUNCH((k_esc_cta<Exp, MODE>), grid, kEscCtaNT, smem, s, e, wrows + t.nw, t.nb,
+                       counts, out_col, out_val);
         }
         if(t.ng > 0)
         {
             unsigned grid = (unsigned)std::min<int64_t>(t.ng, (int64_t)num_sms() * 2);
-            LAB_LAUNCH((k_esc_big<Exp, MODE>), grid, kEscBigNT, 0, s, e,
-                       t.rows.get() + t.nw + t.nb, t.ng, t.g_offsets.get(), t.g_keys.get(),
-                       t.g_vals.get(), counts, out_col, out_val);
+            LAB_LAUNCH((k_esc_big<Exp, MODE>), grid, kEscBigNT, 0, s, e, wrows + t.nw + t.nb,
+                       t.ng, t.g_offsets.get(), t.g_keys.get(), t.g_vals.get(), counts, out_col,
+                       out_val);
         }
         return LAB_OK;
     }

@@ -77,6 +77,7 @@ namespace lab
         S_GNEW  = 4,
         S_RTOL  = 5,
         S_ATOL  = 6,
+        S_ZQ    = 7, // (z_{k+1}, q_k), flexible variant only
         S_COUNT = 8
     };
     enum
@@ -182,13 +183,20 @@ namespace lab
     }
 
     // p = 1*z + beta*p (host_axpy.cpp:47-69), gamma <- (z, r), iter++.
+    // FLEX: beta = -(z_{k+1}, q_k) / (p_k, q_k), the flexible (Polak-Ribiere)
+    // choice: it equals (z_{k+1}, r_{k+1} - r_k) / (z_k, r_k), which keeps the
+    // search directions A-conjugate to the previous one when the preconditioner
+    // is not exactly the same symmetric operator at every application (a V-cycle
+    // rounded to FP32 / BF16).  With a fixed SPD preconditioner both choices agree
+    // in exact arithmetic.
+    template <bool FLEX>
     __global__ void __launch_bounds__(256)
         k_pcg_pupdate(int64_t n, double* __restrict__ p, const double* __restrict__ z, double* sc,
                       int* flags, unsigned int* counter)
     {
         if(flags[F_DONE])
             return;
-        const double beta = sc[S_GNEW] / sc[S_GAMMA];
+        const double beta = FLEX ? -(sc[S_ZQ] / sc[S_PQ]) : sc[S_GNEW] / sc[S_GAMMA];
         for(int64_t i = blockIdx.x * 256ll + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256)
             p[i] = beta == 0.0 ? z[i] : __dadd_rn(z[i], __dmul_rn(beta, p[i]));
         if(grid_ticket(counter))
@@ -304,6 +312,12 @@ namespace lab
         return r;
     }
 
+    // Reduced-precision cycles take the flexible beta (k_pcg_pupdate<true>).
+    static bool pcg_flexible(const precond_impl* M)
+    {
+        return M && M->kind == 0 && M->o.precision != LAB_PREC_FP64;
+    }
+
     // One PCG iteration (cg.cpp:185-213): enqueue only, captured into a graph.
     static lab_status pcg_iteration(lab_csr_impl* A, precond_impl* M, double* x, pcg_ws* w,
                                     cudaStream_t s)
@@ -315,8 +329,15 @@ namespace lab
                    (const double*)w->q, w->sc, w->flags, w->partial + w->partial_n,
                    w->counters + 1);
         LAB_TRY(precond_apply(M, w->r, w->z, s, skip, rbuf(w, 2, w->sc + S_GNEW, skip)));
-        LAB_LAUNCH(k_pcg_pupdate, red_grid(A->m), 256, 0, s, A->m, w->p, (const double*)w->z,
-                   w->sc, w->flags, w->counters + 3);
+        if(pcg_flexible(M))
+        {
+            LAB_TRY(dot_device(A->m, w->z, w->q, rbuf(w, 5, w->sc + S_ZQ, skip), s));
+            LAB_LAUNCH(k_pcg_pupdate<true>, red_grid(A->m), 256, 0, s, A->m, w->p,
+                       (const double*)w->z, w->sc, w->flags, w->counters + 3);
+        }
+        else
+            LAB_LAUNCH(k_pcg_pupdate<false>, red_grid(A->m), 256, 0, s, A->m, w->p,
+                       (const double*)w->z, w->sc, w->flags, w->counters + 3);
         return LAB_OK;
     }
 
@@ -422,13 +443,13 @@ namespace lab
     // Unpreconditioned CG as the reference runs it (cg.cpp:60-134): with
     // restart_iter = -1, `iter % restart_iter == 0` holds for every iter > 0, so
     // each iteration restarts from the true residual (steepest descent).
-    // Mixed precision: FP64 iterative refinement around PCG with the
+    // Mixed precision: FP64 iterative refinement around flexible PCG with the
     // reduced-precision cycle.  Each outer step recomputes the true residual
     // r = b - A x in FP64, applies the reference's stopping test to it, solves
-    // A e = r by PCG (FP64 vectors, scalars and dots; FP32 / BF16 cycle) to a
-    // relative 1e-6 (or just what is still needed), and corrects x += e.  The
-    // restart bounds the drift a reduced-precision preconditioner induces in the
-    // CG recurrences.
+    // A e = r by PCG (FP64 vectors, scalars and dots; FP32 / BF16 cycle; flexible
+    // beta) to what is still needed, and corrects x += e.  Usually one pass
+    // suffices; the outer FP64 check catches a recurrence residual that drifted
+    // from the true one.
     static lab_status pcg_refine(lab_csr_impl* A, precond_impl* M, const double* b, double* x,
                                  const lab_iter_control* ctl, lab_solve_info* info,
                                  cudaStream_t s)
@@ -446,7 +467,7 @@ namespace lab
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
         cudaEventRecord(t0, s);
-        double r0 = 0.0, rn = 0.0;
+        double r0 = 0.0, rn = 0.0, rprev = 0.0;
         int    total = 0, conv = 0;
         bool   nan   = false;
         lab_status st = LAB_OK;
@@ -471,9 +492,12 @@ namespace lab
             }
             if(total > ctl->max_iter)
                 break;
+            if(outer > 0 && !(rn < 0.5 * rprev))
+                break; // the last correction did not help: stop, not converged
+            rprev                  = rn;
             lab_iter_control inner = *ctl;
-            inner.abs_tol          = 0.0;
-            inner.rel_tol          = std::max(1e-6, 0.5 * ctl->rel_tol * r0 / rn);
+            inner.abs_tol          = ctl->abs_tol;
+            inner.rel_tol          = ctl->rel_tol * r0 / rn;
             inner.max_iter         = ctl->max_iter - total;
             lab_solve_info ii{};
             cudaMemsetAsync(e.get(), 0, sizeof(double) * m, s);
@@ -494,6 +518,8 @@ namespace lab
         if(st != LAB_OK)
             return st;
         lab_status status = conv ? LAB_OK : (nan ? LAB_NAN : LAB_NOT_CONVERGED);
+        if(status == LAB_NAN)
+            set_error("pcg: NaN/Inf residual after %d iterations", total);
         if(info)
         {
             info->iterations       = total;
@@ -551,7 +577,7 @@ namespace lab
                        w->counters + 1);
             // gamma = (r, r), beta, p update as the reference (overwritten by the restart)
             LAB_TRY(dot_device(A->m, w->r, w->r, rbuf(w, 2, w->sc + S_GNEW, skip), s));
-            LAB_LAUNCH(k_pcg_pupdate, red_grid(A->m), 256, 0, s, A->m, w->p, (const double*)w->r,
+            LAB_LAUNCH(k_pcg_pupdate<false>, red_grid(A->m), 256, 0, s, A->m, w->p, (const double*)w->r,
                        w->sc, w->flags, w->counters + 3);
             if((it & 7) == 7)
             {
@@ -636,6 +662,8 @@ namespace lab
         cudaEventDestroy(t0);
         cudaEventDestroy(t1);
         lab_status status = conv ? LAB_OK : (nan ? LAB_NAN : LAB_NOT_CONVERGED);
+        if(status == LAB_NAN)
+            set_error("amg_solve: NaN/Inf residual after %d cycles", cyc);
         if(info)
         {
             info->iterations       = cyc;
@@ -887,6 +915,8 @@ namespace lab
         cudaEventDestroy(t0);
         cudaEventDestroy(t1);
         lab_status status = conv ? LAB_OK : (bad ? LAB_NAN : LAB_NOT_CONVERGED);
+        if(status == LAB_NAN)
+            set_error("gmres: NaN/Inf residual after %d iterations", iter);
         if(info)
         {
             info->iterations       = iter;
@@ -1321,6 +1351,8 @@ namespace lab
             nan |= sf[k * GF_N + GF_STATUS] == LAB_NAN;
         }
         lab_status status = allconv ? LAB_OK : (nan ? LAB_NAN : LAB_NOT_CONVERGED);
+        if(status == LAB_NAN)
+            set_error("segmented pcg: a system's residual became NaN/Inf");
         if(info)
         {
             info->iterations       = maxit;

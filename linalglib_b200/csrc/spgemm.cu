@@ -5,41 +5,72 @@
 namespace lab
 {
     // ------------------------------------------------------------ tiers
+    // 0: lane tier, 1: warp tier, 2: CTA tier, 3: global tier
+    __device__ __forceinline__ int tier_of(int u)
+    {
+        return u <= kEscLaneCap ? 0 : (u <= kEscWarpCap ? 1 : (u <= kEscCtaCap ? 2 : 3));
+    }
+
     __global__ void k_tier_count(const int32_t* __restrict__ upper, int64_t m, int* cnt)
     {
-        __shared__ int s[3];
-        if(threadIdx.x < 3)
+        __shared__ int s[4];
+        if(threadIdx.x < 4)
             s[threadIdx.x] = 0;
         __syncthreads();
         for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
             i += (int64_t)gridDim.x * blockDim.x)
-        {
-            int u = upper[i];
-            atomicAdd(&s[u <= kEscWarpCap ? 0 : (u <= kEscCtaCap ? 1 : 2)], 1);
-        }
+            atomicAdd(&s[tier_of(upper[i])], 1);
         __syncthreads();
-        if(threadIdx.x < 3 && s[threadIdx.x])
+        if(threadIdx.x < 4 && s[threadIdx.x])
             atomicAdd(&cnt[threadIdx.x], s[threadIdx.x]);
+    }
+
+    // Append row i to list `t`: one atomic per warp and list (warp-aggregated), so
+    // millions of rows do not serialise on a single counter.  Must be called by
+    // every lane of the warp (inactive lanes pass t < 0).
+    __device__ __forceinline__ int warp_append(int* cursor, int t, int ntiers)
+    {
+        const int lane = threadIdx.x & 31;
+        int       pos  = -1;
+        for(int tt = 0; tt < ntiers; tt++)
+        {
+            unsigned bal = __ballot_sync(0xffffffffu, t == tt);
+            if(!bal)
+                continue;
+            int leader = __ffs(bal) - 1;
+            int base   = 0;
+            if(lane == leader)
+                base = atomicAdd(&cursor[tt], __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if(t == tt)
+                pos = base + __popc(bal & ((1u << lane) - 1u));
+        }
+        return pos;
     }
 
     __global__ void k_tier_fill(const int32_t* __restrict__ upper, int64_t m, int* cursor,
                                 int32_t* rows, int64_t* gsize)
     {
-        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
-            i += (int64_t)gridDim.x * blockDim.x)
+        // warp-uniform trip count: whole warps step together
+        for(int64_t base = blockIdx.x * (int64_t)blockDim.x; base < m;
+            base += (int64_t)gridDim.x * blockDim.x)
         {
-            int u = upper[i];
-            int t = u <= kEscWarpCap ? 0 : (u <= kEscCtaCap ? 1 : 2);
-            int p = atomicAdd(&cursor[t], 1);
-            rows[p] = (int32_t)i;
-            if(t == 2)
-                gsize[p - cursor[5]] = pow2_ceil(u);
+            const int64_t i = base + threadIdx.x;
+            int           u = i < m ? upper[i] : 0;
+            int           t = i < m ? tier_of(u) : -1;
+            int           p = warp_append(cursor, t, 4);
+            if(t >= 0)
+            {
+                rows[p] = (int32_t)i;
+                if(t == 3)
+                    gsize[p - cursor[5]] = pow2_ceil(u);
+            }
         }
     }
 
     lab_status esc_classify(const int32_t* upper, int64_t m, esc_tiers& t, cudaStream_t s)
     {
-        t.nw = t.nb = t.ng = 0;
+        t.nl = t.nw = t.nb = t.ng = 0;
         if(m == 0)
             return LAB_OK;
         dbuf<int> cnt;
@@ -47,13 +78,15 @@ namespace lab
         LAB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * 8, s));
         unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(m, 256), 4096);
         LAB_LAUNCH(k_tier_count, grid, 256, 0, s, upper, m, cnt.get());
-        int h[3];
-        LAB_TRY(copy_d2h_sync(h, cnt.get(), sizeof(int) * 3, s));
-        t.nw = h[0];
-        t.nb = h[1];
-        t.ng = h[2];
-        // cursors: [0]=W start, [1]=B start, [2]=G start, [5]=G start (for gsize index)
-        int cur[8] = {0, t.nw, t.nw + t.nb, 0, 0, t.nw + t.nb, 0, 0};
+        int h[4];
+        LAB_TRY(copy_d2h_sync(h, cnt.get(), sizeof(int) * 4, s));
+        t.nl = h[0];
+        t.nw = h[1];
+        t.nb = h[2];
+        t.ng = h[3];
+        // cursors: [0..3] = start of each tier's run in rows[], [5] = G start (gsize index)
+        const int gs = t.nl + t.nw + t.nb;
+        int cur[8] = {0, t.nl, t.nl + t.nw, gs, 0, gs, 0, 0};
         LAB_CUDA(cudaMemcpyAsync(cnt.get(), cur, sizeof(cur), cudaMemcpyHostToDevice, s));
         LAB_TRY(t.rows.alloc((size_t)m, s));
         LAB_TRY(t.g_offsets.alloc((size_t)std::max(t.ng, 1) + 1, s));
@@ -104,6 +137,17 @@ namespace lab
             }
             G::sync();
             return off;
+        }
+        template <bool VALS, class F>
+        __device__ void emit_seq(int row, F&& f) const
+        {
+            for(int j = A.rp[row]; j < A.rp[row + 1]; j++)
+            {
+                const int    k = A.ci[j];
+                const double a = VALS ? A.v[j] : 0.0;
+                for(int p = B.rp[k]; p < B.rp[k + 1]; p++)
+                    f(B.ci[p], VALS ? __dmul_rn(a, B.v[p]) : 0.0);
+            }
         }
         __device__ int32_t out_start(int row) const
         {
@@ -157,6 +201,14 @@ namespace lab
             G::sync();
             return (a1 - a0) + (b1 - b0);
         }
+        template <bool VALS, class F>
+        __device__ void emit_seq(int row, F&& f) const
+        {
+            for(int p = A.rp[row]; p < A.rp[row + 1]; p++)
+                f(A.ci[p], VALS ? __dmul_rn(alpha, A.v[p]) : 0.0);
+            for(int p = B.rp[row]; p < B.rp[row + 1]; p++)
+                f(B.ci[p], VALS ? __dmul_rn(beta, B.v[p]) : 0.0);
+        }
         __device__ int32_t out_start(int row) const
         {
             return out_rp[row];
@@ -188,6 +240,12 @@ namespace lab
             }
             G::sync();
             return a1 - a0;
+        }
+        template <bool VALS, class F>
+        __device__ void emit_seq(int row, F&& f) const
+        {
+            for(int p = A.rp[row]; p < A.rp[row + 1]; p++)
+                f(A.ci[p], VALS ? A.v[p] : 0.0);
         }
         __device__ int32_t out_start(int row) const
         {
@@ -290,91 +348,203 @@ namespace lab
     }
 
     // ------------------------------------------------------------ hash-accumulator SpGEMM
-    // For rows with many products but few distinct columns (the Galerkin products
-    // R*(A*P) and A*P on coarse levels: up to ~12k products, <= ~300 columns).
-    // One warp per row.  The warp walks the A row in order; for each entry the
-    // lanes take the distinct columns of the matching B row, so no two lanes ever
-    // touch the same table key within a step, and a __syncwarp separates steps:
-    // every column's contributions are added in A-row order, the first one
-    // assigned, exactly as host_csrgemm.cpp:119-139.  Only the distinct columns
-    // are then sorted.
-    constexpr int kHashWarps = 4;
-    constexpr int kHashSym   = 2048; // symbolic table slots per warp (keys only)
-    constexpr int kHashNum   = 1024; // numeric table slots per warp
-    constexpr int kHashNumMaxCnt = kHashNum / 2;
+    // Rows with more than 32 products (A*P and the Galerkin R*(A*P) on every level)
+    // go to a warp-per-row hash accumulator whose table lives in shared memory and
+    // is sized per row class (2x the row's product bound in the symbolic pass, 2x
+    // its exact column count in the numeric pass), so small rows run at high
+    // occupancy.  The row's products are enumerated flat: the A entries of the row
+    // are staged with their B-row bounds and a prefix of the B-row lengths, then
+    // each lane fetches kHashU products 32 apart (independent loads in flight) and
+    // the warp applies them 32 at a time in canonical order.  Lanes holding the
+    // same column in one chunk form a group (match.any) whose lowest lane adds the
+    // members' products one by one, in lane order, to that column's slot; the first
+    // product of a column is assigned.  That is the accumulation order of
+    // host_csrgemm.cpp:119-139 (A-row order, then B-row order, rounded once per
+    // addition).  The filled slots are then sorted by column and written.
+    constexpr int kHashACap    = 64; // A entries staged per piece
+    constexpr int kHashU       = 4;  // products in flight per lane
+    constexpr int kHashClasses = 8;
+
+    template <int MODE, int HS>
+    struct hash_smem
+    {
+        int      key[HS];
+        double   val[MODE == 1 ? HS : 1];
+        uint64_t sk[MODE == 1 ? HS / 2 : 1];
+        double   aa[MODE == 1 ? kHashACap : 1];
+        double   sp[MODE == 1 ? 32 : 1];
+        int      ab0[kHashACap];
+        int      aoff[kHashACap];
+        int      claims;
+    };
 
     __device__ __forceinline__ unsigned hash_slot(int c, unsigned mask)
     {
         return ((unsigned)c * 2654435761u >> 7) & mask;
     }
 
-    // mode 0: symbolic (counts[row], or the row goes to the overflow list)
-    template <int MODE>
-    __global__ void __launch_bounds__(32 * kHashWarps)
+    __device__ __forceinline__ int warp_inclusive_sum(int v)
+    {
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1)
+        {
+            int t = __shfl_up_sync(0xffffffffu, v, o);
+            if(lane >= o)
+                v += t;
+        }
+        return v;
+    }
+
+    // Claims col's slot (linear probing); returns the slot, *isnew if it was empty.
+    template <int HS>
+    __device__ __forceinline__ unsigned hash_claim(int* key, int col, bool* isnew)
+    {
+        constexpr unsigned mask = HS - 1;
+        unsigned           slot = hash_slot(col, mask);
+        *isnew                  = false;
+        for(unsigned probe = 0; probe < HS; probe++)
+        {
+            int old = atomicCAS(&key[slot], -1, col);
+            if(old == -1)
+            {
+                *isnew = true;
+                break;
+            }
+            if(old == col)
+                break;
+            slot = (slot + 1) & mask;
+        }
+        return slot;
+    }
+
+    // MODE 0: symbolic (counts[row], or the row goes to the overflow list when more
+    // than 3/4 of the table fills up); MODE 1: numeric into out_rp / out_ci / out_v.
+    template <int MODE, int HS, int WARPS>
+    __global__ void __launch_bounds__(32 * WARPS)
         k_hash_gemm(csr_ref A, csr_ref B, const int32_t* __restrict__ rows, int nrows,
                     int32_t* counts, const int32_t* __restrict__ out_rp, int32_t* out_ci,
                     double* out_v, int32_t* ovf_rows, int* n_ovf)
     {
+        using S = hash_smem<MODE, HS>;
         extern __shared__ __align__(16) unsigned char hsm[];
         const int      wid  = threadIdx.x >> 5;
         const int      lane = threadIdx.x & 31;
-        constexpr int  H    = MODE == 0 ? kHashSym : kHashNum;
-        const size_t   per  = MODE == 0 ? (size_t)H * 4 : (size_t)H * 4 + (size_t)H * 8 + (size_t)(H / 2) * 8;
-        unsigned char* base = hsm + per * wid;
-        int*           skey = reinterpret_cast<int*>(base);
-        double*        sval = reinterpret_cast<double*>(base + (size_t)H * 4);
-        uint64_t*      sk   = reinterpret_cast<uint64_t*>(base + (size_t)H * 12);
-        __shared__ int s_claims[kHashWarps];
+        S&             sm   = reinterpret_cast<S*>(hsm)[wid];
+        const unsigned full = 0xffffffffu;
 
-        for(int r = blockIdx.x * kHashWarps + wid; r < nrows; r += gridDim.x * kHashWarps)
+        for(int r = blockIdx.x * WARPS + wid; r < nrows; r += gridDim.x * WARPS)
         {
             const int row = rows[r];
-            int       cnt = 0;
-            unsigned  Hr  = H;
-            if(MODE == 1)
-            {
-                cnt = out_rp[row + 1] - out_rp[row];
-                Hr  = (unsigned)max(32, pow2_ceil(2 * cnt));
-            }
-            const unsigned mask = Hr - 1;
-            for(unsigned q = lane; q < Hr; q += 32)
-                skey[q] = -1;
+            for(int q = lane; q < HS; q += 32)
+                sm.key[q] = -1;
             if(lane == 0)
-                s_claims[wid] = 0;
+                sm.claims = 0;
             __syncwarp();
-            bool ovf = false;
-            for(int j = A.rp[row]; j < A.rp[row + 1] && !ovf; j++)
+            bool      ovf   = false;
+            const int a_end = A.rp[row + 1];
+            for(int ps = A.rp[row]; ps < a_end && !ovf; ps += kHashACap)
             {
-                const int    k  = A.ci[j];
-                const double a  = A.v[j];
-                const int    b0 = B.rp[k], b1 = B.rp[k + 1];
-                for(int p = b0 + lane; p < b1; p += 32)
+                const int nA = min(kHashACap, a_end - ps);
+                int       len[2];
+#pragma unroll
+                for(int h = 0; h < 2; h++)
                 {
-                    const int c    = B.ci[p];
-                    unsigned  slot = hash_slot(c, mask);
-                    for(unsigned probe = 0; probe < Hr; probe++)
+                    const int q = lane + 32 * h;
+                    len[h]      = 0;
+                    if(q < nA)
                     {
-                        int old = atomicCAS(&skey[slot], -1, c);
-                        if(old == -1)
-                        {
-                            if(MODE == 1)
-                                sval[slot] = __dmul_rn(a, B.v[p]);
-                            else
-                                atomicAdd(&s_claims[wid], 1);
-                            break;
-                        }
-                        if(old == c)
-                        {
-                            if(MODE == 1)
-                                sval[slot] = __dadd_rn(sval[slot], __dmul_rn(a, B.v[p]));
-                            break;
-                        }
-                        slot = (slot + 1) & mask;
+                        const int k  = A.ci[ps + q];
+                        const int b0 = B.rp[k];
+                        len[h]       = B.rp[k + 1] - b0;
+                        sm.ab0[q]    = b0;
+                        if(MODE == 1)
+                            sm.aa[q] = A.v[ps + q];
                     }
                 }
+                const int inc0 = warp_inclusive_sum(len[0]);
+                const int inc1 = warp_inclusive_sum(len[1]);
+                const int tot0 = __shfl_sync(full, inc0, 31);
+                const int T    = tot0 + __shfl_sync(full, inc1, 31);
+                sm.aoff[lane]      = inc0 - len[0];
+                sm.aoff[lane + 32] = tot0 + inc1 - len[1];
                 __syncwarp();
-                if(MODE == 0 && s_claims[wid] > (int)(3 * H / 4))
-                    ovf = true; // too many distinct columns for this table
+                for(int t0 = 0; t0 < T && !ovf; t0 += 32 * kHashU)
+                {
+                    int    c[kHashU];
+                    int    jj[kHashU];
+                    double bv[kHashU];
+#pragma unroll
+                    for(int u = 0; u < kHashU; u++)
+                    {
+                        const int t = t0 + 32 * u + lane;
+                        c[u]        = -1;
+                        jj[u]       = 0;
+                        bv[u]       = 0.0;
+                        if(t < T)
+                        {
+                            // the A entry j with aoff[j] <= t < aoff[j] + len_j
+                            int lo = 0, hi = nA - 1;
+                            while(lo < hi)
+                            {
+                                const int mid = (lo + hi + 1) >> 1;
+                                if(sm.aoff[mid] <= t)
+                                    lo = mid;
+                                else
+                                    hi = mid - 1;
+                            }
+                            const int p = sm.ab0[lo] + (t - sm.aoff[lo]);
+                            jj[u]       = lo;
+                            c[u]        = __ldg(B.ci + p);
+                            if(MODE == 1)
+                                bv[u] = __ldg(B.v + p);
+                        }
+                    }
+#pragma unroll
+                    for(int u = 0; u < kHashU; u++)
+                    {
+                        const int cc = c[u];
+                        if(MODE == 0)
+                        {
+                            bool isnew = false;
+                            if(cc >= 0)
+                                hash_claim<HS>(sm.key, cc, &isnew);
+                            const unsigned nb = __ballot_sync(full, isnew);
+                            if(lane == 0)
+                                sm.claims += __popc(nb);
+                        }
+                        else
+                        {
+                            const double   pr  = cc >= 0 ? __dmul_rn(sm.aa[jj[u]], bv[u]) : 0.0;
+                            const unsigned grp = __match_any_sync(full, cc);
+                            sm.sp[lane]        = pr;
+                            __syncwarp();
+                            if(cc >= 0 && (grp & ((1u << lane) - 1u)) == 0)
+                            {
+                                bool           isnew = false;
+                                const unsigned slot  = hash_claim<HS>(sm.key, cc, &isnew);
+                                unsigned       mm    = grp;
+                                double         e;
+                                if(isnew)
+                                {
+                                    e = pr;
+                                    mm &= mm - 1u;
+                                }
+                                else
+                                    e = sm.val[slot];
+                                while(mm)
+                                {
+                                    e = __dadd_rn(e, sm.sp[__ffs(mm) - 1]);
+                                    mm &= mm - 1u;
+                                }
+                                sm.val[slot] = e;
+                            }
+                        }
+                        __syncwarp();
+                    }
+                    if(MODE == 0 && sm.claims > 3 * HS / 4)
+                        ovf = true; // too many distinct columns for this table
+                }
                 __syncwarp();
             }
             if(MODE == 0)
@@ -384,62 +554,195 @@ namespace lab
                     if(ovf)
                         ovf_rows[atomicAdd(n_ovf, 1)] = row;
                     else
-                        counts[row] = s_claims[wid];
+                        counts[row] = sm.claims;
                 }
             }
             else
             {
                 // compact the filled slots, sort by column, write
                 int n = 0;
-                for(unsigned q0 = 0; q0 < Hr; q0 += 32)
+                for(int q0 = 0; q0 < HS; q0 += 32)
                 {
-                    unsigned q    = q0 + lane;
-                    bool     full = skey[q] >= 0;
-                    unsigned bal  = __ballot_sync(0xffffffffu, full);
-                    if(full)
-                        sk[n + __popc(bal & ((1u << lane) - 1u))] = make_key(skey[q], (int)q);
+                    const int      q    = q0 + lane;
+                    const bool     fill = sm.key[q] >= 0;
+                    const unsigned bal  = __ballot_sync(full, fill);
+                    if(fill)
+                        sm.sk[n + __popc(bal & ((1u << lane) - 1u))] = make_key(sm.key[q], q);
                     n += __popc(bal);
                 }
                 __syncwarp();
-                bitonic_sort<grp_warp>(sk, n);
+                bitonic_sort<grp_warp>(sm.sk, n);
                 const int32_t o = out_rp[row];
                 for(int i = lane; i < n; i += 32)
                 {
-                    out_ci[o + i] = key_col(sk[i]);
-                    out_v[o + i]  = sval[key_pos(sk[i])];
+                    out_ci[o + i] = key_col(sm.sk[i]);
+                    out_v[o + i]  = sm.val[key_pos(sm.sk[i])];
                 }
             }
             __syncwarp();
         }
     }
 
-    // Split row ids by item count: rows with ub <= 256 to `small`, others to `big`.
-    __global__ void k_split_rows(const int32_t* __restrict__ upper, int64_t m, int32_t* small,
-                                 int32_t* big, int* cnt)
+    // Row classes.  Symbolic (by the product bound ub): 0 = lane tier (ub <= 32),
+    // 1..6 = hash tables of 128..4096 slots (ub <= slots / 2; class 6 takes every
+    // larger row and checks for overflow).  Numeric (by the exact column count of
+    // rows with ub > 32): 1..6 = tables of 64..2048 slots (count <= slots / 2),
+    // 7 = global sort tier.
+    __device__ __forceinline__ int gemm_class(int phase, int ub, int cnt)
     {
-        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
-            i += (int64_t)gridDim.x * blockDim.x)
+        if(ub <= kEscLaneCap)
+            return 0;
+        if(phase == 0)
         {
-            if(upper[i] <= kEscWarpCap)
-                small[atomicAdd(&cnt[0], 1)] = (int32_t)i;
-            else
-                big[atomicAdd(&cnt[1], 1)] = (int32_t)i;
+            int c = 1, hs = 128;
+            while(c < 6 && 2 * ub > hs)
+            {
+                c++;
+                hs <<= 1;
+            }
+            return c;
+        }
+        if(cnt > 1024)
+            return 7;
+        int c = 1, hs = 64;
+        while(2 * cnt > hs)
+        {
+            c++;
+            hs <<= 1;
+        }
+        return c;
+    }
+
+    __global__ void k_gemm_class_count(int phase, const int32_t* __restrict__ upper,
+                                       const int32_t* __restrict__ rp, int64_t m, int* hist)
+    {
+        __shared__ int sh[kHashClasses];
+        if(threadIdx.x < kHashClasses)
+            sh[threadIdx.x] = 0;
+        __syncthreads();
+        for(int64_t base = blockIdx.x * (int64_t)blockDim.x; base < m;
+            base += (int64_t)gridDim.x * blockDim.x)
+        {
+            const int64_t i = base + threadIdx.x;
+            int           c = -1;
+            if(i < m)
+                c = gemm_class(phase, upper[i], rp ? rp[i + 1] - rp[i] : 0);
+            warp_append(sh, c, kHashClasses);
+        }
+        __syncthreads();
+        if(threadIdx.x < kHashClasses && sh[threadIdx.x])
+            atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+    }
+
+    __global__ void k_gemm_class_fill(int phase, const int32_t* __restrict__ upper,
+                                      const int32_t* __restrict__ rp, int64_t m, int* cursor,
+                                      int32_t* rows)
+    {
+        for(int64_t base = blockIdx.x * (int64_t)blockDim.x; base < m;
+            base += (int64_t)gridDim.x * blockDim.x)
+        {
+            const int64_t i = base + threadIdx.x;
+            int           c = -1;
+            if(i < m)
+                c = gemm_class(phase, upper[i], rp ? rp[i + 1] - rp[i] : 0);
+            const int p = warp_append(cursor, c, kHashClasses);
+            if(c >= 0)
+                rows[p] = (int32_t)i;
         }
     }
 
-    // Numeric routing of the big rows: exact count <= kHashNumMaxCnt -> hash, else sort.
-    __global__ void k_split_numeric(const int32_t* __restrict__ big, int nbig,
-                                    const int32_t* __restrict__ rp, int32_t* hash_rows,
-                                    int32_t* sort_rows, int* cnt)
+    // Rows grouped by class: rows[start[c] .. start[c + 1]).
+    struct gemm_classes
     {
-        for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nbig; i += gridDim.x * blockDim.x)
+        dbuf<int32_t> rows;
+        int           start[kHashClasses + 1] = {};
+        int           count(int c) const
         {
-            int row = big[i];
-            if(rp[row + 1] - rp[row] <= kHashNumMaxCnt)
-                hash_rows[atomicAdd(&cnt[0], 1)] = row;
-            else
-                sort_rows[atomicAdd(&cnt[1], 1)] = row;
+            return start[c + 1] - start[c];
         }
+        const int32_t* of(int c) const
+        {
+            return rows.get() + start[c];
+        }
+    };
+
+    static lab_status gemm_classify(int phase, const int32_t* upper, const int32_t* rp, int64_t m,
+                                    gemm_classes& g, cudaStream_t s)
+    {
+        dbuf<int> cnt;
+        LAB_TRY(cnt.alloc(2 * kHashClasses, s));
+        LAB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * kHashClasses, s));
+        const unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(m, 256), 4096);
+        LAB_LAUNCH(k_gemm_class_count, grid, 256, 0, s, phase, upper, rp, m, cnt.get());
+        int h[kHashClasses];
+        LAB_TRY(copy_d2h_sync(h, cnt.get(), sizeof(h), s));
+        for(int c = 0; c < kHashClasses; c++)
+            g.start[c + 1] = g.start[c] + h[c];
+        LAB_CUDA(cudaMemcpyAsync(cnt.get() + kHashClasses, g.start, sizeof(int) * kHashClasses,
+                                 cudaMemcpyHostToDevice, s));
+        LAB_TRY(g.rows.alloc((size_t)m + 1, s));
+        LAB_LAUNCH(k_gemm_class_fill, grid, 256, 0, s, phase, upper, rp, m,
+                   cnt.get() + kHashClasses, g.rows.get());
+        return LAB_OK;
+    }
+
+    template <int MODE, int HS, int WARPS>
+    static lab_status launch_hash_cls(csr_ref Ar, csr_ref Br, const int32_t* rows, int n,
+                                      int32_t* counts, const int32_t* out_rp, int32_t* out_ci,
+                                      double* out_v, int32_t* ovf_rows, int* n_ovf, cudaStream_t s)
+    {
+        if(n == 0)
+            return LAB_OK;
+        constexpr size_t smem = sizeof(hash_smem<MODE, HS>) * WARPS;
+        static_assert(smem <= 227 * 1024, "hash table class exceeds shared memory");
+        static const cudaError_t attr = cudaFuncSetAttribute(
+            k_hash_gemm<MODE, HS, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        LAB_CUDA(attr);
+        static int occ = -1;
+        if(occ < 0)
+        {
+            int o = 0;
+            LAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &o, k_hash_gemm<MODE, HS, WARPS>, 32 * WARPS, smem));
+            occ = std::max(o, 1);
+        }
+        const unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(n, WARPS),
+                                                          (int64_t)num_sms() * occ);
+        LAB_LAUNCH((k_hash_gemm<MODE, HS, WARPS>), grid, 32 * WARPS, smem, s, Ar, Br, rows, n,
+                   counts, out_rp, out_ci, out_v, ovf_rows, n_ovf);
+        return LAB_OK;
+    }
+
+    // One launch per non-empty hash class (1..6) of the phase.
+    template <int MODE>
+    static lab_status launch_hash_classes(const gemm_classes& g, csr_ref Ar, csr_ref Br,
+                                          int32_t* counts, const int32_t* out_rp, int32_t* out_ci,
+                                          double* out_v, int32_t* ovf_rows, int* n_ovf,
+                                          cudaStream_t s)
+    {
+#define LAB_HASH_CLS(C, HS, W)                                                                    \
+    LAB_TRY((launch_hash_cls<MODE, HS, W>(Ar, Br, g.of(C), g.count(C), counts, out_rp, out_ci,    \
+                                          out_v, ovf_rows, n_ovf, s)))
+        if constexpr(MODE == 0)
+        {
+            LAB_HASH_CLS(1, 128, 8);
+            LAB_HASH_CLS(2, 256, 8);
+            LAB_HASH_CLS(3, 512, 8);
+            LAB_HASH_CLS(4, 1024, 8);
+            LAB_HASH_CLS(5, 2048, 8);
+            LAB_HASH_CLS(6, 4096, 4);
+        }
+        else
+        {
+            LAB_HASH_CLS(1, 64, 8);
+            LAB_HASH_CLS(2, 128, 8);
+            LAB_HASH_CLS(3, 256, 8);
+            LAB_HASH_CLS(4, 512, 8);
+            LAB_HASH_CLS(5, 1024, 4);
+            LAB_HASH_CLS(6, 2048, 4);
+        }
+#undef LAB_HASH_CLS
+        return LAB_OK;
     }
 
     __global__ void k_gsizes(const int32_t* __restrict__ rows, int n, const int32_t* __restrict__ upper,
@@ -456,7 +759,7 @@ namespace lab
     static lab_status tiers_for_rows(const int32_t* rows, int n, const int32_t* upper,
                                      esc_tiers& t, cudaStream_t s)
     {
-        t.nw = t.nb = 0;
+        t.nl = t.nw = t.nb = 0;
         t.ng = n;
         if(n == 0)
             return LAB_OK;
@@ -472,23 +775,16 @@ namespace lab
         return LAB_OK;
     }
 
-    template <int MODE>
-    static lab_status launch_hash(csr_ref Ar, csr_ref Br, const int32_t* rows, int n,
-                                  int32_t* counts, const int32_t* out_rp, int32_t* out_ci,
-                                  double* out_v, int32_t* ovf_rows, int* n_ovf, cudaStream_t s)
+    // Lane-tier rows as an ESC tier list.
+    static lab_status lane_tiers(const gemm_classes& g, esc_tiers& t, cudaStream_t s)
     {
-        if(n == 0)
+        t.nl = g.count(0);
+        t.nw = t.nb = t.ng = 0;
+        if(t.nl == 0)
             return LAB_OK;
-        const size_t per  = MODE == 0 ? (size_t)kHashSym * 4
-                                      : (size_t)kHashNum * 12 + (size_t)(kHashNum / 2) * 8;
-        const size_t smem = per * kHashWarps;
-        static const cudaError_t attr = cudaFuncSetAttribute(
-            k_hash_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        LAB_CUDA(attr);
-        unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(n, kHashWarps),
-                                                    (int64_t)num_sms() * 8);
-        LAB_LAUNCH(k_hash_gemm<MODE>, grid, 32 * kHashWarps, smem, s, Ar, Br, rows, n, counts,
-                   out_rp, out_ci, out_v, ovf_rows, n_ovf);
+        LAB_TRY(t.rows.alloc((size_t)t.nl, s));
+        LAB_CUDA(cudaMemcpyAsync(t.rows.get(), g.of(0), sizeof(int32_t) * t.nl,
+                                 cudaMemcpyDeviceToDevice, s));
         return LAB_OK;
     }
 
@@ -522,36 +818,24 @@ namespace lab
         if(m == 0)
             return esc_build(e, upper.get(), m, B->n, C, s);
 
-        // ---- tiers: <= 256 products: warp sort; more: warp hash; hash overflow: global sort
-        dbuf<int32_t> small, big, counts, ovf_rows, rp;
-        dbuf<int>     cnt;
-        LAB_TRY(small.alloc((size_t)m, s));
-        LAB_TRY(big.alloc((size_t)m, s));
+        // ---- symbolic: lane tier (<= 32 products), hash classes, overflow -> global sort
+        gemm_classes gs;
+        LAB_TRY(gemm_classify(0, upper.get(), nullptr, m, gs, s));
+        dbuf<int32_t> counts, ovf_rows, rp;
+        dbuf<int>     novf_d;
         LAB_TRY(counts.alloc((size_t)m + 1, s));
-        LAB_TRY(ovf_rows.alloc((size_t)m, s));
-        LAB_TRY(cnt.alloc(8, s));
-        LAB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * 8, s));
+        LAB_TRY(ovf_rows.alloc((size_t)std::max(gs.count(6), 1), s));
+        LAB_TRY(novf_d.alloc(1, s));
+        LAB_CUDA(cudaMemsetAsync(novf_d.get(), 0, sizeof(int), s));
         LAB_CUDA(cudaMemsetAsync(counts.get(), 0, sizeof(int32_t) * (m + 1), s));
-        unsigned g = (unsigned)std::min<int64_t>(ceil_div<int64_t>(m, 256), 4096);
-        LAB_LAUNCH(k_split_rows, g, 256, 0, s, (const int32_t*)upper.get(), m, small.get(),
-                   big.get(), cnt.get());
-        int hc[2];
-        LAB_TRY(copy_d2h_sync(hc, cnt.get(), sizeof(int) * 2, s));
-        const int nsmall = hc[0], nbig = hc[1];
-
-        esc_tiers ts;
-        ts.nw = nsmall;
-        if(nsmall)
-        {
-            LAB_TRY(ts.rows.alloc((size_t)nsmall, s));
-            LAB_CUDA(cudaMemcpyAsync(ts.rows.get(), small.get(), sizeof(int32_t) * nsmall,
-                                     cudaMemcpyDeviceToDevice, s));
-        }
-        LAB_TRY((esc_run<exp_gemm, 0>(e, m, ts, counts.get(), nullptr, nullptr, s)));
-        LAB_TRY(launch_hash<0>(Ar, Br, big.get(), nbig, counts.get(), nullptr, nullptr, nullptr,
-                               ovf_rows.get(), cnt.get() + 2, s));
+        esc_tiers tl;
+        LAB_TRY(lane_tiers(gs, tl, s));
+        LAB_TRY((esc_run<exp_gemm, 0>(e, m, tl, counts.get(), nullptr, nullptr, s)));
+        LAB_TRY(launch_hash_classes<0>(gs, Ar, Br, counts.get(), nullptr, nullptr, nullptr,
+                                       ovf_rows.get(), novf_d.get(), s));
         int novf = 0;
-        LAB_TRY(copy_d2h_sync(&novf, cnt.get() + 2, sizeof(int), s));
+        if(gs.count(6))
+            LAB_TRY(copy_d2h_sync(&novf, novf_d.get(), sizeof(int), s));
         if(novf)
         {
             esc_tiers tg;
@@ -570,36 +854,23 @@ namespace lab
                            cudaMemcpyDeviceToDevice, s) != cudaSuccess)
             st = LAB_CUDA_ERROR;
 
-        // ---- numeric
+        // ---- numeric: lane tier, hash classes by exact count, > 1024 columns -> sort
         exp_gemm e2 = e;
         e2.out_rp   = out->row_ptr;
+        gemm_classes gn;
         if(st == LAB_OK)
-            st = esc_run<exp_gemm, 1>(e2, m, ts, nullptr, out->col_ind, out->val, s);
-        dbuf<int32_t> hrows, srows;
-        if(st == LAB_OK && nbig)
+            st = esc_run<exp_gemm, 1>(e2, m, tl, nullptr, out->col_ind, out->val, s);
+        if(st == LAB_OK)
+            st = gemm_classify(1, upper.get(), out->row_ptr, m, gn, s);
+        if(st == LAB_OK)
+            st = launch_hash_classes<1>(gn, Ar, Br, nullptr, out->row_ptr, out->col_ind, out->val,
+                                        nullptr, nullptr, s);
+        if(st == LAB_OK && gn.count(7))
         {
-            st = hrows.alloc((size_t)nbig, s);
+            esc_tiers tg;
+            st = tiers_for_rows(gn.of(7), gn.count(7), upper.get(), tg, s);
             if(st == LAB_OK)
-                st = srows.alloc((size_t)nbig, s);
-            if(st == LAB_OK)
-            {
-                cudaMemsetAsync(cnt.get() + 4, 0, sizeof(int) * 2, s);
-                k_split_numeric<<<(unsigned)ceil_div(nbig, 256), 256, 0, s>>>(
-                    big.get(), nbig, out->row_ptr, hrows.get(), srows.get(), cnt.get() + 4);
-                g_launches.fetch_add(1);
-                int hn[2] = {0, 0};
-                st = copy_d2h_sync(hn, cnt.get() + 4, sizeof(int) * 2, s);
-                if(st == LAB_OK)
-                    st = launch_hash<1>(Ar, Br, hrows.get(), hn[0], nullptr, out->row_ptr,
-                                        out->col_ind, out->val, nullptr, nullptr, s);
-                if(st == LAB_OK && hn[1])
-                {
-                    esc_tiers tg;
-                    st = tiers_for_rows(srows.get(), hn[1], upper.get(), tg, s);
-                    if(st == LAB_OK)
-                        st = esc_run<exp_gemm, 1>(e2, m, tg, nullptr, out->col_ind, out->val, s);
-                }
-            }
+                st = esc_run<exp_gemm, 1>(e2, m, tg, nullptr, out->col_ind, out->val, s);
         }
         if(st != LAB_OK)
         {

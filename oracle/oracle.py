@@ -448,14 +448,20 @@ class ReferenceHierarchy:
         return x, it
 
 
-def gmres_restated(A, b, restart, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000, x0=None):
+def gmres_restated(A, b, restart, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000, x0=None,
+                   precond=None):
     """Unpreconditioned restarted GMRES as the reference runs it
     (library/src/iterative_solvers/krylov/gmres.cpp:224-368): modified Gram-Schmidt
     Arnoldi (93-161), Givens rotations (163-199), 2-norm stopping test relative to
     the initial residual, back substitution, restart from the true residual.
     Returns (x, restart cycles).  The reference's own gmres_solver::build leaves
     its residual vectors unsized (gmres.cpp:211-220), so its solve writes out of
-    bounds; this restatement is the checker instead."""
+    bounds; this restatement is the checker instead.
+
+    With ``precond`` (a callable z = M^-1 r): left preconditioning as
+    gmres_solver::solve_precond states it (gmres.cpp:370-523): the stopping test
+    and the Arnoldi basis use z = M^-1 (b - A x) and M^-1 A q (arnoldi,
+    gmres.cpp:112-129, whose preconditioned output this restatement uses)."""
     rp, ci, v = (np.asarray(a) for a in A[:3])
     n = rp.size - 1
     rows = np.repeat(np.arange(n), np.diff(rp))
@@ -471,7 +477,9 @@ def gmres_restated(A, b, restart, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000, x0=
             return False
         return rn <= abs_tol or rn / r0 <= rel_tol
 
-    r = b - mv(x)
+    M = precond if precond is not None else (lambda r: r)
+    op = (lambda q: M(mv(q))) if precond is not None else mv
+    r = M(b - mv(x))
     rn = np.linalg.norm(r)
     r0 = rn
     if conv(rn, r0):
@@ -487,7 +495,7 @@ def gmres_restated(A, b, restart, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000, x0=
         g[0] = rn
         k = 1
         while k <= restart:
-            w = mv(Q[k - 1])
+            w = op(Q[k - 1])
             for i in range(k):
                 H[i, k - 1] = np.dot(Q[i], w)
                 w = w - H[i, k - 1] * Q[i]
@@ -524,7 +532,7 @@ def gmres_restated(A, b, restart, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000, x0=
                 y[i] -= H[i, j] * y[j]
             y[i] /= H[i, i]
         x = x + Q[:k].T @ y
-        r = b - mv(x)
+        r = M(b - mv(x))
         rn = np.linalg.norm(r)
         if conv(rn, r0):
             break
