@@ -52,14 +52,19 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=128, help="grid side of the 3D Poisson system")
+    ap.add_argument("--n", type=int, default=None,
+                    help="grid side (default: 128 for the Poisson step, 160 for mixed, "
+                         "96 for adjoint, 64 for the multi-RHS batch)")
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="full", choices=["full", "profile", "spmv"],
+    ap.add_argument("--mode", default="full",
+                    choices=["full", "profile", "spmv", "mixed", "batched", "adjoint"],
                     help="profile: only the warm-up and timed device-resident steps (the "
                          "command the ncu launch lists in profiles/ are taken from); "
                          "spmv: only the standalone level-0 SpMV timing (5 warm-up launches, "
-                         "then 30 timed ones, each after an L2 flush)")
+                         "then 3 x 20 timed back-to-back launches); mixed / batched / "
+                         "adjoint: the mixed-precision, batched and adjoint workloads "
+                         "(one JSON line each, not the driver's bench line)")
     return ap.parse_args()
 
 
@@ -260,28 +265,31 @@ def run_reference(args, d):
 
 # ------------------------------------------------------------------ our arm
 def dominant_kernel_roofline(core, dA, m, nnz, torch):
-    """Standalone CUDA-event timing of the dominant kernel class (level-0 CSR pass:
-    SpMV on the 128^3 operator, the same row engine as the smoother kernels)."""
+    """CUDA-event timing of the dominant kernel class (level-0 CSR pass: SpMV on
+    the 128^3 operator, the same row engine as the smoother kernels): 20 launches
+    back to back between two events on the launching stream, three times; A_0
+    (217 MB) is larger than L2, so every launch streams it from HBM."""
     x = torch.empty(m, dtype=torch.float64, device="cuda").uniform_(-1, 1)
     y = torch.zeros(m, dtype=torch.float64, device="cuda")
-    flush = torch.empty(160 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
     for _ in range(5):
         dA.spmv(x, y)
     times = []
-    for _ in range(30):
-        flush.fill_(0.0)  # evict L2 (126 MB) between launches
+    reps = 20
+    for _ in range(3):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
         e0.record(stream)
-        dA.spmv(x, y)
+        for _ in range(reps):
+            dA.spmv(x, y)
         e1.record(stream)
         torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1) * 1e-3)
+        times.append(e0.elapsed_time(e1) * 1e-3 / reps)
     t = statistics.median(times)
     algo = spmv_bytes(m, m, nnz)
     achieved = algo / t / 1e9
-    peak, which = 6547.2, "fallback"
+    peak, which = 6650.0, "fallback"
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             peak, which = float(json.load(f)["hbm_gbs"]), "measured"
@@ -293,7 +301,7 @@ def dominant_kernel_roofline(core, dA, m, nnz, torch):
         mt = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(prof).read())
         if mt:
             traffic = float(mt.group(1))
-    return {"bound": "hbm", "kernel": "k_rowseq<op_spmv> on A_0 (level-0 CSR pass)",
+    return {"bound": "hbm", "kernel": "k_pipe<op_spmv, 256, 8> on A_0 (level-0 CSR pass)",
             "achieved": achieved, "peak": peak, "peak_source": which, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": algo,
             "launch_us": t * 1e6}
@@ -448,11 +456,233 @@ def run_ours(args, d):
     return 0
 
 
+# ------------------------------------------------------------------ extra workloads
+def _events_ms(torch, fn, reps):
+    """Median CUDA-event time (ms) of fn() over reps runs (after the caller's warm-up)."""
+    stream = torch.cuda.current_stream()
+    out = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return statistics.median(out), out
+
+
+def _rel_res(torch, dA, x, b):
+    r = dA.residual(x, b)
+    return float(torch.max(torch.abs(r)) / torch.max(torch.abs(b)))
+
+
+def run_mixed(args, d):
+    """27-point variable-coefficient diffusion (lognormal sigma 1.5, z x100) on an
+    n^3 grid: one FP64 SA hierarchy, PCG (omega 2/3) with the FP64, FP32 and
+    FP32+BF16 cycles to rtol 1e-8 and 1e-10; error of each against the FP64 solve."""
+    import torch
+    d.init(need_gpu=True)
+    import linalglib_b200.core as core
+    from linalglib_b200 import _lib as L
+    from linalglib_b200 import problems as P
+    core.init()
+    n = args.n or 160
+    A = P.diffusion27(n, sigma=1.5, zscale=100.0, seed=0)
+    b, xt = P.rhs_from_solution(*A, seed=0)
+    dA = core.CsrMatrix.from_arrays(*A)
+    dA.analyse()
+    bd = core.vec(b)
+    xtd = core.vec(xt)
+    t_setup, _ = _events_ms(torch, lambda: core.Hierarchy(dA), 1)
+    H = core.Hierarchy(dA)
+    res = {"mode": "mixed", "config": {"workload": f"SA-AMG-PCG, 27-point diffusion {n}^3 "
+                                                  "(lognormal sigma 1.5, z x100), omega 2/3",
+                                       "rows": int(A[0].size - 1), "nnz": int(A[2].size),
+                                       "levels": H.levels},
+           "setup_ms": t_setup, "runs": []}
+    names = {L.PREC_FP64: "fp64", L.PREC_FP32: "fp32", L.PREC_FP32_BF16: "fp32+bf16"}
+    for rtol in (1e-8, 1e-10):
+        ctl = core.iter_control(rel_tol=rtol, abs_tol=0.0, max_iter=1000)
+        x64 = None
+        for prec in (L.PREC_FP64, L.PREC_FP32, L.PREC_FP32_BF16):
+            M = core.Preconditioner.amg(H, core.amg_options(omega=2.0 / 3.0, precision=prec))
+            x = torch.zeros_like(bd)
+            core.pcg(dA, bd, x=x, M=M, control=ctl)  # warm-up: value copies, graph capture
+            info = []
+
+            def solve():
+                x.zero_()
+                info.append(core.pcg(dA, bd, x=x, M=M, control=ctl)[1])
+            t, ts = _events_ms(torch, solve, max(3, args.steps))
+            if prec == L.PREC_FP64:
+                x64 = x.clone()
+            err64 = float(torch.max(torch.abs(x - x64)) / torch.max(torch.abs(x64)))
+            res["runs"].append({
+                "rtol": rtol, "precision": names[prec], "solve_ms": t, "solve_ms_all": ts,
+                "iterations": info[-1].iterations, "converged": bool(info[-1].converged),
+                "true_rel_residual": _rel_res(torch, dA, x, bd),
+                "err_vs_fp64_solve": err64,
+                "err_vs_x_true": float(torch.max(torch.abs(x - xtd)))})
+        base = [r for r in res["runs"] if r["rtol"] == rtol and r["precision"] == "fp64"][0]
+        for r in res["runs"]:
+            if r["rtol"] == rtol:
+                r["speedup_vs_fp64"] = base["solve_ms"] / r["solve_ms"]
+    if d.rank == 0:
+        print(json.dumps(res), flush=True)
+    d.close()
+    return 0
+
+
+def run_batched(args, d):
+    """(a) 256 2D 5-point Poisson systems, sides ~U{32..256} (seed 0), stacked block
+    diagonally, one hierarchy, one segmented PCG (per-system convergence mask) to
+    rtol 1e-8; against solving the systems one after another.  (b) 32 right-hand
+    sides ~U[-1,1] on the 3D 7-point n^3 operator by block PCG; against 32 solves."""
+    import torch
+    d.init(need_gpu=True)
+    import linalglib_b200.core as core
+    from linalglib_b200 import problems as P
+    core.init()
+    rng = np.random.default_rng(0)
+    sides = rng.integers(32, 257, size=256)
+    mats = [P.poisson2d(int(s)) for s in sides]
+    blocks = [core.CsrMatrix.from_arrays(*A) for A in mats]
+    S, offs = core.block_diag(blocks)
+    S.analyse()
+    bs = np.concatenate([P.rhs_from_solution(*A, seed=k)[0] for k, A in enumerate(mats)])
+    bd = core.vec(bs)
+    ctl = core.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=1000)
+    t_setup, _ = _events_ms(torch, lambda: core.Hierarchy(S), 1)
+    H = core.Hierarchy(S)
+    M = core.Preconditioner.amg(H, core.amg_options(omega=2.0 / 3.0))
+    x = torch.zeros_like(bd)
+    out = {}
+
+    def batched():
+        x.zero_()
+        out["r"] = core.batched_pcg(S, offs, bd, M, x=x, control=ctl)
+    batched()
+    t_b, _ = _events_ms(torch, batched, max(3, args.steps))
+    _, iters, conv, _ = out["r"]
+    # one system at a time, each with its own hierarchy (setup excluded from the time)
+    singles = []
+    for k, Ak in enumerate(blocks):
+        Hk = core.Hierarchy(Ak)
+        singles.append((Ak, Hk, core.Preconditioner.amg(Hk, core.amg_options(omega=2.0 / 3.0)),
+                        bd[int(offs[k]):int(offs[k + 1])].contiguous()))
+
+    def one_by_one():
+        for Ak, Hk, Mk, bk in singles:
+            core.pcg(Ak, bk, M=Mk, control=ctl)
+    one_by_one()
+    t_s, _ = _events_ms(torch, one_by_one, 3)
+    res = {"mode": "batched", "systems": {
+        "workload": "256 2D 5-point Poisson systems, sides U{32..256} seed 0",
+        "rows": int(offs[-1]), "setup_ms": t_setup, "solve_ms": t_b,
+        "one_by_one_ms": t_s, "speedup": t_s / t_b, "iterations_max": int(iters.max()),
+        "iterations_min": int(iters.min()), "all_converged": bool(conv.all())}}
+    # (b) multi-RHS
+    n = args.n or 64
+    A = P.poisson3d(n)
+    dA = core.CsrMatrix.from_arrays(*A)
+    dA.analyse()
+    H2 = core.Hierarchy(dA)
+    M2 = core.Preconditioner.amg(H2, core.amg_options(omega=2.0 / 3.0))
+    B = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, size=(32, A[0].size - 1))).cuda()
+    X = torch.zeros_like(B)
+
+    def multi():
+        X.zero_()
+        out["m"] = core.multi_rhs_pcg(dA, B, M2, X=X, control=ctl)
+    multi()
+    t_m, _ = _events_ms(torch, multi, max(3, args.steps))
+    _, it2, conv2, _ = out["m"]
+    cols = [B[k].contiguous() for k in range(32)]
+
+    def per_rhs():
+        for bk in cols:
+            core.pcg(dA, bk, M=M2, control=ctl)
+    per_rhs()
+    t_p, _ = _events_ms(torch, per_rhs, 3)
+    res["multi_rhs"] = {"workload": f"32 RHS U[-1,1] on 3D 7-point {n}^3", "solve_ms": t_m,
+                        "one_by_one_ms": t_p, "speedup": t_p / t_m,
+                        "iterations_max": int(it2.max()), "all_converged": bool(conv2.all())}
+    if d.rank == 0:
+        print(json.dumps(res), flush=True)
+    d.close()
+    return 0
+
+
+def run_adjoint(args, d):
+    """Weighted 7-point graph Laplacian (lognormal sigma 1, shift 1e-3) on n^3:
+    forward SA-AMG-PCG to 1e-10, adjoint solve lambda = A^-T (x - x_target), and
+    dL/dA on the pattern; a central finite difference along b checks dL/db."""
+    import torch
+    d.init(need_gpu=True)
+    import linalglib_b200.core as core
+    from linalglib_b200 import problems as P
+    core.init()
+    n = args.n or 96
+    A = P.graph_laplacian3d(n, sigma=1.0, shift=1e-3, seed=0)
+    b, _ = P.rhs_from_solution(*A, seed=0)
+    xt = core.vec(np.random.default_rng(1).standard_normal(A[0].size - 1))
+    dA = core.CsrMatrix.from_arrays(*A)
+    dA.analyse()
+    bd = core.vec(b)
+    ctl = core.iter_control(rel_tol=1e-10, abs_tol=0.0, max_iter=2000)
+    t_setup, _ = _events_ms(torch, lambda: core.Hierarchy(dA), 1)
+    H = core.Hierarchy(dA)
+    M = core.Preconditioner.amg(H, core.amg_options(omega=2.0 / 3.0))
+    st = {}
+
+    def forward():
+        st["x"], st["fi"] = core.pcg(dA, bd, M=M, control=ctl)
+
+    def backward():
+        g = st["x"] - xt
+        st["lam"], st["ai"] = core.adjoint_solve(dA, g, M=M, symmetric=True, control=ctl)
+        st["gA"] = core.adjoint_grad_A(dA, st["lam"], st["x"])
+    forward()
+    backward()
+    t_f, _ = _events_ms(torch, forward, max(3, args.steps))
+    t_b, _ = _events_ms(torch, backward, max(3, args.steps))
+    # directional check of dL/db = lambda along a random direction
+    v = torch.from_numpy(np.random.default_rng(2).standard_normal(A[0].size - 1)).cuda()
+    h = 1e-4
+
+    def loss(bb):
+        xx, _ = core.pcg(dA, bb.contiguous(), M=M, control=ctl)
+        return 0.5 * float(torch.sum((xx - xt) ** 2))
+    fd = (loss(bd + h * v) - loss(bd - h * v)) / (2 * h)
+    an = float(torch.dot(st["lam"], v))
+    res = {"mode": "adjoint", "config": {"workload": f"graph Laplacian {n}^3 (lognormal sigma 1, "
+                                                     "shift 1e-3), rtol 1e-10",
+                                         "rows": int(A[0].size - 1), "nnz": int(A[2].size)},
+           "setup_ms": t_setup, "forward_ms": t_f, "adjoint_ms": t_b,
+           "forward_iterations": st["fi"].iterations, "adjoint_iterations": st["ai"].iterations,
+           "dLdb_directional": {"adjoint": an, "finite_difference": fd,
+                                "rel_diff": abs(an - fd) / max(abs(fd), 1e-300)}}
+    if d.rank == 0:
+        print(json.dumps(res), flush=True)
+    d.close()
+    return 0
+
+
 def main():
     args = parse()
     d = Dist()
     if args.impl == "reference":
+        args.n = args.n or 128
         return run_reference(args, d)
+    if args.mode == "mixed":
+        return run_mixed(args, d)
+    if args.mode == "batched":
+        return run_batched(args, d)
+    if args.mode == "adjoint":
+        return run_adjoint(args, d)
+    args.n = args.n or 128
     return run_ours(args, d)
 
 

@@ -48,6 +48,13 @@ namespace linalg
         SSOR
     };
 
+    // Write the levels of a built hierarchy to a file / load them back onto the
+    // device (bit-identical), so a rerun on the same operator skips the setup.
+    // No counterpart in the reference.  Return false on failure (the reason is
+    // printed, as the reference reports its errors).
+    bool save_hierarchy(const hierarchy& h, const char* path);
+    bool load_hierarchy(const char* path, hierarchy& h);
+
     // amg.h:411-418.  Returns the number of cycles (amg.cpp:570).
     int amg_solve(const hierarchy&      hierarchy,
                   vector<double>&       x,

@@ -117,6 +117,14 @@ LAB_API lab_status lab_spmv_analysis(lab_csr A, lab_stream s);
 /* Force an algorithm (LAB_SPMV_AUTO restores the analysed choice). */
 LAB_API lab_status lab_spmv_set_algorithm(lab_csr A, lab_spmv_alg alg, int lanes);
 LAB_API lab_status lab_spmv_get_algorithm(lab_csr A, int* alg, int* lanes);
+/* Autotuner: time every candidate SpMV schedule on this matrix (one thread per
+ * row, and unless `exact` W = 2..32 lanes per row) and keep the fastest; the
+ * winner's time per SpMV in microseconds goes to *best_us (may be NULL).  With
+ * exact != 0 only schedules that accumulate in CSR order (bit-identical to the
+ * reference, host_matrix_vector.cpp:60-84) are candidates.  No counterpart in the
+ * reference, which rebuilds a fixed descriptor per call (csr_matrix.cpp:307-314).
+ * A solver iteration graph already captured on A is dropped and re-captured. */
+LAB_API lab_status lab_spmv_autotune(lab_csr A, int exact, double* best_us, lab_stream s);
 /* y = alpha*A*x + beta*y (beta == 0: y is not read).
  * Replaces csrmv_solve (library/include/linalg_math.h:304-310) and
  * csr_matrix::multiply_by_vector(_and_add) (csr_matrix.cpp:303-330). */
@@ -241,6 +249,19 @@ LAB_API lab_status lab_hierarchy_level(lab_hierarchy h, int level, lab_csr* A, l
                                        lab_csr* R);
 /* Setup timing of the last lab_amg_setup on this hierarchy, milliseconds. */
 LAB_API lab_status lab_hierarchy_setup_ms(lab_hierarchy h, double* ms);
+/* Write a built hierarchy (every A_l, P_l, R_l) to a binary file, and load one
+ * back onto the device: a loaded hierarchy is bit-identical to the saved one, so
+ * reruns on the same operator skip the setup.  No counterpart in the reference
+ * (its hierarchy exists only in memory, amg.h:65-144); the next-row item "hierarchy
+ * (de)serialisation".  A file with a bad header, a checksum mismatch or levels
+ * whose shapes do not chain is rejected with LAB_BAD_ARG. */
+/* lab_spmv_autotune on every level operator, prolongation and restriction; the
+ * fused V-cycle passes run on the schedule chosen for their matrix.  Tune before
+ * creating preconditioners on h: iteration graphs captured earlier keep their
+ * schedules (their results stay correct). */
+LAB_API lab_status lab_hierarchy_autotune(lab_hierarchy h, int exact, lab_stream s);
+LAB_API lab_status lab_hierarchy_save(lab_hierarchy h, const char* path, lab_stream s);
+LAB_API lab_status lab_hierarchy_load(const char* path, lab_hierarchy* h, lab_stream s);
 
 /* ------------------------------------------------------------------ cycles */
 typedef enum lab_cycle

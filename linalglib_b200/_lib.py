@@ -99,6 +99,10 @@ _SIGS = {
     "lab_hierarchy_levels": [_p, C.POINTER(_i)],
     "lab_hierarchy_level": [_p, _i, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p)],
     "lab_hierarchy_setup_ms": [_p, C.POINTER(_d)],
+    "lab_spmv_autotune": [_p, _i, C.POINTER(_d), _p],
+    "lab_hierarchy_autotune": [_p, _i, _p],
+    "lab_hierarchy_save": [_p, C.c_char_p, _p],
+    "lab_hierarchy_load": [C.c_char_p, C.POINTER(_p), _p],
     "lab_amg_cycle": [_p, C.POINTER(AmgOptions), _p, _p, _p],
     "lab_amg_solve": [_p, C.POINTER(AmgOptions), _p, _p, C.POINTER(IterControl),
                       C.POINTER(SolveInfo), _p],

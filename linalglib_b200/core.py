@@ -121,6 +121,13 @@ class CsrMatrix:
         call("lab_spmv_set_algorithm", self.h, alg, lanes)
         self.analyse()
 
+    def autotune(self, exact=False):
+        """Time every SpMV schedule on this matrix and keep the fastest; returns
+        the winner's microseconds per SpMV."""
+        us = C.c_double()
+        call("lab_spmv_autotune", self.h, int(bool(exact)), C.byref(us), stream_handle())
+        return us.value
+
     def algorithm(self):
         a, w = C.c_int(), C.c_int()
         call("lab_spmv_get_algorithm", self.h, C.byref(a), C.byref(w))
@@ -227,10 +234,24 @@ def iter_control(rel_tol=1e-6, abs_tol=1e-6, max_iter=1000, max_cycle=200):
 
 # ---------------------------------------------------------------- AMG
 class Hierarchy:
-    def __init__(self, A: CsrMatrix, kind=L.AMG_SA, max_level=20, stream=None):
+    def __init__(self, A: CsrMatrix | None, kind=L.AMG_SA, max_level=20, stream=None):
         init()
         self.h = C.c_void_p()
-        call("lab_amg_setup", kind, A.h, max_level, C.byref(self.h), stream_handle(stream))
+        if A is not None:
+            call("lab_amg_setup", kind, A.h, max_level, C.byref(self.h), stream_handle(stream))
+
+    @classmethod
+    def load(cls, path, stream=None):
+        """A hierarchy written by save(), back on the device."""
+        H = cls(None)
+        call("lab_hierarchy_load", str(path).encode(), C.byref(H.h), stream_handle(stream))
+        return H
+
+    def autotune(self, exact=False):
+        call("lab_hierarchy_autotune", self.h, int(bool(exact)), stream_handle())
+
+    def save(self, path, stream=None):
+        call("lab_hierarchy_save", self.h, str(path).encode(), stream_handle(stream))
 
     def __del__(self):
         try:
@@ -280,7 +301,7 @@ class Hierarchy:
             x = torch.zeros_like(b)
         info = SolveInfo()
         call_solve("lab_amg_solve", self.h, C.byref(options), ptr(b), ptr(x), C.byref(control),
-             C.byref(info), stream_handle())
+                   C.byref(info), stream_handle())
         return x, info
 
 
@@ -323,7 +344,7 @@ def pcg(A: CsrMatrix, b, x=None, M: Preconditioner | None = None, control=None):
         x = torch.zeros_like(b)
     info = SolveInfo()
     call_solve("lab_pcg_solve", A.h, M.h if M is not None else None, ptr(b), ptr(x),
-         C.byref(control), C.byref(info), stream_handle())
+               C.byref(control), C.byref(info), stream_handle())
     return x, info
 
 
@@ -332,7 +353,7 @@ def pcg_host(A: CsrMatrix, b: np.ndarray, x: np.ndarray, M=None, control=None):
     control = control or iter_control()
     info = SolveInfo()
     call_solve("lab_pcg_solve_host", A.h, M.h if M is not None else None, ptr(b), ptr(x),
-         C.byref(control), C.byref(info), stream_handle())
+               C.byref(control), C.byref(info), stream_handle())
     return x, info
 
 
@@ -342,7 +363,7 @@ def gmres(A: CsrMatrix, b, x=None, M: Preconditioner | None = None, restart=30, 
         x = torch.zeros_like(b)
     info = SolveInfo()
     call_solve("lab_gmres_solve", A.h, M.h if M is not None else None, restart, ptr(b), ptr(x),
-         C.byref(control), C.byref(info), stream_handle())
+               C.byref(control), C.byref(info), stream_handle())
     return x, info
 
 
@@ -353,8 +374,8 @@ def adjoint_solve(A: CsrMatrix, g, M: Preconditioner | None = None, symmetric=Tr
     if lam is None:
         lam = torch.zeros_like(g)
     info = SolveInfo()
-    call_solve("lab_adjoint_solve", A.h, M.h if M is not None else None, int(bool(symmetric)), ptr(g),
-         ptr(lam), C.byref(control), C.byref(info), stream_handle())
+    call_solve("lab_adjoint_solve", A.h, M.h if M is not None else None, int(bool(symmetric)),
+               ptr(g), ptr(lam), C.byref(control), C.byref(info), stream_handle())
     return lam, info
 
 
@@ -385,8 +406,8 @@ def batched_pcg(A: CsrMatrix, offsets, b, M: Preconditioner, x=None, control=Non
     iters = (C.c_int * nsys)()
     conv = (C.c_int * nsys)()
     info = SolveInfo()
-    call_solve("lab_batched_pcg_solve", A.h, M.h, nsys, offs, ptr(b), ptr(x), C.byref(control), iters,
-         conv, C.byref(info), stream_handle())
+    call_solve("lab_batched_pcg_solve", A.h, M.h, nsys, offs, ptr(b), ptr(x), C.byref(control),
+               iters, conv, C.byref(info), stream_handle())
     return x, np.array(iters[:]), np.array(conv[:]), info
 
 
@@ -399,6 +420,6 @@ def multi_rhs_pcg(A: CsrMatrix, B, M: Preconditioner, X=None, control=None):
     iters = (C.c_int * k)()
     conv = (C.c_int * k)()
     info = SolveInfo()
-    call_solve("lab_multi_rhs_pcg_solve", A.h, M.h, k, ptr(B), ptr(X), C.byref(control), iters, conv,
-         C.byref(info), stream_handle())
+    call_solve("lab_multi_rhs_pcg_solve", A.h, M.h, k, ptr(B), ptr(X), C.byref(control), iters,
+               conv, C.byref(info), stream_handle())
     return X, np.array(iters[:]), np.array(conv[:]), info

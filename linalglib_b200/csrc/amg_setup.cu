@@ -97,15 +97,17 @@ namespace lab
     }
 
     // One round of host_find_maximum_distance_two_node (host_amg_aggregation.cpp:95-180).
-    // Reads the round's snapshot `st`, writes max_state / agg for its own row only,
-    // so the parallel round equals the sequential one.  The lexicographic maximum
-    // replaces the running winner only on a strictly larger (state, hash), so the
-    // CSR scan order decides ties exactly as in the reference (lines 77-93).
+    // Reads the round's snapshot `st`, writes the row's new state to `out` (the
+    // other buffer of a ping-pong pair; unchanged rows are copied through) and
+    // agg for its own row only, so the parallel round equals the sequential one.
+    // The lexicographic maximum replaces the running winner only on a strictly
+    // larger (state, hash), so the CSR scan order decides ties exactly as in the
+    // reference (lines 77-93).
     // Rounds after the first complete one return at once (amg_aggregation.cpp:154).
     __global__ void k_pmis_round(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                  const int32_t* __restrict__ conn, int64_t m,
                                  const int32_t* __restrict__ st, const int32_t* __restrict__ hash,
-                                 int32_t* __restrict__ max_state, int64_t* __restrict__ agg,
+                                 int32_t* __restrict__ out, int64_t* __restrict__ agg,
                                  int32_t* flags, int round)
     {
         if(round > 0 && flags[round - 1] == 0)
@@ -139,47 +141,64 @@ namespace lab
                 br = c;
             }
         }
-        if(st[i] == 0)
+        int ns = st[i];
+        if(ns == 0)
         {
             if(br == i)
             {
-                max_state[i] = 1;
-                agg[i]       = 1;
+                ns     = 1;
+                agg[i] = 1;
             }
             else if(bs == 1)
             {
-                max_state[i] = -1;
-                agg[i]       = 0;
+                ns     = -1;
+                agg[i] = 0;
             }
             else
                 flags[round] = 1;
         }
+        out[i] = ns;
     }
 
-    // host_add_unassigned_nodes_to_closest_aggregation (host_amg_aggregation.cpp:182-221)
+    // Rounds that ran: round r runs iff r == 0 or round r-1 left a row undecided.
+    __device__ __forceinline__ int pmis_rounds_run(const int32_t* flags)
+    {
+        int k = 1;
+        while(k < 20 && flags[k - 1] != 0)
+            k++;
+        return k;
+    }
+
+    // host_add_unassigned_nodes_to_closest_aggregation (host_amg_aggregation.cpp:182-221),
+    // pass k of 2.  The rounds left the state in buffer (K & 1) of the pair
+    // {b0, b1} (K = rounds run); pass k reads buffer (K + k) & 1 and writes the other.
     __global__ void k_pmis_attach(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                  const int32_t* __restrict__ conn, int64_t m,
-                                  const int32_t* __restrict__ st, int32_t* __restrict__ max_state,
+                                  const int32_t* __restrict__ conn, int64_t m, int32_t* b0,
+                                  int32_t* b1, const int32_t* __restrict__ flags, int k,
                                   int64_t* __restrict__ agg)
     {
         int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
         if(i >= m)
             return;
-        int s = st[i];
+        const int      sel = (pmis_rounds_run(flags) + k) & 1;
+        const int32_t* st  = sel ? b1 : b0;
+        int32_t*       out = sel ? b0 : b1;
+        int            s   = st[i];
         if(s == -1)
         {
             for(int j = rp[i]; j < rp[i + 1]; j++)
             {
                 if(conn[j] == 1 && st[ci[j]] == 1)
                 {
-                    agg[i]       = agg[ci[j]];
-                    max_state[i] = 1;
+                    agg[i] = agg[ci[j]];
+                    s      = 1;
                     break;
                 }
             }
         }
         else if(s == -2)
             agg[i] = -2;
+        out[i] = s;
     }
 
     __global__ void k_count_rounds(const int32_t* flags, int* out)
@@ -217,13 +236,12 @@ namespace lab
         LAB_CUDA(cudaMemsetAsync(flags.get(), 0, sizeof(int32_t) * 24, s));
         const unsigned g = (unsigned)ceil_div<int64_t>(m, 256);
         LAB_LAUNCH(k_pmis_init, g, 256, 0, s, A->row_ptr, conn, m, state.get(), hash.get(), agg);
+        // ping-pong: round r reads buffer r & 1 of {state, snap} and writes the other
+        int32_t* buf[2] = {state.get(), snap.get()};
         for(int r = 0; r < 20; r++)
-        {
-            LAB_CUDA(cudaMemcpyAsync(snap.get(), state.get(), sizeof(int32_t) * m,
-                                     cudaMemcpyDeviceToDevice, s));
-            LAB_LAUNCH(k_pmis_round, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m, snap.get(),
-                       hash.get(), state.get(), agg, flags.get(), r);
-        }
+            LAB_LAUNCH(k_pmis_round, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                       (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg, flags.get(),
+                       r);
         if(rounds)
         {
             dbuf<int> d;
@@ -235,12 +253,8 @@ namespace lab
             LAB_LAUNCH(k_pmis_roots, g, 256, 0, s, (const int64_t*)agg, m, roots);
         LAB_TRY(scan_i64(agg, m, s));
         for(int k = 0; k < 2; k++)
-        {
-            LAB_CUDA(cudaMemcpyAsync(snap.get(), state.get(), sizeof(int32_t) * m,
-                                     cudaMemcpyDeviceToDevice, s));
-            LAB_LAUNCH(k_pmis_attach, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m, snap.get(),
-                       state.get(), agg);
-        }
+            LAB_LAUNCH(k_pmis_attach, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m, state.get(),
+                       snap.get(), (const int32_t*)flags.get(), k, agg);
         return LAB_OK;
     }
 

@@ -974,6 +974,25 @@ namespace linalg
         setup(LAB_AMG_RS, A, max_level, h);
     }
 
+    bool save_hierarchy(const hierarchy& h, const char* path)
+    {
+        if(!h.device)
+        {
+            std::cerr << "Error: save_hierarchy: the hierarchy has not been set up" << std::endl;
+            return false;
+        }
+        return ok(lab_hierarchy_save(h.device.get(), path, nullptr), "save_hierarchy");
+    }
+
+    bool load_hierarchy(const char* path, hierarchy& h)
+    {
+        lab_hierarchy hh = nullptr;
+        if(!ok(lab_hierarchy_load(path, &hh, nullptr), "load_hierarchy"))
+            return false;
+        h.adopt(hh);
+        return true;
+    }
+
     static lab_amg_options make_options(int n1, int n2, cycle c, smoother s, double omega)
     {
         lab_amg_options o;

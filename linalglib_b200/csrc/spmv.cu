@@ -25,11 +25,11 @@ namespace lab
         return w;
     }
 
-    // Schedule choice from row statistics.  Short, bounded rows (stencils) take
-    // the staged thread-per-row kernel, whose fma order matches the reference's
-    // host SpMV bit for bit; longer rows take W lanes per row with W the power of
-    // two nearest a third of the mean row length, which keeps >= 80 % of the lanes
-    // busy on the last stride.
+    // Schedule choice from row statistics.  Short, bounded rows (stencils up to
+    // 27 points: at most 32 entries) take the staged thread-per-row kernel, whose
+    // fma order matches the reference's host SpMV bit for bit; longer rows take W
+    // lanes per row with W the power of two nearest a third of the mean row
+    // length, which keeps >= 80 % of the lanes busy on the last stride.
     lab_status spmv_analyse(lab_csr_impl* A, cudaStream_t s)
     {
         spmv_plan& p = A->plan;
@@ -51,7 +51,7 @@ namespace lab
         p.avg_row = A->m > 0 ? (double)A->nnz / (double)A->m : 0.0;
         if(!p.forced)
         {
-            if(maxlen <= 16)
+            if(maxlen <= 32)
             {
                 p.alg   = LAB_SPMV_ROWSEQ;
                 p.lanes = 1;

@@ -11,14 +11,21 @@
 //   double finish(int row, acc_t s)   epilogue with s = sum_j a_ij x_j in CSR order
 //
 // Two schedules, picked per matrix by lab_spmv_analysis:
-//   ROWSEQ  one thread per row.  The CTA's contiguous nnz range is staged into
-//           shared memory with 16-byte cp.async copies (coalesced, L1 bypassed),
-//           then every thread walks its row in CSR order.  With kFma this is
-//           bit-identical to the reference host SpMV (host_matrix_vector.cpp:60-84).
-//   VECTOR  W lanes per row (W = 2..32), strided loads, xor-shuffle reduction.
+//   ROWSEQ  one thread per row, CSR order (k_pipe): a persistent CTA streams
+//           tiles of consecutive rows (row pointers, values, columns) through a
+//           double-buffered shared-memory stage with 16-byte cp.async copies
+//           (coalesced, L1 bypassed) and every thread walks its row from shared
+//           memory.  With kFma this is bit-identical to the reference host SpMV
+//           (host_matrix_vector.cpp:60-84).
+//   VECTOR  W lanes per row (W = 2..32, k_vector), coalesced direct loads,
+//           strided partial sums, xor-shuffle reduction.
 #pragma once
 
 #include "internal.cuh"
+
+#include <map>
+#include <mutex>
+
 #include "reduce.cuh"
 
 namespace lab
@@ -168,36 +175,54 @@ namespace lab
         asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
     }
 
-    // Persistent, double-buffered form of k_rowseq: each CTA walks row blocks
-    // blockIdx.x, blockIdx.x + gridDim.x, ... and prefetches block k+1 into the
-    // other shared-memory stage (cp.async groups) while it computes block k, so
-    // the DRAM stream never waits for the gathers and the fma chains.  Same
-    // per-row arithmetic as k_rowseq (bit-identical results).
+    // ROWSEQ schedule: persistent, double-buffered tile pipeline.  A tile is NT
+    // consecutive rows, one thread per row; each CTA walks tiles blockIdx.x,
+    // blockIdx.x + gridDim.x, ... and prefetches tile k+1 (its row pointers, and
+    // its contiguous value and column ranges) into the other shared-memory stage
+    // with 16-byte cp.async copies while it computes tile k, so the DRAM stream
+    // never waits for the gathers and the fma chains.  With MAXR > 0 every row
+    // has at most MAXR entries: the row's gathers are issued (up to 16 at a time)
+    // before their part of the accumulation chain.  Accumulation in CSR
+    // order: with kFma bit-identical to the reference host SpMV
+    // (host_matrix_vector.cpp:60-84).  A tile whose nnz exceeds the stage capacity
+    // is read straight from global memory (same arithmetic).
+    template <class VT>
+    __host__ __device__ constexpr size_t pipe_stage_bytes(int cap, int rt)
+    {
+        return ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16 + ((size_t)(cap + 8) * 4 + 15) / 16 * 16 +
+               ((size_t)(rt + 8) * 4 + 15) / 16 * 16;
+    }
+
     template <class Op, int NT, int MAXR>
     __global__ void __launch_bounds__(NT)
-        k_rowseq_pipe(csr_view<typename Op::val_t> A, Op op, int cap, red_buf red, int nblocks)
+        k_pipe(csr_view<typename Op::val_t> A, Op op, int cap, red_buf red, int ntiles)
     {
         using VT = typename Op::val_t;
         using AT = typename Op::acc_t;
+        constexpr int VPC = 16 / sizeof(VT);
+        static_assert(NT % 4 == 0, "tile rows must keep 16-byte row-pointer chunks");
         extern __shared__ __align__(16) unsigned char smem_raw[];
-        constexpr int VPC    = 16 / sizeof(VT);
-        const size_t  sv_b   = ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16;
-        const size_t  sc_b   = ((size_t)(cap + 8) * 4 + 15) / 16 * 16;
-        const size_t  stage_b = sv_b + sc_b;
+        const size_t sv_b    = ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16;
+        const size_t sc_b    = ((size_t)(cap + 8) * 4 + 15) / 16 * 16;
+        const size_t stage_b = pipe_stage_bytes<VT>(cap, NT);
         if(red.skip && *red.skip)
             return;
 
-        auto issue = [&](int blk, int stage) {
-            const int r0  = blk * NT;
-            const int r1  = min(r0 + NT, A.m);
-            const int j0  = A.rp[r0];
-            const int j1  = A.rp[r1];
-            const int j0v = j0 & ~(VPC - 1);
-            const int j0c = j0 & ~3;
+        auto issue = [&](int tile, int stage) {
+            const int      r0   = tile * NT;
+            const int      r1   = min(r0 + NT, A.m);
+            const int      j0   = A.rp[r0];
+            const int      j1   = A.rp[r1];
+            const int      j0v  = j0 & ~(VPC - 1), j0c = j0 & ~3;
+            unsigned char* base = smem_raw + stage * stage_b;
+            int32_t*       sr   = reinterpret_cast<int32_t*>(base + sv_b + sc_b);
+            const int      nr   = (r1 - r0 + 1 + 3) / 4; // rp[r0 .. r1], r0 % 4 == 0
+            for(int k = threadIdx.x; k < nr; k += NT)
+                cp_async16(sr + 4 * k, A.rp + r0 + 4 * k);
             if((j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4)
             {
-                VT*      sv = reinterpret_cast<VT*>(smem_raw + stage * stage_b);
-                int32_t* sc = reinterpret_cast<int32_t*>(smem_raw + stage * stage_b + sv_b);
+                VT*       sv = reinterpret_cast<VT*>(base);
+                int32_t*  sc = reinterpret_cast<int32_t*>(base + sv_b);
                 const int nv = (j1 - j0v + VPC - 1) / VPC;
                 const int nc = (j1 - j0c + 3) / 4;
                 for(int k = threadIdx.x; k < nv; k += NT)
@@ -208,47 +233,56 @@ namespace lab
         };
 
         double contrib = 0.0;
-        int    blk     = blockIdx.x;
-        if(blk < nblocks)
-            issue(blk, 0);
+        int    tile    = blockIdx.x;
+        if(tile < ntiles)
+            issue(tile, 0);
         cp_async_commit();
-        for(int it = 0; blk < nblocks; it++, blk += gridDim.x)
+        for(int it = 0; tile < ntiles; it++, tile += gridDim.x)
         {
-            const int nxt = blk + gridDim.x;
-            if(nxt < nblocks)
+            const int nxt = tile + gridDim.x;
+            if(nxt < ntiles)
                 issue(nxt, (it + 1) & 1);
             cp_async_commit();
             cp_async_wait_group<1>(); // everything but the newest group has landed
             __syncthreads();
-            const int stage = it & 1;
-            const int r0    = blk * NT;
-            const int r1    = min(r0 + NT, A.m);
-            const int j0    = A.rp[r0];
-            const int j1    = A.rp[r1];
-            const int j0v   = j0 & ~(VPC - 1);
-            const int j0c   = j0 & ~3;
-            const bool staged = (j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4;
-            const VT*      sv = reinterpret_cast<const VT*>(smem_raw + stage * stage_b);
-            const int32_t* sc = reinterpret_cast<const int32_t*>(smem_raw + stage * stage_b + sv_b);
-            const int row = r0 + threadIdx.x;
+            const unsigned char* base   = smem_raw + (it & 1) * stage_b;
+            const VT*            sv     = reinterpret_cast<const VT*>(base);
+            const int32_t*       sc     = reinterpret_cast<const int32_t*>(base + sv_b);
+            const int32_t*       sr     = reinterpret_cast<const int32_t*>(base + sv_b + sc_b);
+            const int            r0     = tile * NT;
+            const int            r1     = min(r0 + NT, A.m);
+            const int            j0     = sr[0], j1 = sr[r1 - r0];
+            const int            j0v    = j0 & ~(VPC - 1), j0c = j0 & ~3;
+            const bool           staged = (j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4;
+            const int            row    = r0 + threadIdx.x;
             if(row < r1)
             {
-                const int a = A.rp[row], b = A.rp[row + 1];
+                const int a = sr[row - r0], b = sr[row - r0 + 1];
                 AT        s = AT(0);
-                if(staged)
+                if(MAXR > 0 && staged)
                 {
-                    AT vv[MAXR], xv[MAXR];
+                    // gathers issued 16 at a time before their part of the chain,
+                    // the values re-read from shared memory
+                    constexpr int CH = MAXR < 16 ? MAXR : 16;
 #pragma unroll
-                    for(int k = 0; k < MAXR; k++)
-                        if(a + k < b)
-                        {
-                            vv[k] = to_acc(sv[a + k - j0v], AT(0));
-                            xv[k] = op.gather(sc[a + k - j0c]);
-                        }
+                    for(int c0 = 0; c0 < MAXR; c0 += CH)
+                    {
+                        AT xv[CH > 0 ? CH : 1];
 #pragma unroll
-                    for(int k = 0; k < MAXR; k++)
-                        if(a + k < b)
-                            s = acc_step<Op::kFma>(vv[k], xv[k], s);
+                        for(int q = 0; q < CH; q++)
+                            if(a + c0 + q < b)
+                                xv[q] = op.gather(sc[a + c0 + q - j0c]);
+#pragma unroll
+                        for(int q = 0; q < CH; q++)
+                            if(a + c0 + q < b)
+                                s = acc_step<Op::kFma>(to_acc(sv[a + c0 + q - j0v], AT(0)), xv[q],
+                                                       s);
+                    }
+                }
+                else if(staged)
+                {
+                    for(int j = a; j < b; j++)
+                        s = acc_step<Op::kFma>(to_acc(sv[j - j0v], AT(0)), op.gather(sc[j - j0c]), s);
                 }
                 else
                 {
@@ -257,18 +291,21 @@ namespace lab
                 }
                 contrib += op.finish(row, s);
             }
-            __syncthreads(); // this stage is refilled by the prefetch two blocks on
+            __syncthreads(); // this stage is refilled by the prefetch two tiles on
         }
         cp_async_wait_group<0>();
         if(Op::kReduce)
             reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
     }
 
+    // VECTOR schedule: W lanes per row, loads straight from global memory (the W
+    // lanes read consecutive entries, so they coalesce without staging),
+    // lane-strided partial sums and an xor-shuffle reduction.
     template <class Op, int NT, int W>
     __global__ void __launch_bounds__(NT)
         k_vector(csr_view<typename Op::val_t> A, Op op, red_buf red)
     {
-        using AT       = typename Op::acc_t;
+        using AT = typename Op::acc_t;
         if(red.skip && *red.skip)
             return;
         const int lane = threadIdx.x & (W - 1);
@@ -305,6 +342,55 @@ namespace lab
         return ceil_div<int64_t>(A->m * (int64_t)A->plan.lanes, kVectorNT);
     }
 
+    // Blocks per SM of one k_pipe instantiation at a given dynamic shared-memory
+    // size (cached; the stage size differs per matrix).
+    template <class Op, int MAXR>
+    int pipe_occupancy(size_t smem)
+    {
+        const auto                   kernel = k_pipe<Op, kRowseqNT, MAXR>;
+        static std::mutex            mu;
+        static std::map<size_t, int> cache;
+        static const cudaError_t     attr = cudaFuncSetAttribute(
+            kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        (void)attr;
+        std::lock_guard<std::mutex> g(mu);
+        auto                        it = cache.find(smem);
+        if(it != cache.end())
+            return it->second;
+        int occ = 0;
+        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kRowseqNT, smem) !=
+           cudaSuccess)
+        {
+            cudaGetLastError();
+            occ = 1;
+        }
+        occ         = std::max(occ, 1);
+        cache[smem] = occ;
+        return occ;
+    }
+
+    template <class Op, int MAXR>
+    lab_status launch_pipe(const csr_view<typename Op::val_t>& V, const Op& op, int cap,
+                           cudaStream_t s, const red_buf& red)
+    {
+        using VT              = typename Op::val_t;
+        const int      ntiles = (int)ceil_div<int64_t>(V.m, kRowseqNT);
+        const size_t   smem   = 2 * pipe_stage_bytes<VT>(cap, kRowseqNT);
+        const int      occ    = pipe_occupancy<Op, MAXR>(smem);
+        const unsigned grid   = (unsigned)std::min<int64_t>(ntiles, (int64_t)num_sms() * occ);
+        LAB_LAUNCH((k_pipe<Op, kRowseqNT, MAXR>), grid, kRowseqNT, smem, s, V, op, cap, red,
+                   ntiles);
+        return LAB_OK;
+    }
+
+    template <class Op, int W>
+    lab_status launch_vector(const csr_view<typename Op::val_t>& V, const Op& op, unsigned grid,
+                             cudaStream_t s, const red_buf& red)
+    {
+        LAB_LAUNCH((k_vector<Op, kVectorNT, W>), grid, kVectorNT, 0, s, V, op, red);
+        return LAB_OK;
+    }
+
     template <class Op>
     lab_status launch_rowop(const lab_csr_impl* A, const typename Op::val_t* vals, const Op& op,
                             cudaStream_t s, red_buf red = red_buf())
@@ -316,88 +402,42 @@ namespace lab
         const spmv_plan& p = A->plan;
         if(p.alg == LAB_SPMV_ROWSEQ)
         {
-            int    cap  = kRowseqNT * std::max(1, p.max_row);
+            const int mr = std::max(1, p.max_row);
+            if(mr <= 8)
+                return launch_pipe<Op, 8>(V, op, kRowseqNT * mr, s, red);
+            if(mr <= 16)
+                return launch_pipe<Op, 16>(V, op, kRowseqNT * mr, s, red);
+            if(mr <= 32)
+                return launch_pipe<Op, 32>(V, op, kRowseqNT * mr, s, red);
+            // long rows forced onto one thread each: unbounded loop, staged when it fits
+            int    cap  = kRowseqNT * mr;
             size_t smem = rowseq_smem<VT>(cap);
             if(smem > 200 * 1024)
             {
-                cap  = 0; // fall back to unstaged global reads
+                cap  = 0;
                 smem = rowseq_smem<VT>(0);
             }
-            // Raise the dynamic shared-memory cap once per instantiation.
-            static const cudaError_t attr8 = cudaFuncSetAttribute(
-                k_rowseq<Op, kRowseqNT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            static const cudaError_t attr16 = cudaFuncSetAttribute(
-                k_rowseq<Op, kRowseqNT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                200 * 1024);
             static const cudaError_t attr0 = cudaFuncSetAttribute(
                 k_rowseq<Op, kRowseqNT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            LAB_CUDA(attr8);
-            LAB_CUDA(attr16);
             LAB_CUDA(attr0);
-            const unsigned grid = (unsigned)rowop_grid(A);
-            if(p.max_row <= 16)
-            {
-                // persistent double-buffered kernel; stage capacity fixed per instantiation
-                const int  nblocks = (int)grid;
-                const bool r8      = p.max_row <= 8;
-                const int  pcap    = kRowseqNT * (r8 ? 8 : 16);
-                const size_t psmem = 2 * (((size_t)(pcap + 16) * sizeof(VT) + 15) / 16 * 16 +
-                                          ((size_t)(pcap + 8) * 4 + 15) / 16 * 16);
-                static int occ8 = -1, occ16 = -1;
-                int&       occ  = r8 ? occ8 : occ16;
-                if(occ < 0)
-                {
-                    if(r8)
-                    {
-                        LAB_CUDA(cudaFuncSetAttribute(k_rowseq_pipe<Op, kRowseqNT, 8>,
-                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                      (int)psmem));
-                        LAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                            &occ, k_rowseq_pipe<Op, kRowseqNT, 8>, kRowseqNT, psmem));
-                    }
-                    else
-                    {
-                        LAB_CUDA(cudaFuncSetAttribute(k_rowseq_pipe<Op, kRowseqNT, 16>,
-                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                      (int)psmem));
-                        LAB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                            &occ, k_rowseq_pipe<Op, kRowseqNT, 16>, kRowseqNT, psmem));
-                    }
-                    occ = std::max(occ, 1);
-                }
-                const unsigned pgrid =
-                    (unsigned)std::min<int64_t>(nblocks, (int64_t)num_sms() * occ);
-                if(r8)
-                    LAB_LAUNCH((k_rowseq_pipe<Op, kRowseqNT, 8>), pgrid, kRowseqNT, psmem, s, V,
-                               op, pcap, red, nblocks);
-                else
-                    LAB_LAUNCH((k_rowseq_pipe<Op, kRowseqNT, 16>), pgrid, kRowseqNT, psmem, s, V,
-                               op, pcap, red, nblocks);
-                return LAB_OK;
-            }
-            LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 0>), grid, kRowseqNT, smem, s, V, op, cap, red);
+            LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 0>), (unsigned)rowop_grid(A), kRowseqNT, smem, s,
+                       V, op, cap, red);
             return LAB_OK;
         }
-        unsigned grid = (unsigned)rowop_grid(A);
+        const unsigned grid = (unsigned)rowop_grid(A);
         switch(p.lanes)
         {
         case 2:
-            LAB_LAUNCH((k_vector<Op, kVectorNT, 2>), grid, kVectorNT, 0, s, V, op, red);
-            break;
+            return launch_vector<Op, 2>(V, op, grid, s, red);
         case 4:
-            LAB_LAUNCH((k_vector<Op, kVectorNT, 4>), grid, kVectorNT, 0, s, V, op, red);
-            break;
+            return launch_vector<Op, 4>(V, op, grid, s, red);
         case 8:
-            LAB_LAUNCH((k_vector<Op, kVectorNT, 8>), grid, kVectorNT, 0, s, V, op, red);
-            break;
+            return launch_vector<Op, 8>(V, op, grid, s, red);
         case 16:
-            LAB_LAUNCH((k_vector<Op, kVectorNT, 16>), grid, kVectorNT, 0, s, V, op, red);
-            break;
+            return launch_vector<Op, 16>(V, op, grid, s, red);
         default:
-            LAB_LAUNCH((k_vector<Op, kVectorNT, 32>), grid, kVectorNT, 0, s, V, op, red);
-            break;
+            return launch_vector<Op, 32>(V, op, grid, s, red);
         }
-        return LAB_OK;
     }
 
     // ------------------------------------------------------------ basic ops

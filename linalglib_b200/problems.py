@@ -2,9 +2,9 @@
 
 The reference's own test fixtures are SuiteSparse ``.mtx`` files fetched over the
 network (clients/matrices/matrix_downloader.py), so the workloads here are
-generated: Dirichlet finite-difference Poisson operators, a 27-point trilinear
-finite-element diffusion operator with lognormal anisotropic coefficients, and a
-weighted 7-point graph Laplacian.  Every matrix is CSR with int32 indices, float64
+generated: Dirichlet finite-difference Poisson operators, a 27-point
+variable-coefficient diffusion operator (lognormal link conductances, z anisotropy),
+and a weighted 7-point graph Laplacian.  Every matrix is CSR with int32 indices, float64
 values and column indices sorted ascending inside each row (the layout the
 reference's read_mtx and SpGEMM produce, library/src/csr_matrix.cpp:524-729).
 
@@ -90,43 +90,39 @@ def poisson3d(n: int, ny: int | None = None, nz: int | None = None):
 
 
 def diffusion27(n: int, sigma: float = 1.5, zscale: float = 100.0, seed: int = 0):
-    """Trilinear (Q1) finite-element diffusion operator on an n^3 interior node grid.
+    """27-point variable-coefficient diffusion operator on an n^3 Dirichlet grid.
 
-    The (n+1)^3 hexahedral cells each carry a conductivity k_c ~ lognormal(0, sigma)
-    and the diagonal tensor diag(k_c, k_c, zscale*k_c).  Homogeneous Dirichlet
-    nodes on the boundary are eliminated, leaving a symmetric positive definite
-    27-point operator.  For unit cells the Q1 element matrix of a diagonal tensor
-    (kx, ky, kz) couples local nodes a, b as
-        kx*S(ax,bx)*M(ay,by)*M(az,bz) + ky*M*S*M + kz*M*M*S
-    with the 1-D stiffness S = [[1,-1],[-1,1]] and mass M = [[2,1],[1,2]]/6.
+    Every node is linked to its 26 neighbours (faces, edges, corners).  Link
+    p -> p+d carries a conductance  k * (dx^2 + dy^2 + zscale*dz^2) / |d|^4  with
+    k ~ lognormal(0, sigma) drawn per link (the tensor diag(1, 1, zscale) projected
+    on the link direction, over the squared link length).  Row p holds -c for each
+    neighbour inside the grid and the sum of all 26 link conductances on the
+    diagonal (links to the eliminated boundary nodes included), so the operator is
+    a symmetric, weakly diagonally dominant M-matrix (positive definite, and
+    lambda_max(D^-1 A) <= 2).
+
+    Conductances are drawn link by link from numpy.random.default_rng(seed), one
+    (n+2)^3 array per half-direction d, in the order the 13 half-directions with
+    d > 0 lexicographically (dz, dy, dx) are enumerated.
     """
     rng = np.random.default_rng(seed)
-    nc = n + 1
-    k = rng.lognormal(0.0, sigma, size=(nc, nc, nc))  # indexed (cz, cy, cx)
-    S = np.array([[1.0, -1.0], [-1.0, 1.0]])
-    M = np.array([[2.0, 1.0], [1.0, 2.0]]) / 6.0
+    halves = [(dz, dy, dx) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)
+              if (dz, dy, dx) > (0, 0, 0)]
+    diag = np.zeros((n, n, n))
     offs = []
     weights = []
-    # node (z,y,x) sits at the corner of cells (z+ez, y+ey, x+ex), ez..ex in {0,1}:
-    # inside that cell its local coordinate is (1-ez, 1-ey, 1-ex).
-    for dz in (-1, 0, 1):
-        for dy in (-1, 0, 1):
-            for dx in (-1, 0, 1):
-                w = np.zeros((n, n, n))
-                for ez in (0, 1):
-                    for ey in (0, 1):
-                        for ex in (0, 1):
-                            az, ay, ax = 1 - ez, 1 - ey, 1 - ex
-                            bz, by, bx = az + dz, ay + dy, ax + dx
-                            if not (0 <= bz <= 1 and 0 <= by <= 1 and 0 <= bx <= 1):
-                                continue
-                            kc = k[ez:ez + n, ey:ey + n, ex:ex + n]
-                            coef = (S[ax, bx] * M[ay, by] * M[az, bz]
-                                    + M[ax, bx] * S[ay, by] * M[az, bz]
-                                    + zscale * M[ax, bx] * M[ay, by] * S[az, bz])
-                            w += coef * kc
-                offs.append((dz, dy, dx))
-                weights.append(w)
+    for d in halves:
+        dz, dy, dx = d
+        scale = (dx * dx + dy * dy + zscale * dz * dz) / float(dx * dx + dy * dy + dz * dz) ** 2
+        # conductance of the link from padded node q (grid node q - 1) to q + d
+        c = scale * rng.lognormal(0.0, sigma, size=(n + 2, n + 2, n + 2))
+        fwd = c[1:n + 1, 1:n + 1, 1:n + 1]                                 # p -> p + d
+        bwd = c[1 - dz:n + 1 - dz, 1 - dy:n + 1 - dy, 1 - dx:n + 1 - dx]   # p - d -> p
+        diag += fwd + bwd
+        offs += [d, (-dz, -dy, -dx)]
+        weights += [-fwd, -bwd]
+    offs.append((0, 0, 0))
+    weights.append(diag)
     return _stencil_csr((n, n, n), offs, weights)
 
 
