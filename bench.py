@@ -56,6 +56,9 @@ def parse():
                     help="grid side (default: 128 for the Poisson step, 160 for mixed, "
                          "96 for adjoint, 64 for the multi-RHS batch)")
     ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--matrix", default="poisson", choices=["poisson", "diffusion27"],
+                    help="operator of --mode spmv: 3D 7-point Poisson (default) or the "
+                         "27-point diffusion operator")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="full",
                     choices=["full", "profile", "spmv", "mixed", "batched", "adjoint"],
@@ -264,7 +267,7 @@ def run_reference(args, d):
 
 
 # ------------------------------------------------------------------ our arm
-def dominant_kernel_roofline(core, dA, m, nnz, torch):
+def dominant_kernel_roofline(core, dA, m, nnz, torch, profiled=True):
     """CUDA-event timing of the dominant kernel class (level-0 CSR pass: SpMV on
     the 128^3 operator, the same row engine as the smoother kernels): 20 launches
     back to back between two events on the launching stream, three times; A_0
@@ -297,11 +300,14 @@ def dominant_kernel_roofline(core, dA, m, nnz, torch):
         peak, which = 6650.0, "fallback"
     traffic = None
     prof = os.path.join(ROOT, "profiles", "spmv_poisson3d_128.md")
-    if os.path.exists(prof):
+    if profiled and os.path.exists(prof):
         mt = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(prof).read())
         if mt:
             traffic = float(mt.group(1))
-    return {"bound": "hbm", "kernel": "k_pipe<op_spmv, 256, 8> on A_0 (level-0 CSR pass)",
+    alg, lanes = dA.algorithm()
+    kname = ("k_pipe<op_spmv> (one thread per row, staged tiles)" if alg == 1
+             else f"k_vector<op_spmv> ({lanes} lanes per row)")
+    return {"bound": "hbm", "kernel": kname + " on A_0 (level-0 CSR pass)",
             "achieved": achieved, "peak": peak, "peak_source": which, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": algo,
             "launch_us": t * 1e6}
@@ -314,16 +320,22 @@ def run_ours(args, d):
     import linalglib_b200.core as core
     from linalglib_b200 import _lib as L
     core.init()
-    A, b, xt = problem(args.n)
+    if args.mode == "spmv" and args.matrix == "diffusion27":
+        from linalglib_b200 import problems as P
+        A = P.diffusion27(args.n, seed=0)
+        b, xt = P.rhs_from_solution(*A, seed=0)
+    else:
+        A, b, xt = problem(args.n)
     m, nnz = A[0].size - 1, A[2].size
     stream = torch.cuda.current_stream()
     dA = core.CsrMatrix.from_arrays(*A)
     dA.analyse()
     if args.mode == "spmv":
-        roof = dominant_kernel_roofline(core, dA, m, nnz, torch)
+        roof = dominant_kernel_roofline(core, dA, m, nnz, torch,
+                                        profiled=args.matrix == "poisson" and args.n == 128)
         if d.rank == 0:
-            print(json.dumps({"mode": "spmv", "rows": int(m), "nnz": int(nnz), "roofline": roof}),
-                  flush=True)
+            print(json.dumps({"mode": "spmv", "matrix": f"{args.matrix} {args.n}^3", "rows": int(m),
+                              "nnz": int(nnz), "roofline": roof}), flush=True)
         d.close()
         return 0
     bd = core.vec(b)
@@ -425,7 +437,7 @@ def run_ours(args, d):
     h2d = 4 * (m + 1) + 4 * nnz + 8 * nnz + 8 * m + 8 * m  # A, b, x0
     d2h = 8 * m
 
-    roof = dominant_kernel_roofline(core, dA, m, nnz, torch)
+    roof = dominant_kernel_roofline(core, dA, m, nnz, torch, profiled=args.n == 128)
 
     if d.rank == 0:
         cpu = None

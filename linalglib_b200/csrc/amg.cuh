@@ -18,6 +18,10 @@ namespace lab
         float*  bf  = nullptr;
         float*  rf  = nullptr;
         float*  tf  = nullptr;
+        double* xk  = nullptr; // block cycle vectors: m_l x 8 columns, interleaved per row
+        double* bk  = nullptr;
+        double* rk  = nullptr;
+        double* tk  = nullptr;
         int32_t* colour = nullptr; // multicolour GS: row order by colour
         int32_t* colour_ptr_h = nullptr; // host copy of colour offsets
         int      ncolours = 0;

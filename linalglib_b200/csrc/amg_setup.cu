@@ -160,6 +160,97 @@ namespace lab
         out[i] = ns;
     }
 
+    // Warp-per-row form of k_pmis_round for long rows (coarse levels).  The
+    // sequential scan keeps the first (state, hash) maximum it meets, so its result
+    // is the lexicographic maximum of (state, hash, -scan position) over the start
+    // value (position -1) and the strong neighbours; lanes take strided positions
+    // and a shuffle reduction picks that maximum: the same winner as the scan.
+    struct pmis_best
+    {
+        int s, h, pos, node;
+    };
+    __device__ __forceinline__ bool pmis_better(const pmis_best& a, const pmis_best& b)
+    {
+        if(a.s != b.s)
+            return a.s > b.s;
+        if(a.h != b.h)
+            return a.h > b.h;
+        return a.pos < b.pos;
+    }
+    __device__ __forceinline__ pmis_best pmis_warp_max(pmis_best v)
+    {
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+        {
+            pmis_best w;
+            w.s    = __shfl_xor_sync(0xffffffffu, v.s, o);
+            w.h    = __shfl_xor_sync(0xffffffffu, v.h, o);
+            w.pos  = __shfl_xor_sync(0xffffffffu, v.pos, o);
+            w.node = __shfl_xor_sync(0xffffffffu, v.node, o);
+            if(pmis_better(w, v))
+                v = w;
+        }
+        return v;
+    }
+    // best over {start} and the strong neighbours of row r (positions in CSR order)
+    __device__ __forceinline__ pmis_best pmis_scan_warp(const int32_t* __restrict__ rp,
+                                                        const int32_t* __restrict__ ci,
+                                                        const int32_t* __restrict__ conn,
+                                                        const int32_t* __restrict__ st,
+                                                        const int32_t* __restrict__ hash, int r,
+                                                        pmis_best start, int lane)
+    {
+        pmis_best v = start;
+        const int a = rp[r], b = rp[r + 1];
+        for(int j = a + lane; j < b; j += 32)
+        {
+            if(conn[j] != 1)
+                continue;
+            const int c = ci[j];
+            pmis_best w{st[c], hash[c], j - a, c};
+            if(pmis_better(w, v))
+                v = w;
+        }
+        return pmis_warp_max(v);
+    }
+
+    __global__ void k_pmis_round_warp(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                      const int32_t* __restrict__ conn, int64_t m,
+                                      const int32_t* __restrict__ st,
+                                      const int32_t* __restrict__ hash, int32_t* __restrict__ out,
+                                      int64_t* __restrict__ agg, int32_t* flags, int round)
+    {
+        if(round > 0 && flags[round - 1] == 0)
+            return;
+        const int64_t i    = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        const int     lane = threadIdx.x & 31;
+        if(i >= m)
+            return;
+        pmis_best v = pmis_scan_warp(rp, ci, conn, st, hash, (int)i,
+                                     pmis_best{st[i], hash[i], -1, (int)i}, lane);
+        // second scan over the winner's row, starting from the winner (position -1)
+        v = pmis_scan_warp(rp, ci, conn, st, hash, v.node, pmis_best{v.s, v.h, -1, v.node}, lane);
+        if(lane != 0)
+            return;
+        int ns = st[i];
+        if(ns == 0)
+        {
+            if(v.node == i)
+            {
+                ns     = 1;
+                agg[i] = 1;
+            }
+            else if(v.s == 1)
+            {
+                ns     = -1;
+                agg[i] = 0;
+            }
+            else
+                flags[round] = 1;
+        }
+        out[i] = ns;
+    }
+
     // Rounds that ran: round r runs iff r == 0 or round r-1 left a row undecided.
     __device__ __forceinline__ int pmis_rounds_run(const int32_t* flags)
     {
@@ -201,6 +292,46 @@ namespace lab
         out[i] = s;
     }
 
+    // Warp-per-row form of k_pmis_attach for long rows: the first strong neighbour
+    // in CSR order whose state is 1 (ballot per 32-entry chunk, lowest lane first).
+    __global__ void k_pmis_attach_warp(const int32_t* __restrict__ rp,
+                                       const int32_t* __restrict__ ci,
+                                       const int32_t* __restrict__ conn, int64_t m, int32_t* b0,
+                                       int32_t* b1, const int32_t* __restrict__ flags, int k,
+                                       int64_t* __restrict__ agg)
+    {
+        const int64_t i    = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        const int     lane = threadIdx.x & 31;
+        if(i >= m)
+            return;
+        const int      sel = (pmis_rounds_run(flags) + k) & 1;
+        const int32_t* st  = sel ? b1 : b0;
+        int32_t*       out = sel ? b0 : b1;
+        int            s   = st[i];
+        if(s == -1)
+        {
+            const int a = rp[i], b = rp[i + 1];
+            for(int base = a; base < b; base += 32)
+            {
+                const int      j   = base + lane;
+                const bool     hit = j < b && conn[j] == 1 && st[ci[j]] == 1;
+                const unsigned bal = __ballot_sync(0xffffffffu, hit);
+                if(bal)
+                {
+                    const int first = base + __ffs(bal) - 1;
+                    if(lane == 0)
+                        agg[i] = agg[ci[first]];
+                    s = 1;
+                    break;
+                }
+            }
+        }
+        else if(s == -2 && lane == 0)
+            agg[i] = -2;
+        if(lane == 0)
+            out[i] = s;
+    }
+
     __global__ void k_count_rounds(const int32_t* flags, int* out)
     {
         int r = 0;
@@ -238,10 +369,20 @@ namespace lab
         LAB_LAUNCH(k_pmis_init, g, 256, 0, s, A->row_ptr, conn, m, state.get(), hash.get(), agg);
         // ping-pong: round r reads buffer r & 1 of {state, snap} and writes the other
         int32_t* buf[2] = {state.get(), snap.get()};
+        // long rows (coarse levels): a warp per row
+        const bool     wide = A->nnz > 12 * m;
+        const unsigned gw   = (unsigned)ceil_div<int64_t>(m * 32, 256);
         for(int r = 0; r < 20; r++)
-            LAB_LAUNCH(k_pmis_round, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
-                       (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg, flags.get(),
-                       r);
+        {
+            if(wide)
+                LAB_LAUNCH(k_pmis_round_warp, gw, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                           (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg,
+                           flags.get(), r);
+            else
+                LAB_LAUNCH(k_pmis_round, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                           (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg,
+                           flags.get(), r);
+        }
         if(rounds)
         {
             dbuf<int> d;
@@ -253,8 +394,14 @@ namespace lab
             LAB_LAUNCH(k_pmis_roots, g, 256, 0, s, (const int64_t*)agg, m, roots);
         LAB_TRY(scan_i64(agg, m, s));
         for(int k = 0; k < 2; k++)
-            LAB_LAUNCH(k_pmis_attach, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m, state.get(),
-                       snap.get(), (const int32_t*)flags.get(), k, agg);
+        {
+            if(wide)
+                LAB_LAUNCH(k_pmis_attach_warp, gw, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                           state.get(), snap.get(), (const int32_t*)flags.get(), k, agg);
+            else
+                LAB_LAUNCH(k_pmis_attach, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                           state.get(), snap.get(), (const int32_t*)flags.get(), k, agg);
+        }
         return LAB_OK;
     }
 
@@ -761,7 +908,8 @@ namespace lab
             if(h->A[l])
                 csr_release(h->A[l]);
             level_ws& w = h->ws[l];
-            void*     ptrs[] = {w.x, w.b, w.r, w.t, w.xf, w.bf, w.rf, w.tf, w.colour};
+            void*     ptrs[] = {w.x,  w.b,  w.r,  w.t,  w.xf, w.bf, w.rf,
+                                w.tf, w.xk, w.bk, w.rk, w.tk, w.colour};
             for(void* p : ptrs)
                 if(p)
                     cudaFree(p);

@@ -721,7 +721,8 @@ namespace lab
                                ? (T)o->omega_sor
                                : T(1);
         const bool sym   = o->smoother == LAB_SMOOTH_SSOR;
-        const int  lanes = A->plan.alg == LAB_SPMV_ROWSEQ ? 1 : std::min(A->plan.lanes, 32);
+        const int  lanes = A->plan.alg == LAB_SPMV_VECTOR ? std::min(A->plan.lanes, 32)
+                           : (A->plan.max_row <= 32 ? 1 : A->plan.vlanes);
         auto pass = [&](int col) -> lab_status {
             return with_vals<T>(A, bf, [&](auto* vals) -> lab_status {
                 using VT = vt_of<decltype(vals)>;

@@ -27,6 +27,15 @@ namespace lab
     // place; reduced-precision cycles run in correction form x += cycle(0; b - A x).
     lab_status cycle_iterate(hierarchy_impl* h, const cyc_ctx& c, const double* b, double* x);
 
+    // Block V-cycle over many right-hand sides (cycle_blk.cu): whether the options
+    // are covered (V-cycle, Jacobi, FP64, 1x1 or dense coarsest solve; call after
+    // cycle_prepare), the block workspace (outside graph capture), and
+    // z[:, k] = cycle(0; r[:, k]) for ncols column-major columns, 8 per pass.
+    bool       cycle_block_supported(const hierarchy_impl* h, const lab_amg_options* o);
+    lab_status cycle_prepare_block(hierarchy_impl* h, cudaStream_t s);
+    lab_status cycle_precond_block(hierarchy_impl* h, const cyc_ctx& c, int ncols, const double* r,
+                                   int64_t ldr, double* z, int64_t ldz);
+
     // deterministic device reductions into r.out (grid <= kRedBlocks)
     lab_status dot_device(int64_t n, const double* x, const double* y, red_buf r, cudaStream_t s);
     lab_status norm_inf_device(int64_t n, const double* x, red_buf r, cudaStream_t s);

@@ -119,6 +119,7 @@ namespace lab
         int    analysed = 0;
         int    alg      = LAB_SPMV_ROWSEQ; // lab_spmv_alg
         int    lanes    = 1;               // lanes per row for LAB_SPMV_VECTOR
+        int    vlanes   = 2;               // lanes a multi-lane kernel would use (mean row / 3)
         int    forced   = 0;
         int    max_row  = 0;
         double avg_row  = 0.0;

@@ -1143,6 +1143,7 @@ namespace lab
         precond_impl* M     = nullptr;
         int           multi = 0; // 0: stacked systems, 1: nseg columns of one matrix
         int64_t       n     = 0; // rows of A (multi-RHS column length)
+        int           block = 0; // multi-RHS: block V-cycle over up to 8 columns per pass
     };
 
     static lab_status seg_apply_A(const seg_ops& o, seg_ws& w, const double* in, double* out,
@@ -1170,6 +1171,11 @@ namespace lab
     {
         if(!o.multi)
             return precond_apply(o.M, r, z, s, skip, red_buf());
+        if(o.block)
+        {
+            cyc_ctx c{&o.M->o, s, skip};
+            return cycle_precond_block(o.M->h, c, w.nseg, r, o.n, z, o.n);
+        }
         for(int c = 0; c < w.nseg; c++)
             LAB_TRY(precond_apply(o.M, r + (int64_t)c * o.n, z + (int64_t)c * o.n, s, skip,
                                   red_buf()));
@@ -1640,6 +1646,11 @@ LAB_API lab_status lab_multi_rhs_pcg_solve(lab_csr A, lab_precond M, int nrhs, c
     o.M     = M;
     o.multi = 1;
     o.n     = A->m;
+    if(M->kind == 0 && cycle_block_supported(M->h, &M->o))
+    {
+        LAB_TRY(cycle_prepare_block(M->h, s));
+        o.block = 1;
+    }
     return seg_solve(o, nrhs, off.data(), B, X, c, iterations, converged, info, s);
 }
 

@@ -17,19 +17,24 @@ namespace lab
             atomicMax(maxlen, local);
     }
 
-    static int pow2_at_least(double v)
+    // Largest power of two <= v, clamped to 2..32.
+    static int pow2_at_most(double v)
     {
         int w = 2;
-        while(w < 32 && w < v)
+        while(w < 32 && 2 * w <= v)
             w <<= 1;
         return w;
     }
 
-    // Schedule choice from row statistics.  Short, bounded rows (stencils up to
-    // 27 points: at most 32 entries) take the staged thread-per-row kernel, whose
-    // fma order matches the reference's host SpMV bit for bit; longer rows take W
-    // lanes per row with W the power of two nearest a third of the mean row
-    // length, which keeps >= 80 % of the lanes busy on the last stride.
+    // Schedule choice from row statistics.  Rows of at most 32 entries (stencils up
+    // to 27 points) take the one-thread-per-row order (ROWSEQ: staged tiles for
+    // <= 16, warp tiles for <= 32), whose fma chain matches the reference's host
+    // SpMV bit for bit.  Longer rows (coarse AMG levels) take W lanes per row with
+    // W the largest power of two <= mean row / 5 -- the fastest lane count measured
+    // on B200 across the SA levels of 7- and 27-point operators (W = 4 at 23
+    // entries, 8 at 41-73, 16 at 143-178, 16-32 beyond); lab_spmv_autotune times
+    // every choice on the actual matrix instead.  vlanes is also the lane count of
+    // SpMM and multicolour Gauss-Seidel on long rows.
     lab_status spmv_analyse(lab_csr_impl* A, cudaStream_t s)
     {
         spmv_plan& p = A->plan;
@@ -49,18 +54,11 @@ namespace lab
         }
         p.max_row = maxlen;
         p.avg_row = A->m > 0 ? (double)A->nnz / (double)A->m : 0.0;
+        p.vlanes  = pow2_at_most(p.avg_row / 5.0);
         if(!p.forced)
         {
-            if(maxlen <= 32)
-            {
-                p.alg   = LAB_SPMV_ROWSEQ;
-                p.lanes = 1;
-            }
-            else
-            {
-                p.alg   = LAB_SPMV_VECTOR;
-                p.lanes = pow2_at_least(p.avg_row / 3.0);
-            }
+            p.alg   = maxlen <= 32 ? LAB_SPMV_ROWSEQ : LAB_SPMV_VECTOR;
+            p.lanes = maxlen <= 32 ? 1 : p.vlanes;
         }
         p.analysed = 1;
         return LAB_OK;
@@ -119,7 +117,8 @@ namespace lab
     {
         if(A->m == 0 || k <= 0)
             return LAB_OK;
-        int      lanes = A->plan.alg == LAB_SPMV_ROWSEQ ? 4 : A->plan.lanes;
+        int      lanes = A->plan.alg == LAB_SPMV_VECTOR ? A->plan.lanes
+                       : (A->plan.max_row <= 32 ? 4 : A->plan.vlanes);
         unsigned grid  = (unsigned)ceil_div<int64_t>(A->m * (int64_t)lanes, 256);
         int32_t  m     = (int32_t)A->m;
         if(k == 8)
@@ -223,7 +222,8 @@ LAB_API lab_status lab_spmm(double alpha, lab_csr A, int nrhs, const double* X, 
     LAB_TRY(spmv_analyse(A, s));
     if(A->m == 0)
         return LAB_OK;
-    int      lanes = A->plan.alg == LAB_SPMV_ROWSEQ ? 4 : A->plan.lanes;
+    int      lanes = A->plan.alg == LAB_SPMV_VECTOR ? A->plan.lanes
+                       : (A->plan.max_row <= 32 ? 4 : A->plan.vlanes);
     unsigned grid  = (unsigned)ceil_div<int64_t>(A->m * (int64_t)lanes, 256);
     for(int c = 0; c < nrhs; c += 8)
     {

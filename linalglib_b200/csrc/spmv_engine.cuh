@@ -86,85 +86,6 @@ namespace lab
         asm volatile("cp.async.wait_all;\n" ::: "memory");
     }
 
-    // Shared-memory bytes the ROWSEQ kernel needs for `cap` staged entries.
-    template <class VT>
-    __host__ __device__ constexpr size_t rowseq_smem(int cap)
-    {
-        return ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16 + (size_t)(cap + 8) * 4;
-    }
-
-    // MAXR > 0: every row has at most MAXR entries (from the analysis); the row is
-    // read into registers with all its gathers issued before the fma chain, which
-    // keeps MAXR loads in flight per thread.  The accumulation order is unchanged.
-    template <class Op, int NT, int MAXR>
-    __global__ void __launch_bounds__(NT)
-        k_rowseq(csr_view<typename Op::val_t> A, Op op, int cap, red_buf red)
-    {
-        using VT = typename Op::val_t;
-        using AT = typename Op::acc_t;
-        extern __shared__ __align__(16) unsigned char smem_raw[];
-        constexpr int VPC = 16 / sizeof(VT); // values per 16-byte chunk
-        VT*           sv  = reinterpret_cast<VT*>(smem_raw);
-        int32_t*      sc  = reinterpret_cast<int32_t*>(smem_raw + ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16);
-        if(red.skip && *red.skip)
-            return;
-
-        const int r0  = blockIdx.x * NT;
-        const int r1  = min(r0 + NT, A.m);
-        const int j0  = A.rp[r0];
-        const int j1  = A.rp[r1];
-        const int j0v = j0 & ~(VPC - 1);
-        const int j0c = j0 & ~3;
-        const bool staged = (j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4;
-        if(staged)
-        {
-            const int nv = (j1 - j0v + VPC - 1) / VPC;
-            const int nc = (j1 - j0c + 3) / 4;
-            for(int k = threadIdx.x; k < nv; k += NT)
-                cp_async16(sv + (size_t)k * VPC, A.v + j0v + (size_t)k * VPC);
-            for(int k = threadIdx.x; k < nc; k += NT)
-                cp_async16(sc + (size_t)k * 4, A.ci + j0c + (size_t)k * 4);
-            cp_async_wait_all();
-        }
-        __syncthreads();
-
-        double contrib = 0.0;
-        const int row  = r0 + threadIdx.x;
-        if(row < r1)
-        {
-            const int a = A.rp[row], b = A.rp[row + 1];
-            AT        s = AT(0);
-            if(staged && MAXR > 0)
-            {
-                AT vv[MAXR > 0 ? MAXR : 1], xv[MAXR > 0 ? MAXR : 1];
-#pragma unroll
-                for(int k = 0; k < MAXR; k++)
-                    if(a + k < b)
-                    {
-                        vv[k] = to_acc(sv[a + k - j0v], AT(0));
-                        xv[k] = op.gather(sc[a + k - j0c]);
-                    }
-#pragma unroll
-                for(int k = 0; k < MAXR; k++)
-                    if(a + k < b)
-                        s = acc_step<Op::kFma>(vv[k], xv[k], s);
-            }
-            else if(staged)
-            {
-                for(int j = a; j < b; j++)
-                    s = acc_step<Op::kFma>(to_acc(sv[j - j0v], AT(0)), op.gather(sc[j - j0c]), s);
-            }
-            else
-            {
-                for(int j = a; j < b; j++)
-                    s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), op.gather(A.ci[j]), s);
-            }
-            contrib = op.finish(row, s);
-        }
-        if(Op::kReduce)
-            reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
-    }
-
     __device__ __forceinline__ void cp_async_commit()
     {
         asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -298,6 +219,144 @@ namespace lab
             reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
     }
 
+    // ROWSEQ schedule for rows of 17..32 entries (27-point stencils): a warp owns a
+    // tile of 32 consecutive rows, stages the tile's row pointers, values and
+    // columns into its own shared-memory region with cp.async, and each lane
+    // walks its row from there (CSR-order fma chain, bit-identical to k_pipe).
+    // No block barrier: per-warp single buffering keeps the shared memory per
+    // resident row small, so about 20 warps per SM stream tiles independently
+    // (a CTA-wide double-buffered 256-row tile of 27-entry rows leaves one CTA,
+    // 8 warps, per SM).  `cap` = 32 x the longest row; a larger tile is read from
+    // global memory directly.
+    constexpr int kWarpPipeWarps = 4;
+
+    template <class VT>
+    __host__ __device__ constexpr size_t warp_stage_bytes(int cap)
+    {
+        return ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16 + ((size_t)(cap + 8) * 4 + 15) / 16 * 16 +
+               ((size_t)(32 + 8) * 4 + 15) / 16 * 16;
+    }
+
+    template <class Op, int MAXR>
+    __global__ void __launch_bounds__(32 * kWarpPipeWarps)
+        k_pipe_warp(csr_view<typename Op::val_t> A, Op op, int cap, red_buf red, int ntiles)
+    {
+        using VT = typename Op::val_t;
+        using AT = typename Op::acc_t;
+        constexpr int VPC = 16 / sizeof(VT);
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        const size_t   sv_b = ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16;
+        const size_t   sc_b = ((size_t)(cap + 8) * 4 + 15) / 16 * 16;
+        const int      wid  = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        unsigned char* base = smem_raw + (size_t)wid * warp_stage_bytes<VT>(cap);
+        VT*            sv   = reinterpret_cast<VT*>(base);
+        int32_t*       sc   = reinterpret_cast<int32_t*>(base + sv_b);
+        int32_t*       sr   = reinterpret_cast<int32_t*>(base + sv_b + sc_b);
+        if(red.skip && *red.skip)
+            return;
+        double contrib = 0.0;
+        for(int tile = blockIdx.x * kWarpPipeWarps + wid; tile < ntiles;
+            tile += gridDim.x * kWarpPipeWarps)
+        {
+            const int  r0     = tile * 32;
+            const int  r1     = min(r0 + 32, A.m);
+            const int  j0     = A.rp[r0];
+            const int  j1     = A.rp[r1];
+            const int  j0v    = j0 & ~(VPC - 1), j0c = j0 & ~3;
+            const bool staged = (j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4;
+            const int  nr     = (r1 - r0 + 1 + 3) / 4; // rp[r0 .. r1], r0 % 4 == 0
+            for(int k = lane; k < nr; k += 32)
+                cp_async16(sr + 4 * k, A.rp + r0 + 4 * k);
+            if(staged)
+            {
+                const int nv = (j1 - j0v + VPC - 1) / VPC;
+                const int nc = (j1 - j0c + 3) / 4;
+                for(int k = lane; k < nv; k += 32)
+                    cp_async16(sv + (size_t)k * VPC, A.v + j0v + (size_t)k * VPC);
+                for(int k = lane; k < nc; k += 32)
+                    cp_async16(sc + (size_t)k * 4, A.ci + j0c + (size_t)k * 4);
+            }
+            cp_async_commit();
+            cp_async_wait_group<0>();
+            __syncwarp();
+            const int row = r0 + lane;
+            if(row < r1)
+            {
+                const int a = sr[lane], b = sr[lane + 1];
+                AT        s = AT(0);
+                if(staged)
+                {
+                    constexpr int CH = 16;
+#pragma unroll
+                    for(int c0 = 0; c0 < MAXR; c0 += CH)
+                    {
+                        AT xv[CH];
+#pragma unroll
+                        for(int q = 0; q < CH; q++)
+                            if(a + c0 + q < b)
+                                xv[q] = op.gather(sc[a + c0 + q - j0c]);
+#pragma unroll
+                        for(int q = 0; q < CH; q++)
+                            if(a + c0 + q < b)
+                                s = acc_step<Op::kFma>(to_acc(sv[a + c0 + q - j0v], AT(0)), xv[q],
+                                                       s);
+                    }
+                }
+                else
+                {
+                    for(int j = a; j < b; j++)
+                        s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), op.gather(A.ci[j]), s);
+                }
+                contrib += op.finish(row, s);
+            }
+            __syncwarp(); // the region is refilled by the warp's next tile
+        }
+        if(Op::kReduce)
+            reduce_finish_sum<32 * kWarpPipeWarps>(contrib, red.partial, red.counter, red.out);
+    }
+
+    // ROWSEQ schedule for rows longer than 32 entries (coarse AMG levels): one
+    // thread per row, the row walked in segments of SEG entries whose values,
+    // columns and gathers are all issued before that segment's part of the
+    // accumulation chain (CSR order, bit-identical to the reference host SpMV).
+    // A lane's SEG consecutive entries share one or two L1 lines, so the strided
+    // pattern across the warp costs L1 wavefronts, not DRAM traffic.
+    constexpr int kSegLen = 8;
+
+    template <class Op, int NT>
+    __global__ void __launch_bounds__(NT)
+        k_row_seg(csr_view<typename Op::val_t> A, Op op, red_buf red)
+    {
+        using AT = typename Op::acc_t;
+        if(red.skip && *red.skip)
+            return;
+        double    contrib = 0.0;
+        const int row     = blockIdx.x * NT + threadIdx.x;
+        if(row < A.m)
+        {
+            const int a = A.rp[row], b = A.rp[row + 1];
+            AT        s = AT(0);
+            for(int c0 = a; c0 < b; c0 += kSegLen)
+            {
+                AT vv[kSegLen], xv[kSegLen];
+#pragma unroll
+                for(int q = 0; q < kSegLen; q++)
+                    if(c0 + q < b)
+                    {
+                        vv[q] = to_acc(A.v[c0 + q], AT(0));
+                        xv[q] = op.gather(A.ci[c0 + q]);
+                    }
+#pragma unroll
+                for(int q = 0; q < kSegLen; q++)
+                    if(c0 + q < b)
+                        s = acc_step<Op::kFma>(vv[q], xv[q], s);
+            }
+            contrib = op.finish(row, s);
+        }
+        if(Op::kReduce)
+            reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
+    }
+
     // VECTOR schedule: W lanes per row, loads straight from global memory (the W
     // lanes read consecutive entries, so they coalesce without staging),
     // lane-strided partial sums and an xor-shuffle reduction.
@@ -377,9 +436,58 @@ namespace lab
         const int      ntiles = (int)ceil_div<int64_t>(V.m, kRowseqNT);
         const size_t   smem   = 2 * pipe_stage_bytes<VT>(cap, kRowseqNT);
         const int      occ    = pipe_occupancy<Op, MAXR>(smem);
-        const unsigned grid   = (unsigned)std::min<int64_t>(ntiles, (int64_t)num_sms() * occ);
+        const unsigned grid   = (unsigned)std::min<int64_t>(
+            std::min<int64_t>(ntiles, (int64_t)num_sms() * occ), kRedBlocks);
         LAB_LAUNCH((k_pipe<Op, kRowseqNT, MAXR>), grid, kRowseqNT, smem, s, V, op, cap, red,
                    ntiles);
+        return LAB_OK;
+    }
+
+    template <class Op, int MAXR>
+    lab_status launch_pipe_warp(const csr_view<typename Op::val_t>& V, const Op& op, int cap,
+                                cudaStream_t s, const red_buf& red)
+    {
+        using VT                    = typename Op::val_t;
+        constexpr int  NT           = 32 * kWarpPipeWarps;
+        const auto     kernel       = k_pipe_warp<Op, MAXR>;
+        const int      ntiles       = (int)ceil_div<int64_t>(V.m, 32);
+        const size_t   smem         = kWarpPipeWarps * warp_stage_bytes<VT>(cap);
+        static std::mutex            mu;
+        static std::map<size_t, int> cache;
+        static const cudaError_t     attr = cudaFuncSetAttribute(
+            kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        LAB_CUDA(attr);
+        int occ = 1;
+        {
+            std::lock_guard<std::mutex> g(mu);
+            auto                        it = cache.find(smem);
+            if(it == cache.end())
+            {
+                int o = 0;
+                if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, NT, smem) != cudaSuccess)
+                {
+                    cudaGetLastError();
+                    o = 1;
+                }
+                it = cache.emplace(smem, std::max(o, 1)).first;
+            }
+            occ = it->second;
+        }
+        // persistent grid, at most kRedBlocks CTAs (the reduction partial buffers)
+        const unsigned grid = (unsigned)std::min<int64_t>(
+            std::min<int64_t>(ceil_div<int64_t>(ntiles, kWarpPipeWarps), (int64_t)num_sms() * occ),
+            kRedBlocks);
+        LAB_LAUNCH((k_pipe_warp<Op, MAXR>), grid, NT, smem, s, V, op, cap, red, ntiles);
+        return LAB_OK;
+    }
+
+    template <class Op>
+    lab_status launch_row_seg(const csr_view<typename Op::val_t>& V, const Op& op,
+                              cudaStream_t s, const red_buf& red)
+    {
+        // one thread per row: ceil(m / 256) CTAs, the ROWSEQ partial-buffer size
+        const unsigned grid = (unsigned)ceil_div<int64_t>(V.m, kRowseqNT);
+        LAB_LAUNCH((k_row_seg<Op, kRowseqNT>), grid, kRowseqNT, 0, s, V, op, red);
         return LAB_OK;
     }
 
@@ -408,21 +516,8 @@ namespace lab
             if(mr <= 16)
                 return launch_pipe<Op, 16>(V, op, kRowseqNT * mr, s, red);
             if(mr <= 32)
-                return launch_pipe<Op, 32>(V, op, kRowseqNT * mr, s, red);
-            // long rows forced onto one thread each: unbounded loop, staged when it fits
-            int    cap  = kRowseqNT * mr;
-            size_t smem = rowseq_smem<VT>(cap);
-            if(smem > 200 * 1024)
-            {
-                cap  = 0;
-                smem = rowseq_smem<VT>(0);
-            }
-            static const cudaError_t attr0 = cudaFuncSetAttribute(
-                k_rowseq<Op, kRowseqNT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            LAB_CUDA(attr0);
-            LAB_LAUNCH((k_rowseq<Op, kRowseqNT, 0>), (unsigned)rowop_grid(A), kRowseqNT, smem, s,
-                       V, op, cap, red);
-            return LAB_OK;
+                return launch_pipe_warp<Op, 32>(V, op, 32 * mr, s, red);
+            return launch_row_seg<Op>(V, op, s, red);
         }
         const unsigned grid = (unsigned)rowop_grid(A);
         switch(p.lanes)

@@ -30,14 +30,16 @@ def test_save_load_roundtrip_bit_exact(gpu, tmp_path, kind, make):
         for X, Y in pairs:
             x, y = X.to_numpy(), Y.to_numpy()
             assert csr_equal(x, y), (l, csr_diff(x, y))
+    # (RS levels can hold the reference's 0/0 NaN, rsamg.cpp:838-839, so a cycle may
+    # be all NaN: then both must be)
     r = gpu.vec(np.random.default_rng(0).uniform(-1, 1, A[0].size - 1))
-    assert np.array_equal(H.cycle(r).cpu().numpy(), G.cycle(r).cpu().numpy())
+    assert np.array_equal(H.cycle(r).cpu().numpy(), G.cycle(r).cpu().numpy(), equal_nan=True)
     b = gpu.vec(P.rhs_from_solution(*A, seed=1)[0])
     ctl = gpu.iter_control(rel_tol=1e-8, abs_tol=0.0)
     x1, i1 = gpu.pcg(dA, b, M=gpu.Preconditioner.amg(H), control=ctl)
     x2, i2 = gpu.pcg(dA, b, M=gpu.Preconditioner.amg(G), control=ctl)
-    assert i1.iterations == i2.iterations
-    assert np.array_equal(x1.cpu().numpy(), x2.cpu().numpy())
+    assert (i1.iterations, i1.status) == (i2.iterations, i2.status)
+    assert np.array_equal(x1.cpu().numpy(), x2.cpu().numpy(), equal_nan=True)
 
 
 def test_damaged_and_foreign_files_are_refused(gpu, tmp_path):
