@@ -172,6 +172,8 @@ namespace lab
             cudaFree(A->lp.bf16);
         if(A->lp.invd32)
             cudaFree(A->lp.invd32);
+        if(A->lp.dcol)
+            cudaFree(A->lp.dcol);
         A->lp = csr_values_lp();
     }
 

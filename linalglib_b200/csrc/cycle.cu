@@ -433,6 +433,32 @@ namespace lab
     }
 
     // FP32 (or BF16) value copies of a matrix and its FP32 inverse diagonal.
+    // 1 in *wide when some column offset col - row leaves the int16 range.
+    __global__ void k_dcol_check(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                 int64_t m, int* wide)
+    {
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+            i += (int64_t)gridDim.x * blockDim.x)
+            for(int j = rp[i]; j < rp[i + 1]; j++)
+            {
+                const int64_t d = (int64_t)ci[j] - i;
+                if(d < INT16_MIN || d > INT16_MAX)
+                {
+                    atomicOr(wide, 1);
+                    break;
+                }
+            }
+    }
+
+    __global__ void k_dcol_fill(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                int64_t m, int16_t* __restrict__ dcol)
+    {
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+            i += (int64_t)gridDim.x * blockDim.x)
+            for(int j = rp[i]; j < rp[i + 1]; j++)
+                dcol[j] = (int16_t)(ci[j] - (int)i);
+    }
+
     lab_status csr_ensure_lowp(lab_csr_impl* A, int precision, int use_bf16, cudaStream_t s)
     {
         if(precision == LAB_PREC_FP64)
@@ -450,6 +476,26 @@ namespace lab
             LAB_TRY(dalloc(&A->lp.f32, (size_t)nz, s));
             if(A->nnz)
                 LAB_LAUNCH(k_vals_f32, g, 256, 0, s, (const double*)A->val, A->nnz, A->lp.f32);
+        }
+        if(A->lp.dcol_state == 0 && A->m > 0 && A->nnz > 0)
+        {
+            // compact 16-bit column offsets when every |col - row| fits
+            dbuf<int> wide;
+            LAB_TRY(wide.alloc(1, s));
+            LAB_CUDA(cudaMemsetAsync(wide.get(), 0, sizeof(int), s));
+            LAB_LAUNCH(k_dcol_check, grid_for(A->m), 256, 0, s, A->row_ptr, A->col_ind, A->m,
+                       wide.get());
+            int h = 1;
+            LAB_TRY(copy_d2h_sync(&h, wide.get(), sizeof(int), s));
+            if(h)
+                A->lp.dcol_state = -1;
+            else
+            {
+                LAB_TRY(dalloc(&A->lp.dcol, (size_t)A->nnz, s));
+                LAB_LAUNCH(k_dcol_fill, grid_for(A->m), 256, 0, s, A->row_ptr, A->col_ind, A->m,
+                           A->lp.dcol);
+                A->lp.dcol_state = 1;
+            }
         }
         if(A->m == A->n && !A->lp.invd32)
         {

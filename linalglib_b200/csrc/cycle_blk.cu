@@ -163,7 +163,7 @@ namespace lab
         constexpr int CH  = (16 / K) > 0 ? 16 / K : 1;
         extern __shared__ __align__(16) unsigned char smem_raw[];
         const size_t sv_b    = ((size_t)(cap + 16) * sizeof(double) + 15) / 16 * 16;
-        const size_t sc_b    = ((size_t)(cap + 8) * 4 + 15) / 16 * 16;
+        const size_t sc_b    = ((size_t)(cap + 16) * 4 + 15) / 16 * 16;
         const size_t stage_b = pipe_stage_bytes<double>(cap, NT);
         if(skip && *skip)
             return;

@@ -137,6 +137,10 @@ namespace lab
         float*          f32  = nullptr;
         __nv_bfloat16*  bf16 = nullptr;
         float*          invd32 = nullptr;
+        // column minus row as int16 (when every offset fits), read with the
+        // reduced-precision values: 2 instead of 4 index bytes per entry
+        int16_t*        dcol       = nullptr;
+        int             dcol_state = 0; // 0 not examined, 1 built, -1 offsets too wide
     };
 
     // Unique ids for cached solver state (graphs are keyed by object identity,

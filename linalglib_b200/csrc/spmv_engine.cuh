@@ -25,6 +25,7 @@
 
 #include <map>
 #include <mutex>
+#include <type_traits>
 
 #include "reduce.cuh"
 
@@ -38,14 +39,26 @@ namespace lab
         const int*    skip    = nullptr; // kernel returns at once when *skip != 0
     };
 
-    template <class VT>
+    // CSR operand of a row kernel.  IT = int32_t: absolute column indices (the
+    // stored layout); IT = int16_t: column minus row, the compact copy kept with
+    // the reduced-precision values of a matrix whose offsets all fit in 16 bits.
+    template <class VT, class IT = int32_t>
     struct csr_view
     {
         const int32_t* rp;
-        const int32_t* ci;
+        const IT*      ci;
         const VT*      v;
         int32_t        m;
     };
+
+    template <class IT>
+    __device__ __forceinline__ int col_of(IT c, int row)
+    {
+        if constexpr(sizeof(IT) == 2)
+            return row + (int)c;
+        else
+            return (int)c;
+    }
 
     __device__ __forceinline__ double to_acc(double v, double)
     {
@@ -107,25 +120,26 @@ namespace lab
     // order: with kFma bit-identical to the reference host SpMV
     // (host_matrix_vector.cpp:60-84).  A tile whose nnz exceeds the stage capacity
     // is read straight from global memory (same arithmetic).
-    template <class VT>
+    template <class VT, class IT = int32_t>
     __host__ __device__ constexpr size_t pipe_stage_bytes(int cap, int rt)
     {
-        return ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16 + ((size_t)(cap + 8) * 4 + 15) / 16 * 16 +
-               ((size_t)(rt + 8) * 4 + 15) / 16 * 16;
+        return ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16 +
+               ((size_t)(cap + 16) * sizeof(IT) + 15) / 16 * 16 + ((size_t)(rt + 8) * 4 + 15) / 16 * 16;
     }
 
-    template <class Op, int NT, int MAXR>
+    template <class Op, int NT, int MAXR, class IT>
     __global__ void __launch_bounds__(NT)
-        k_pipe(csr_view<typename Op::val_t> A, Op op, int cap, red_buf red, int ntiles)
+        k_pipe(csr_view<typename Op::val_t, IT> A, Op op, int cap, red_buf red, int ntiles)
     {
         using VT = typename Op::val_t;
         using AT = typename Op::acc_t;
         constexpr int VPC = 16 / sizeof(VT);
+        constexpr int CPC = 16 / sizeof(IT);
         static_assert(NT % 4 == 0, "tile rows must keep 16-byte row-pointer chunks");
         extern __shared__ __align__(16) unsigned char smem_raw[];
         const size_t sv_b    = ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16;
-        const size_t sc_b    = ((size_t)(cap + 8) * 4 + 15) / 16 * 16;
-        const size_t stage_b = pipe_stage_bytes<VT>(cap, NT);
+        const size_t sc_b    = ((size_t)(cap + 16) * sizeof(IT) + 15) / 16 * 16;
+        const size_t stage_b = pipe_stage_bytes<VT, IT>(cap, NT);
         if(red.skip && *red.skip)
             return;
 
@@ -134,22 +148,22 @@ namespace lab
             const int      r1   = min(r0 + NT, A.m);
             const int      j0   = A.rp[r0];
             const int      j1   = A.rp[r1];
-            const int      j0v  = j0 & ~(VPC - 1), j0c = j0 & ~3;
+            const int      j0v  = j0 & ~(VPC - 1), j0c = j0 & ~(CPC - 1);
             unsigned char* base = smem_raw + stage * stage_b;
             int32_t*       sr   = reinterpret_cast<int32_t*>(base + sv_b + sc_b);
             const int      nr   = (r1 - r0 + 1 + 3) / 4; // rp[r0 .. r1], r0 % 4 == 0
             for(int k = threadIdx.x; k < nr; k += NT)
                 cp_async16(sr + 4 * k, A.rp + r0 + 4 * k);
-            if((j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4)
+            if((j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 8)
             {
                 VT*       sv = reinterpret_cast<VT*>(base);
-                int32_t*  sc = reinterpret_cast<int32_t*>(base + sv_b);
+                IT*       sc = reinterpret_cast<IT*>(base + sv_b);
                 const int nv = (j1 - j0v + VPC - 1) / VPC;
-                const int nc = (j1 - j0c + 3) / 4;
+                const int nc = (j1 - j0c + CPC - 1) / CPC;
                 for(int k = threadIdx.x; k < nv; k += NT)
                     cp_async16(sv + (size_t)k * VPC, A.v + j0v + (size_t)k * VPC);
                 for(int k = threadIdx.x; k < nc; k += NT)
-                    cp_async16(sc + (size_t)k * 4, A.ci + j0c + (size_t)k * 4);
+                    cp_async16(sc + (size_t)k * CPC, A.ci + j0c + (size_t)k * CPC);
             }
         };
 
@@ -168,13 +182,13 @@ namespace lab
             __syncthreads();
             const unsigned char* base   = smem_raw + (it & 1) * stage_b;
             const VT*            sv     = reinterpret_cast<const VT*>(base);
-            const int32_t*       sc     = reinterpret_cast<const int32_t*>(base + sv_b);
+            const IT*            sc     = reinterpret_cast<const IT*>(base + sv_b);
             const int32_t*       sr     = reinterpret_cast<const int32_t*>(base + sv_b + sc_b);
             const int            r0     = tile * NT;
             const int            r1     = min(r0 + NT, A.m);
             const int            j0     = sr[0], j1 = sr[r1 - r0];
-            const int            j0v    = j0 & ~(VPC - 1), j0c = j0 & ~3;
-            const bool           staged = (j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4;
+            const int            j0v    = j0 & ~(VPC - 1), j0c = j0 & ~(CPC - 1);
+            const bool           staged = (j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 8;
             const int            row    = r0 + threadIdx.x;
             if(row < r1)
             {
@@ -192,7 +206,7 @@ namespace lab
 #pragma unroll
                         for(int q = 0; q < CH; q++)
                             if(a + c0 + q < b)
-                                xv[q] = op.gather(sc[a + c0 + q - j0c]);
+                                xv[q] = op.gather(col_of<IT>(sc[a + c0 + q - j0c], row));
 #pragma unroll
                         for(int q = 0; q < CH; q++)
                             if(a + c0 + q < b)
@@ -203,12 +217,14 @@ namespace lab
                 else if(staged)
                 {
                     for(int j = a; j < b; j++)
-                        s = acc_step<Op::kFma>(to_acc(sv[j - j0v], AT(0)), op.gather(sc[j - j0c]), s);
+                        s = acc_step<Op::kFma>(to_acc(sv[j - j0v], AT(0)),
+                                               op.gather(col_of<IT>(sc[j - j0c], row)), s);
                 }
                 else
                 {
                     for(int j = a; j < b; j++)
-                        s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), op.gather(A.ci[j]), s);
+                        s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)),
+                                               op.gather(col_of<IT>(A.ci[j], row)), s);
                 }
                 contrib += op.finish(row, s);
             }
@@ -230,27 +246,28 @@ namespace lab
     // global memory directly.
     constexpr int kWarpPipeWarps = 4;
 
-    template <class VT>
+    template <class VT, class IT = int32_t>
     __host__ __device__ constexpr size_t warp_stage_bytes(int cap)
     {
-        return ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16 + ((size_t)(cap + 8) * 4 + 15) / 16 * 16 +
-               ((size_t)(32 + 8) * 4 + 15) / 16 * 16;
+        return ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16 +
+               ((size_t)(cap + 16) * sizeof(IT) + 15) / 16 * 16 + ((size_t)(32 + 8) * 4 + 15) / 16 * 16;
     }
 
-    template <class Op, int MAXR>
+    template <class Op, int MAXR, class IT>
     __global__ void __launch_bounds__(32 * kWarpPipeWarps)
-        k_pipe_warp(csr_view<typename Op::val_t> A, Op op, int cap, red_buf red, int ntiles)
+        k_pipe_warp(csr_view<typename Op::val_t, IT> A, Op op, int cap, red_buf red, int ntiles)
     {
         using VT = typename Op::val_t;
         using AT = typename Op::acc_t;
         constexpr int VPC = 16 / sizeof(VT);
+        constexpr int CPC = 16 / sizeof(IT);
         extern __shared__ __align__(16) unsigned char smem_raw[];
         const size_t   sv_b = ((size_t)(cap + 16) * sizeof(VT) + 15) / 16 * 16;
-        const size_t   sc_b = ((size_t)(cap + 8) * 4 + 15) / 16 * 16;
+        const size_t   sc_b = ((size_t)(cap + 16) * sizeof(IT) + 15) / 16 * 16;
         const int      wid  = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        unsigned char* base = smem_raw + (size_t)wid * warp_stage_bytes<VT>(cap);
+        unsigned char* base = smem_raw + (size_t)wid * warp_stage_bytes<VT, IT>(cap);
         VT*            sv   = reinterpret_cast<VT*>(base);
-        int32_t*       sc   = reinterpret_cast<int32_t*>(base + sv_b);
+        IT*            sc   = reinterpret_cast<IT*>(base + sv_b);
         int32_t*       sr   = reinterpret_cast<int32_t*>(base + sv_b + sc_b);
         if(red.skip && *red.skip)
             return;
@@ -262,19 +279,19 @@ namespace lab
             const int  r1     = min(r0 + 32, A.m);
             const int  j0     = A.rp[r0];
             const int  j1     = A.rp[r1];
-            const int  j0v    = j0 & ~(VPC - 1), j0c = j0 & ~3;
-            const bool staged = (j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 4;
+            const int  j0v    = j0 & ~(VPC - 1), j0c = j0 & ~(CPC - 1);
+            const bool staged = (j1 - j0v) <= cap + 8 && (j1 - j0c) <= cap + 8;
             const int  nr     = (r1 - r0 + 1 + 3) / 4; // rp[r0 .. r1], r0 % 4 == 0
             for(int k = lane; k < nr; k += 32)
                 cp_async16(sr + 4 * k, A.rp + r0 + 4 * k);
             if(staged)
             {
                 const int nv = (j1 - j0v + VPC - 1) / VPC;
-                const int nc = (j1 - j0c + 3) / 4;
+                const int nc = (j1 - j0c + CPC - 1) / CPC;
                 for(int k = lane; k < nv; k += 32)
                     cp_async16(sv + (size_t)k * VPC, A.v + j0v + (size_t)k * VPC);
                 for(int k = lane; k < nc; k += 32)
-                    cp_async16(sc + (size_t)k * 4, A.ci + j0c + (size_t)k * 4);
+                    cp_async16(sc + (size_t)k * CPC, A.ci + j0c + (size_t)k * CPC);
             }
             cp_async_commit();
             cp_async_wait_group<0>();
@@ -294,7 +311,7 @@ namespace lab
 #pragma unroll
                         for(int q = 0; q < CH; q++)
                             if(a + c0 + q < b)
-                                xv[q] = op.gather(sc[a + c0 + q - j0c]);
+                                xv[q] = op.gather(col_of<IT>(sc[a + c0 + q - j0c], row));
 #pragma unroll
                         for(int q = 0; q < CH; q++)
                             if(a + c0 + q < b)
@@ -305,7 +322,8 @@ namespace lab
                 else
                 {
                     for(int j = a; j < b; j++)
-                        s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), op.gather(A.ci[j]), s);
+                        s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)),
+                                               op.gather(col_of<IT>(A.ci[j], row)), s);
                 }
                 contrib += op.finish(row, s);
             }
@@ -323,9 +341,9 @@ namespace lab
     // pattern across the warp costs L1 wavefronts, not DRAM traffic.
     constexpr int kSegLen = 8;
 
-    template <class Op, int NT>
+    template <class Op, int NT, class IT>
     __global__ void __launch_bounds__(NT)
-        k_row_seg(csr_view<typename Op::val_t> A, Op op, red_buf red)
+        k_row_seg(csr_view<typename Op::val_t, IT> A, Op op, red_buf red)
     {
         using AT = typename Op::acc_t;
         if(red.skip && *red.skip)
@@ -344,7 +362,7 @@ namespace lab
                     if(c0 + q < b)
                     {
                         vv[q] = to_acc(A.v[c0 + q], AT(0));
-                        xv[q] = op.gather(A.ci[c0 + q]);
+                        xv[q] = op.gather(col_of<IT>(A.ci[c0 + q], row));
                     }
 #pragma unroll
                 for(int q = 0; q < kSegLen; q++)
@@ -360,9 +378,9 @@ namespace lab
     // VECTOR schedule: W lanes per row, loads straight from global memory (the W
     // lanes read consecutive entries, so they coalesce without staging),
     // lane-strided partial sums and an xor-shuffle reduction.
-    template <class Op, int NT, int W>
+    template <class Op, int NT, int W, class IT>
     __global__ void __launch_bounds__(NT)
-        k_vector(csr_view<typename Op::val_t> A, Op op, red_buf red)
+        k_vector(csr_view<typename Op::val_t, IT> A, Op op, red_buf red)
     {
         using AT = typename Op::acc_t;
         if(red.skip && *red.skip)
@@ -375,7 +393,8 @@ namespace lab
             const int a = A.rp[row], b = A.rp[row + 1];
 #pragma unroll 4
             for(int j = a + lane; j < b; j += W)
-                s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), op.gather(A.ci[j]), s);
+                s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), op.gather(col_of<IT>(A.ci[j], row)),
+                                       s);
         }
 #pragma unroll
         for(int o = W / 2; o > 0; o >>= 1)
@@ -403,10 +422,10 @@ namespace lab
 
     // Blocks per SM of one k_pipe instantiation at a given dynamic shared-memory
     // size (cached; the stage size differs per matrix).
-    template <class Op, int MAXR>
+    template <class Op, int MAXR, class IT>
     int pipe_occupancy(size_t smem)
     {
-        const auto                   kernel = k_pipe<Op, kRowseqNT, MAXR>;
+        const auto                   kernel = k_pipe<Op, kRowseqNT, MAXR, IT>;
         static std::mutex            mu;
         static std::map<size_t, int> cache;
         static const cudaError_t     attr = cudaFuncSetAttribute(
@@ -428,30 +447,30 @@ namespace lab
         return occ;
     }
 
-    template <class Op, int MAXR>
-    lab_status launch_pipe(const csr_view<typename Op::val_t>& V, const Op& op, int cap,
+    template <class Op, int MAXR, class IT>
+    lab_status launch_pipe(const csr_view<typename Op::val_t, IT>& V, const Op& op, int cap,
                            cudaStream_t s, const red_buf& red)
     {
         using VT              = typename Op::val_t;
         const int      ntiles = (int)ceil_div<int64_t>(V.m, kRowseqNT);
-        const size_t   smem   = 2 * pipe_stage_bytes<VT>(cap, kRowseqNT);
-        const int      occ    = pipe_occupancy<Op, MAXR>(smem);
+        const size_t   smem   = 2 * pipe_stage_bytes<VT, IT>(cap, kRowseqNT);
+        const int      occ    = pipe_occupancy<Op, MAXR, IT>(smem);
         const unsigned grid   = (unsigned)std::min<int64_t>(
             std::min<int64_t>(ntiles, (int64_t)num_sms() * occ), kRedBlocks);
-        LAB_LAUNCH((k_pipe<Op, kRowseqNT, MAXR>), grid, kRowseqNT, smem, s, V, op, cap, red,
+        LAB_LAUNCH((k_pipe<Op, kRowseqNT, MAXR, IT>), grid, kRowseqNT, smem, s, V, op, cap, red,
                    ntiles);
         return LAB_OK;
     }
 
-    template <class Op, int MAXR>
-    lab_status launch_pipe_warp(const csr_view<typename Op::val_t>& V, const Op& op, int cap,
+    template <class Op, int MAXR, class IT>
+    lab_status launch_pipe_warp(const csr_view<typename Op::val_t, IT>& V, const Op& op, int cap,
                                 cudaStream_t s, const red_buf& red)
     {
         using VT                    = typename Op::val_t;
         constexpr int  NT           = 32 * kWarpPipeWarps;
-        const auto     kernel       = k_pipe_warp<Op, MAXR>;
+        const auto     kernel       = k_pipe_warp<Op, MAXR, IT>;
         const int      ntiles       = (int)ceil_div<int64_t>(V.m, 32);
-        const size_t   smem         = kWarpPipeWarps * warp_stage_bytes<VT>(cap);
+        const size_t   smem         = kWarpPipeWarps * warp_stage_bytes<VT, IT>(cap);
         static std::mutex            mu;
         static std::map<size_t, int> cache;
         static const cudaError_t     attr = cudaFuncSetAttribute(
@@ -477,28 +496,64 @@ namespace lab
         const unsigned grid = (unsigned)std::min<int64_t>(
             std::min<int64_t>(ceil_div<int64_t>(ntiles, kWarpPipeWarps), (int64_t)num_sms() * occ),
             kRedBlocks);
-        LAB_LAUNCH((k_pipe_warp<Op, MAXR>), grid, NT, smem, s, V, op, cap, red, ntiles);
+        LAB_LAUNCH((k_pipe_warp<Op, MAXR, IT>), grid, NT, smem, s, V, op, cap, red, ntiles);
         return LAB_OK;
     }
 
-    template <class Op>
-    lab_status launch_row_seg(const csr_view<typename Op::val_t>& V, const Op& op,
+    template <class Op, class IT>
+    lab_status launch_row_seg(const csr_view<typename Op::val_t, IT>& V, const Op& op,
                               cudaStream_t s, const red_buf& red)
     {
         // one thread per row: ceil(m / 256) CTAs, the ROWSEQ partial-buffer size
         const unsigned grid = (unsigned)ceil_div<int64_t>(V.m, kRowseqNT);
-        LAB_LAUNCH((k_row_seg<Op, kRowseqNT>), grid, kRowseqNT, 0, s, V, op, red);
+        LAB_LAUNCH((k_row_seg<Op, kRowseqNT, IT>), grid, kRowseqNT, 0, s, V, op, red);
         return LAB_OK;
     }
 
-    template <class Op, int W>
-    lab_status launch_vector(const csr_view<typename Op::val_t>& V, const Op& op, unsigned grid,
-                             cudaStream_t s, const red_buf& red)
+    template <class Op, int W, class IT>
+    lab_status launch_vector(const csr_view<typename Op::val_t, IT>& V, const Op& op,
+                             unsigned grid, cudaStream_t s, const red_buf& red)
     {
-        LAB_LAUNCH((k_vector<Op, kVectorNT, W>), grid, kVectorNT, 0, s, V, op, red);
+        LAB_LAUNCH((k_vector<Op, kVectorNT, W, IT>), grid, kVectorNT, 0, s, V, op, red);
         return LAB_OK;
     }
 
+    template <class Op, class IT>
+    lab_status launch_rowop_view(const lab_csr_impl* A, const csr_view<typename Op::val_t, IT>& V,
+                                 const Op& op, cudaStream_t s, const red_buf& red)
+    {
+        const spmv_plan& p = A->plan;
+        if(p.alg == LAB_SPMV_ROWSEQ)
+        {
+            const int mr = std::max(1, p.max_row);
+            if(mr <= 8)
+                return launch_pipe<Op, 8, IT>(V, op, kRowseqNT * mr, s, red);
+            if(mr <= 16)
+                return launch_pipe<Op, 16, IT>(V, op, kRowseqNT * mr, s, red);
+            if(mr <= 32)
+                return launch_pipe_warp<Op, 32, IT>(V, op, 32 * mr, s, red);
+            return launch_row_seg<Op, IT>(V, op, s, red);
+        }
+        const unsigned grid = (unsigned)rowop_grid(A);
+        switch(p.lanes)
+        {
+        case 2:
+            return launch_vector<Op, 2, IT>(V, op, grid, s, red);
+        case 4:
+            return launch_vector<Op, 4, IT>(V, op, grid, s, red);
+        case 8:
+            return launch_vector<Op, 8, IT>(V, op, grid, s, red);
+        case 16:
+            return launch_vector<Op, 16, IT>(V, op, grid, s, red);
+        default:
+            return launch_vector<Op, 32, IT>(V, op, grid, s, red);
+        }
+    }
+
+    // One CSR pass of `op` over A with the given value array.  Reduced-precision
+    // values read the matrix's 16-bit column offsets when it has them (compact
+    // storage of the mixed-precision cycle); FP64 values read the stored int32
+    // columns (the reference layout).
     template <class Op>
     lab_status launch_rowop(const lab_csr_impl* A, const typename Op::val_t* vals, const Op& op,
                             cudaStream_t s, red_buf red = red_buf())
@@ -506,33 +561,16 @@ namespace lab
         using VT = typename Op::val_t;
         if(A->m == 0)
             return LAB_OK;
-        csr_view<VT> V{A->row_ptr, A->col_ind, vals, (int32_t)A->m};
-        const spmv_plan& p = A->plan;
-        if(p.alg == LAB_SPMV_ROWSEQ)
+        if constexpr(!std::is_same<VT, double>::value)
         {
-            const int mr = std::max(1, p.max_row);
-            if(mr <= 8)
-                return launch_pipe<Op, 8>(V, op, kRowseqNT * mr, s, red);
-            if(mr <= 16)
-                return launch_pipe<Op, 16>(V, op, kRowseqNT * mr, s, red);
-            if(mr <= 32)
-                return launch_pipe_warp<Op, 32>(V, op, 32 * mr, s, red);
-            return launch_row_seg<Op>(V, op, s, red);
+            if(A->lp.dcol)
+            {
+                csr_view<VT, int16_t> V{A->row_ptr, A->lp.dcol, vals, (int32_t)A->m};
+                return launch_rowop_view<Op, int16_t>(A, V, op, s, red);
+            }
         }
-        const unsigned grid = (unsigned)rowop_grid(A);
-        switch(p.lanes)
-        {
-        case 2:
-            return launch_vector<Op, 2>(V, op, grid, s, red);
-        case 4:
-            return launch_vector<Op, 4>(V, op, grid, s, red);
-        case 8:
-            return launch_vector<Op, 8>(V, op, grid, s, red);
-        case 16:
-            return launch_vector<Op, 16>(V, op, grid, s, red);
-        default:
-            return launch_vector<Op, 32>(V, op, grid, s, red);
-        }
+        csr_view<VT, int32_t> V{A->row_ptr, A->col_ind, vals, (int32_t)A->m};
+        return launch_rowop_view<Op, int32_t>(A, V, op, s, red);
     }
 
     // ------------------------------------------------------------ basic ops
