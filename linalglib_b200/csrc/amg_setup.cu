@@ -115,6 +115,12 @@ namespace lab
         int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
         if(i >= m)
             return;
+        if(st[i] != 0)
+        {
+            // decided rows keep their state; their scans would change nothing
+            out[i] = st[i];
+            return;
+        }
         int bs = st[i], bh = hash[i], br = (int)i;
         for(int j = rp[i]; j < rp[i + 1]; j++)
         {
@@ -226,6 +232,12 @@ namespace lab
         const int     lane = threadIdx.x & 31;
         if(i >= m)
             return;
+        if(st[i] != 0)
+        {
+            if(lane == 0)
+                out[i] = st[i];
+            return;
+        }
         pmis_best v = pmis_scan_warp(rp, ci, conn, st, hash, (int)i,
                                      pmis_best{st[i], hash[i], -1, (int)i}, lane);
         // second scan over the winner's row, starting from the winner (position -1)

@@ -109,7 +109,9 @@ namespace lab
         }
     };
 
-    // y = R r
+    // y = R r; with x0 set, also x0 = omega D_c^-1 y: the coarse level's first
+    // Jacobi sweep from zero, the value op_pre0 would compute there, so the coarse
+    // pre-smoothing pass gathers one vector instead of two.
     template <class VT, class T>
     struct op_restrict
     {
@@ -119,6 +121,9 @@ namespace lab
         static constexpr bool kReduce = false;
         const T* __restrict__ r;
         T* __restrict__ y;
+        const T* __restrict__ invd_c = nullptr;
+        T omega                      = T(0);
+        T* __restrict__ x0           = nullptr;
         __device__ __forceinline__ T gather(int c) const
         {
             return __ldg(r + c);
@@ -126,6 +131,8 @@ namespace lab
         __device__ __forceinline__ double finish(int i, T s) const
         {
             y[i] = s;
+            if(x0)
+                x0[i] = omega * (__ldg(invd_c + i) * s);
             return 0.0;
         }
     };
@@ -852,9 +859,24 @@ namespace lab
     // 1 = W (269-390), 2 = F (392-513).  zero_guess: x enters as 0 (not read).
     // With `dv` (level 0 of the FP64 preconditioner) the kernel writing the final
     // x also accumulates (x, dv) into dot.out.
+    // The buffer a zero-guess Jacobi cycle on level l starts in: x, or the level's
+    // scratch vector when the number of Jacobi writes is odd, so the last write
+    // lands in x.
+    template <class T>
+    static T* cycle_start(hierarchy_impl* h, int l, int kind, T* x, const lab_amg_options* o)
+    {
+        const int visits = kind == 0 ? 1 : 2;
+        const int flips  = (o->n1 >= 1) ? (o->n1 - 1) + visits * (1 + o->n2)
+                                        : o->n1 + visits * (1 + o->n2);
+        return (flips & 1) ? lv<T>::t(h->ws[l]) : x;
+    }
+
+    // x0_ready: the caller's restriction already wrote omega D^-1 b into the
+    // buffer cycle_start() names (zero guess, Jacobi, n1 >= 1 only).
     template <class T>
     static lab_status cycle(hierarchy_impl* h, int l, int kind, T* x, const T* b, bool zero_guess,
-                            const cyc_ctx& c, red_buf dot = red_buf(), const T* dv = nullptr)
+                            const cyc_ctx& c, red_buf dot = red_buf(), const T* dv = nullptr,
+                            bool x0_ready = false)
     {
         const lab_amg_options* o = c.o;
         red_buf                rb;
@@ -915,10 +937,13 @@ namespace lab
         // ---- pre-smoothing + residual
         if(zero_guess && n1 >= 1 && jac)
         {
-            LAB_TRY(with_vals<T>(A, bf, [&](auto* vals) -> lab_status {
-                op_pre0<vt_of<decltype(vals)>, T> op{b, invd, (T)o->omega, cur, wr};
-                return launch_rowop(A, vals, op, c.s, rb);
-            }));
+            if(x0_ready)
+                LAB_TRY(residual()); // cur = omega D^-1 b already
+            else
+                LAB_TRY(with_vals<T>(A, bf, [&](auto* vals) -> lab_status {
+                    op_pre0<vt_of<decltype(vals)>, T> op{b, invd, (T)o->omega, cur, wr};
+                    return launch_rowop(A, vals, op, c.s, rb);
+                }));
             for(int k = 1; k < n1; k++)
             {
                 T* res = nullptr;
@@ -943,11 +968,15 @@ namespace lab
 
         // ---- restrict, recurse, correct
         auto coarse_correct = [&](bool cz, int ckind, bool last) -> lab_status {
+            // fuse the coarse level's first sweep from zero into the restriction
+            const bool fuse_x0 = cz && jac && n1 >= 1 && l + 1 < h->levels;
+            T*         x0      = fuse_x0 ? cycle_start<T>(h, l + 1, ckind, cx, o) : nullptr;
             LAB_TRY(with_vals<T>(R, bf, [&](auto* vals) -> lab_status {
-                op_restrict<vt_of<decltype(vals)>, T> op{wr, cb};
+                op_restrict<vt_of<decltype(vals)>, T> op{wr, cb, lv<T>::invd(h->A[l + 1]),
+                                                         (T)o->omega, x0};
                 return launch_rowop(R, vals, op, c.s, rb);
             }));
-            LAB_TRY(cycle<T>(h, l + 1, ckind, cx, cb, cz, c));
+            LAB_TRY(cycle<T>(h, l + 1, ckind, cx, cb, cz, c, red_buf(), nullptr, fuse_x0));
             const bool fuse = last && dv && n2 == 0 && kind == 0;
             T*         dst  = jac ? oth : cur;
             LAB_TRY(with_vals<T>(P, bf, [&](auto* vals) -> lab_status {
