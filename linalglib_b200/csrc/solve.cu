@@ -113,11 +113,17 @@ namespace lab
         const double* key_x   = nullptr;
         uint64_t      key_A   = 0;
         cudaStream_t  key_s   = nullptr;
+        // iterative-refinement vectors (mixed precision): kept with the matrix so the
+        // inner solve's iteration graph (keyed by its x = ir_e) is captured once
+        double*       ir_r   = nullptr;
+        double*       ir_e   = nullptr;
+        double*       ir_sc  = nullptr;
+        unsigned int* ir_cnt = nullptr;
         ~pcg_ws()
         {
             if(graph)
                 cudaGraphExecDestroy(graph);
-            void* dp[] = {r, z, p, q, sc, flags, partial, counters};
+            void* dp[] = {r, z, p, q, sc, flags, partial, counters, ir_r, ir_e, ir_sc, ir_cnt};
             for(void* x : dp)
                 if(x)
                     cudaFree(x);
@@ -455,14 +461,26 @@ namespace lab
                                  cudaStream_t s)
     {
         const int64_t m = A->m;
-        dbuf<double>  r, e, sc;
-        dbuf<unsigned int> cnt;
-        LAB_TRY(r.alloc((size_t)m + 1, s));
-        LAB_TRY(e.alloc((size_t)m + 1, s));
-        LAB_TRY(sc.alloc((size_t)kRedBlocks + 4, s));
-        LAB_TRY(cnt.alloc(2, s));
-        LAB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(unsigned int) * 2, s));
-        red_buf rb{sc.get() + 4, cnt.get(), sc.get(), nullptr};
+        pcg_ws*       w = nullptr;
+        {
+            std::lock_guard<std::mutex> g(g_pcg_mu);
+            auto                        it = g_pcg_cache.find(A);
+            if(it == g_pcg_cache.end())
+                it = g_pcg_cache.emplace(A, new pcg_ws()).first;
+            w = it->second;
+        }
+        if(!w->ir_r)
+        {
+            LAB_TRY(dalloc(&w->ir_r, (size_t)m + 1, s));
+            LAB_TRY(dalloc(&w->ir_e, (size_t)m + 1, s));
+            LAB_TRY(dalloc(&w->ir_sc, (size_t)kRedBlocks + 4, s));
+            LAB_TRY(dalloc(&w->ir_cnt, 2, s));
+            LAB_CUDA(cudaMemsetAsync(w->ir_cnt, 0, sizeof(unsigned int) * 2, s));
+        }
+        double* r  = w->ir_r;
+        double* e  = w->ir_e;
+        double* sc = w->ir_sc;
+        red_buf rb{w->ir_sc + 4, w->ir_cnt, w->ir_sc, nullptr};
         cudaEvent_t t0, t1;
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
@@ -473,12 +491,12 @@ namespace lab
         lab_status st = LAB_OK;
         for(int outer = 0; outer < 50; outer++)
         {
-            op_residual opr{x, b, r.get()};
+            op_residual opr{x, b, r};
             if((st = launch_rowop(A, A->val, opr, s)) != LAB_OK)
                 break;
-            if((st = norm_inf_device(m, r.get(), rb, s)) != LAB_OK)
+            if((st = norm_inf_device(m, r, rb, s)) != LAB_OK)
                 break;
-            if((st = copy_d2h_sync(&rn, sc.get(), sizeof(double), s)) != LAB_OK)
+            if((st = copy_d2h_sync(&rn, sc, sizeof(double), s)) != LAB_OK)
                 break;
             if(outer == 0)
                 r0 = rn;
@@ -500,13 +518,13 @@ namespace lab
             inner.rel_tol          = ctl->rel_tol * r0 / rn;
             inner.max_iter         = ctl->max_iter - total;
             lab_solve_info ii{};
-            cudaMemsetAsync(e.get(), 0, sizeof(double) * m, s);
-            st = pcg_solve(A, M, r.get(), e.get(), &inner, &ii, s);
+            cudaMemsetAsync(e, 0, sizeof(double) * m, s);
+            st = pcg_solve(A, M, r, e, &inner, &ii, s);
             if(st != LAB_OK && st != LAB_NOT_CONVERGED)
                 break;
             st = LAB_OK;
             total += ii.iterations + (ii.converged ? 0 : 1);
-            if((st = lab_axpy(m, 1.0, e.get(), x, s)) != LAB_OK)
+            if((st = lab_axpy(m, 1.0, e, x, s)) != LAB_OK)
                 break;
         }
         cudaEventRecord(t1, s);

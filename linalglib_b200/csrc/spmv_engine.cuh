@@ -375,26 +375,83 @@ namespace lab
             reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
     }
 
-    // VECTOR schedule: W lanes per row, loads straight from global memory (the W
-    // lanes read consecutive entries, so they coalesce without staging),
-    // lane-strided partial sums and an xor-shuffle reduction.
+    // Four consecutive entries from a 4-aligned position, as wide loads.
+    __device__ __forceinline__ void ld4(const double* p, double (&o)[4])
+    {
+        const double2 u = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 w = __ldg(reinterpret_cast<const double2*>(p + 2));
+        o[0] = u.x, o[1] = u.y, o[2] = w.x, o[3] = w.y;
+    }
+    __device__ __forceinline__ void ld4(const float* p, float (&o)[4])
+    {
+        const float4 u = __ldg(reinterpret_cast<const float4*>(p));
+        o[0] = u.x, o[1] = u.y, o[2] = u.z, o[3] = u.w;
+    }
+    __device__ __forceinline__ void ld4(const __nv_bfloat16* p, __nv_bfloat16 (&o)[4])
+    {
+        const uint2           u = __ldg(reinterpret_cast<const uint2*>(p));
+        const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&u);
+        o[0] = h[0], o[1] = h[1], o[2] = h[2], o[3] = h[3];
+    }
+    __device__ __forceinline__ void ld4(const int32_t* p, int32_t (&o)[4])
+    {
+        const int4 u = __ldg(reinterpret_cast<const int4*>(p));
+        o[0] = u.x, o[1] = u.y, o[2] = u.z, o[3] = u.w;
+    }
+    __device__ __forceinline__ void ld4(const int16_t* p, int16_t (&o)[4])
+    {
+        const uint2    u = __ldg(reinterpret_cast<const uint2*>(p));
+        const int16_t* h = reinterpret_cast<const int16_t*>(&u);
+        o[0] = h[0], o[1] = h[1], o[2] = h[2], o[3] = h[3];
+    }
+
+    // VECTOR schedule (rows longer than 32 entries): W lanes per row and an
+    // xor-shuffle reduction over the W lane sums.  FP64 values: lane-strided
+    // single entries.  Reduced-precision values: each lane takes aligned quads of
+    // entries with one wide load of values and one of columns (the row's first and
+    // last quads masked to [a, b)) and its four gathers in flight together; loads
+    // start at the row's aligned-down position and may run up to three entries
+    // past the matrix end, inside the allocations' padding.
     template <class Op, int NT, int W, class IT>
     __global__ void __launch_bounds__(NT)
         k_vector(csr_view<typename Op::val_t, IT> A, Op op, red_buf red)
     {
+        using VT = typename Op::val_t;
         using AT = typename Op::acc_t;
         if(red.skip && *red.skip)
             return;
         const int lane = threadIdx.x & (W - 1);
         const int row  = (int)(((int64_t)blockIdx.x * NT + threadIdx.x) / W);
         AT        s    = AT(0);
-        if(row < A.m)
+        if(row < A.m && sizeof(VT) == 8)
         {
+            // FP64 values: one entry per lane step (a quad would need two loads anyway)
             const int a = A.rp[row], b = A.rp[row + 1];
 #pragma unroll 4
             for(int j = a + lane; j < b; j += W)
                 s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), op.gather(col_of<IT>(A.ci[j], row)),
                                        s);
+        }
+        else if(row < A.m)
+        {
+            const int a = A.rp[row], b = A.rp[row + 1];
+#pragma unroll 2
+            for(int q = (a & ~3) + 4 * lane; q < b; q += 4 * W)
+            {
+                VT v4[4];
+                IT c4[4];
+                ld4(A.v + q, v4);
+                ld4(A.ci + q, c4);
+                AT xg[4];
+#pragma unroll
+                for(int t = 0; t < 4; t++)
+                    if(q + t >= a && q + t < b)
+                        xg[t] = op.gather(col_of<IT>(c4[t], row));
+#pragma unroll
+                for(int t = 0; t < 4; t++)
+                    if(q + t >= a && q + t < b)
+                        s = acc_step<Op::kFma>(to_acc(v4[t], AT(0)), xg[t], s);
+            }
         }
 #pragma unroll
         for(int o = W / 2; o > 0; o >>= 1)
