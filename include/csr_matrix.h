@@ -76,6 +76,9 @@ namespace linalg
         lab_csr device() const;
         // Adopt a device matrix produced by the library (owned or borrowed).
         void adopt(lab_csr A, bool owned);
+        // The library changed the device matrix's values in place: the host
+        // arrays are refreshed on their next read.
+        void device_changed();
         // Back to an empty 0 x 0 host matrix, dropping any device matrix.
         void reset();
     };

@@ -1,5 +1,6 @@
 // Preconditioner plug-in point (library/include/iterative_solvers/preconditioner/preconditioner.h:59-99)
-// with the Jacobi preconditioner (101-118) and the AMG preconditioner the
+// with the reference's Jacobi, Gauss-Seidel, SOR, ILU(0) and IC(0)
+// preconditioners (preconditioner.cpp:33-545) and the AMG preconditioner the
 // reference lacks: one multigrid cycle from a zero guess per application.
 #ifndef LINALG_B200_PRECONDITIONER_H
 #define LINALG_B200_PRECONDITIONER_H
@@ -47,6 +48,67 @@ namespace linalg
         {
             return M;
         }
+    };
+
+    // The triangular-solve preconditioners share one device implementation: build()
+    // copies A (and factors the copy for ILU(0) / IC(0)); solve() runs the
+    // level-scheduled triangular solves in the reference's arithmetic order.
+    class tri_precond_base : public preconditioner
+    {
+    protected:
+        lab_precond M       = nullptr;
+        bool        on_host = true;
+        void        rebuild(lab_precond created);
+
+    public:
+        ~tri_precond_base();
+        void        solve(const vector<double>& rhs, vector<double>& x) const override;
+        void        move_to_device() override;
+        void        move_to_host() override;
+        bool        is_on_host() const override;
+        lab_precond device_handle() const override
+        {
+            return M;
+        }
+    };
+
+    // x = (D + L)^-1 rhs (preconditioner.cpp:80-105)
+    class gauss_seidel_precond : public tri_precond_base
+    {
+    public:
+        gauss_seidel_precond() {}
+        void build(const csr_matrix<double>& A) override;
+    };
+
+    // x = (D / omega + L)^-1 rhs (preconditioner.cpp:121-156)
+    class SOR_precond : public tri_precond_base
+    {
+    private:
+        double omega;
+
+    public:
+        SOR_precond(double omega)
+            : omega(omega)
+        {
+        }
+        void build(const csr_matrix<double>& A) override;
+    };
+
+    // x = U^-1 L^-1 rhs with the in-place ILU(0) of a copy of A (preconditioner.cpp:418-467)
+    class ilu_precond : public tri_precond_base
+    {
+    public:
+        ilu_precond() {}
+        void build(const csr_matrix<double>& A) override;
+    };
+
+    // the IC(0) of a copy of A, then a lower and an upper solve on it
+    // (preconditioner.cpp:492-542)
+    class ic_precond : public tri_precond_base
+    {
+    public:
+        ic_precond() {}
+        void build(const csr_matrix<double>& A) override;
     };
 
     // AMG preconditioner: z = cycle(0; r).  build() runs the setup of `kind`

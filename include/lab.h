@@ -175,6 +175,19 @@ LAB_API lab_status lab_exclusive_scan_i32(int64_t n, int32_t* x, lab_stream s);
  * calls that overlap on the GPU (other streams, other threads) race. */
 LAB_API lab_status lab_exclusive_scan_i64_noalloc(int64_t n, int64_t* x, lab_stream s);
 
+/* Sparse triangular solve x = T^-1 b on the lower (columns < i) or upper part
+ * of A, unit or stored diagonal (csrtrsv_analysis / csrtrsv_solve,
+ * linalg_math.h:229-254; host_csrtrsv.cpp).  The level schedule is built on first
+ * use and kept with A. */
+LAB_API lab_status lab_csrtrsv(lab_csr A, int lower, int unit_diag, const double* b, double* x,
+                               lab_stream s);
+/* In-place incomplete factorizations of A's values: ILU(0) (csrilu0,
+ * linalg_math.h:109; host_csrilu0.cpp) and IC(0) (csric0, linalg_math.h:95;
+ * host_csric0.cpp, the upper part left unchanged).  The smallest column with a
+ * missing / zero pivot goes to *structural_zero / *numeric_zero (-1: none). */
+LAB_API lab_status lab_csrilu0(lab_csr A, int* structural_zero, int* numeric_zero, lab_stream s);
+LAB_API lab_status lab_csric0(lab_csr A, int* structural_zero, int* numeric_zero, lab_stream s);
+
 /* ------------------------------------------------------------------ sparse products */
 /* C = A*B (new matrix), rows sorted by column, each entry accumulated in A-row
  * then B-row order exactly as the reference host SpGEMM, so results are
@@ -344,6 +357,14 @@ LAB_API lab_status lab_precond_create_amg(lab_hierarchy h, const lab_amg_options
                                           lab_precond* M, lab_stream s);
 /* jacobi_precond (preconditioner.h:101-118; preconditioner.cpp:41-78). */
 LAB_API lab_status lab_precond_create_jacobi(lab_csr A, lab_precond* M, lab_stream s);
+/* Triangular-solve preconditioners (preconditioner.h:172-580): ILU(0) and IC(0)
+ * factor a copy of A (ilu_precond / ic_precond::build), Gauss-Seidel and SOR(omega)
+ * solve with A's lower part (gauss_seidel_precond, SOR_precond).  Each application
+ * runs the reference's triangular solves, level-scheduled, bit-identical. */
+LAB_API lab_status lab_precond_create_ilu0(lab_csr A, lab_precond* M, lab_stream s);
+LAB_API lab_status lab_precond_create_ic0(lab_csr A, lab_precond* M, lab_stream s);
+LAB_API lab_status lab_precond_create_gauss_seidel(lab_csr A, lab_precond* M, lab_stream s);
+LAB_API lab_status lab_precond_create_sor(lab_csr A, double omega, lab_precond* M, lab_stream s);
 /* z = M^{-1} r.  preconditioner::solve (preconditioner.h:78). */
 LAB_API lab_status lab_precond_apply(lab_precond M, const double* r, double* z, lab_stream s);
 LAB_API lab_status lab_precond_destroy(lab_precond M);

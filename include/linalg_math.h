@@ -23,6 +23,36 @@ namespace linalg
     double norm_euclid(const vector<double>& array);
     double norm_inf(const vector<double>& array);
 
+    // In-place incomplete factorizations (linalg_math.h:95, 109; host_csric0.cpp,
+    // host_csrilu0.cpp), computed on the GPU bit-identically to the reference's
+    // host loops.  As there, the column of a missing (structural) or zero
+    // (numeric) pivot is folded into *structural_zero / *numeric_zero with
+    // std::min, so callers initialise them (e.g. to INT_MAX); null is allowed.
+    void csric0(csr_matrix<double>& LL, int* structural_zero, int* numeric_zero);
+    void csrilu0(csr_matrix<double>& LU, int* structural_zero, int* numeric_zero);
+
+    // Sparse triangular solve on the lower or upper part of A (linalg_math.h:
+    // 198-254, linalg_enums.h:37-48).  The analysis builds the level schedule of
+    // A's pattern (cached on the matrix); x = T^-1 (alpha b).
+    enum class triangular_type
+    {
+        lower,
+        upper
+    };
+    enum class diagonal_type
+    {
+        non_unit,
+        unit
+    };
+    struct csrtrsv_descr;
+    void create_csrtrsv_descr(csrtrsv_descr** descr);
+    void destroy_csrtrsv_descr(csrtrsv_descr* descr);
+    void csrtrsv_analysis(const csr_matrix<double>& A, triangular_type tri_type,
+                          diagonal_type diag_type, csrtrsv_descr* descr);
+    void csrtrsv_solve(const csr_matrix<double>& A, const vector<double>& b, vector<double>& x,
+                       double alpha, triangular_type tri_type, diagonal_type diag_type,
+                       const csrtrsv_descr* descr);
+
     // csrmv descriptor: a cached SpMV plan (linalg_math.h:263-310)
     enum class csrmv_algorithm
     {

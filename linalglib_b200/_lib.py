@@ -99,6 +99,13 @@ _SIGS = {
     "lab_hierarchy_levels": [_p, C.POINTER(_i)],
     "lab_hierarchy_level": [_p, _i, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p)],
     "lab_hierarchy_setup_ms": [_p, C.POINTER(_d)],
+    "lab_csrtrsv": [_p, _i, _i, _p, _p, _p],
+    "lab_csrilu0": [_p, C.POINTER(_i), C.POINTER(_i), _p],
+    "lab_csric0": [_p, C.POINTER(_i), C.POINTER(_i), _p],
+    "lab_precond_create_ilu0": [_p, C.POINTER(_p), _p],
+    "lab_precond_create_ic0": [_p, C.POINTER(_p), _p],
+    "lab_precond_create_gauss_seidel": [_p, C.POINTER(_p), _p],
+    "lab_precond_create_sor": [_p, _d, C.POINTER(_p), _p],
     "lab_spmv_autotune": [_p, _i, C.POINTER(_d), _p],
     "lab_hierarchy_autotune": [_p, _i, _p],
     "lab_hierarchy_save": [_p, C.c_char_p, _p],

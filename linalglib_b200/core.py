@@ -167,6 +167,22 @@ class CsrMatrix:
     def transpose(self):
         return self._new("lab_transpose", self.h)
 
+    def trsv(self, b, lower=True, unit_diag=False, x=None):
+        """x = T^-1 b on the lower or upper part (level-scheduled, reference order)."""
+        if x is None:
+            x = torch.empty_like(b)
+        call("lab_csrtrsv", self.h, int(bool(lower)), int(bool(unit_diag)), ptr(b), ptr(x),
+             stream_handle())
+        return x
+
+    def factor(self, kind):
+        """In-place ILU(0) ('ilu0') or IC(0) ('ic0'); returns (structural_zero,
+        numeric_zero), -1 meaning none."""
+        sz, nz = C.c_int(), C.c_int()
+        call("lab_csrilu0" if kind == "ilu0" else "lab_csric0", self.h, C.byref(sz), C.byref(nz),
+             stream_handle())
+        return sz.value, nz.value
+
     def spgemm(self, B):
         return self._new("lab_spgemm", self.h, B.h)
 
@@ -322,6 +338,28 @@ class Preconditioner:
         h = C.c_void_p()
         call("lab_precond_create_jacobi", A.h, C.byref(h), stream_handle())
         return cls(h, keep=A)
+
+    @classmethod
+    def _tri(cls, fn, A, *extra):
+        h = C.c_void_p()
+        call(fn, A.h, *extra, C.byref(h), stream_handle())
+        return cls(h, keep=A)
+
+    @classmethod
+    def ilu0(cls, A: CsrMatrix):
+        return cls._tri("lab_precond_create_ilu0", A)
+
+    @classmethod
+    def ic0(cls, A: CsrMatrix):
+        return cls._tri("lab_precond_create_ic0", A)
+
+    @classmethod
+    def gauss_seidel(cls, A: CsrMatrix):
+        return cls._tri("lab_precond_create_gauss_seidel", A)
+
+    @classmethod
+    def sor(cls, A: CsrMatrix, omega: float):
+        return cls._tri("lab_precond_create_sor", A, C.c_double(omega))
 
     def apply(self, r, z=None):
         if z is None:

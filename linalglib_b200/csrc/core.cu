@@ -197,6 +197,7 @@ namespace lab
             cudaFree(A->invdiag);
         plan_release(A->plan);
         lp_release(A);
+        tri_release(A);
         delete static_cast<lab_csr_s*>(A);
     }
 

@@ -369,6 +369,13 @@ namespace linalg
     }
 
     template <typename T>
+    void csr_matrix<T>::device_changed()
+    {
+        if(dev)
+            host_valid = false;
+    }
+
+    template <typename T>
     void csr_matrix<T>::reset()
     {
         dev.reset();
@@ -776,6 +783,81 @@ namespace linalg
         ok(lab_spmv(alpha, A.device(), x.device_read(), beta, yp, nullptr), "csrmv_solve");
     }
 
+    // ============================================================ triangular path
+    static void fold_min(int* out, int col)
+    {
+        if(out && col >= 0)
+            *out = std::min(*out, col);
+    }
+    void csric0(csr_matrix<double>& LL, int* structural_zero, int* numeric_zero)
+    {
+        int sz = -1, nz = -1;
+        if(ok(lab_csric0(LL.device(), &sz, &nz, nullptr), "csric0"))
+        {
+            LL.device_changed();
+            fold_min(structural_zero, sz);
+            fold_min(numeric_zero, nz);
+        }
+    }
+    void csrilu0(csr_matrix<double>& LU, int* structural_zero, int* numeric_zero)
+    {
+        int sz = -1, nz = -1;
+        if(ok(lab_csrilu0(LU.device(), &sz, &nz, nullptr), "csrilu0"))
+        {
+            LU.device_changed();
+            fold_min(structural_zero, sz);
+            fold_min(numeric_zero, nz);
+        }
+    }
+
+    struct csrtrsv_descr
+    {
+        int analysed = 0;
+    };
+    void create_csrtrsv_descr(csrtrsv_descr** d)
+    {
+        *d = new csrtrsv_descr();
+    }
+    void destroy_csrtrsv_descr(csrtrsv_descr* d)
+    {
+        delete d;
+    }
+    void csrtrsv_analysis(const csr_matrix<double>& A, triangular_type, diagonal_type,
+                          csrtrsv_descr* d)
+    {
+        // the schedule is built and cached on the matrix by its first solve: a
+        // zero-length solve is not enough, so solve once into scratch
+        const int m = A.get_m();
+        if(m > 0)
+        {
+            vector<double> b(m), x(m);
+            b.zeros();
+            ok(lab_csrtrsv(A.device(), 1, 1, b.device_read(), x.device_write(), nullptr),
+               "csrtrsv_analysis");
+        }
+        if(d)
+            d->analysed = 1;
+    }
+    void csrtrsv_solve(const csr_matrix<double>& A, const vector<double>& b, vector<double>& x,
+                       double alpha, triangular_type tri_type, diagonal_type diag_type,
+                       const csrtrsv_descr*)
+    {
+        const int lower = tri_type == triangular_type::lower;
+        const int unit  = diag_type == diagonal_type::unit;
+        if(alpha == 1.0)
+        {
+            ok(lab_csrtrsv(A.device(), lower, unit, b.device_read(), x.device_write(), nullptr),
+               "csrtrsv_solve");
+            return;
+        }
+        vector<double> ab(b.get_size());
+        ab.zeros();
+        ok(lab_axpy(b.get_size(), alpha, b.device_read(), ab.device_readwrite(), nullptr),
+           "csrtrsv_solve");
+        ok(lab_csrtrsv(A.device(), lower, unit, ab.device_read(), x.device_write(), nullptr),
+           "csrtrsv_solve");
+    }
+
     void create_csrgeam_descr(csrgeam_descr** d)
     {
         *d = new csrgeam_descr();
@@ -1111,6 +1193,59 @@ namespace linalg
     bool jacobi_precond::is_on_host() const
     {
         return on_host;
+    }
+
+    void tri_precond_base::rebuild(lab_precond created)
+    {
+        if(M)
+            lab_precond_destroy(M);
+        M = created;
+    }
+    tri_precond_base::~tri_precond_base()
+    {
+        if(M)
+            lab_precond_destroy(M);
+    }
+    void tri_precond_base::solve(const vector<double>& rhs, vector<double>& x) const
+    {
+        ok(lab_precond_apply(M, rhs.device_read(), x.device_write(), nullptr),
+           "preconditioner::solve");
+    }
+    void tri_precond_base::move_to_device()
+    {
+        on_host = false;
+    }
+    void tri_precond_base::move_to_host()
+    {
+        on_host = true;
+    }
+    bool tri_precond_base::is_on_host() const
+    {
+        return on_host;
+    }
+    void gauss_seidel_precond::build(const csr_matrix<double>& A)
+    {
+        lab_precond P = nullptr;
+        ok(lab_precond_create_gauss_seidel(A.device(), &P, nullptr), "gauss_seidel_precond::build");
+        rebuild(P);
+    }
+    void SOR_precond::build(const csr_matrix<double>& A)
+    {
+        lab_precond P = nullptr;
+        ok(lab_precond_create_sor(A.device(), omega, &P, nullptr), "SOR_precond::build");
+        rebuild(P);
+    }
+    void ilu_precond::build(const csr_matrix<double>& A)
+    {
+        lab_precond P = nullptr;
+        ok(lab_precond_create_ilu0(A.device(), &P, nullptr), "ilu_precond::build");
+        rebuild(P);
+    }
+    void ic_precond::build(const csr_matrix<double>& A)
+    {
+        lab_precond P = nullptr;
+        ok(lab_precond_create_ic0(A.device(), &P, nullptr), "ic_precond::build");
+        rebuild(P);
     }
 
     amg_precond::amg_precond(int n1, int n2, cycle c, smoother s, double omega)

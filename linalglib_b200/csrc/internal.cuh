@@ -161,7 +161,9 @@ namespace lab
         double* diag    = nullptr;
         double* invdiag = nullptr;
         csr_values_lp lp;
+        struct tri_plan* tri = nullptr; // triangular-solve levels (tri.cu), on demand
     };
+    void tri_release(lab_csr_impl* A);
 
     lab_status csr_alloc(lab_csr_impl** A, int64_t m, int64_t n, int64_t nnz, cudaStream_t s);
     void       csr_release(lab_csr_impl* A);

@@ -1,6 +1,7 @@
 // Solve phase: fused multigrid cycles, preconditioners, PCG (device-resident
 // scalars, one CUDA graph per iteration), stationary AMG and GMRES.
 #include "cycle.cuh"
+#include "tri.cuh"
 
 #include <cmath>
 #include <map>
@@ -13,11 +14,21 @@ namespace lab
     struct precond_impl
     {
         uint64_t         uid  = next_uid();
-        int              kind = 0; // 0 = AMG, 1 = Jacobi
+        int              kind = 0; // 0 AMG, 1 Jacobi, 2 ILU(0), 3 IC(0), 4 Gauss-Seidel, 5 SOR
         hierarchy_impl*  h    = nullptr;
         lab_amg_options  o;
-        lab_csr_impl*    A    = nullptr; // Jacobi
+        lab_csr_impl*    A    = nullptr; // Jacobi, Gauss-Seidel, SOR: the operator
         double*          diag = nullptr; // Jacobi: the reference divides by the diagonal
+        lab_csr_impl*    F    = nullptr; // ILU(0) / IC(0): factored copy of the operator
+        double*          y    = nullptr; // ILU(0) / IC(0): intermediate of the two solves
+        double           dscale = 0.0;   // SOR: diagonal scale 1 / omega
+        ~precond_impl()
+        {
+            if(F)
+                csr_release(F);
+            if(y)
+                cudaFree(y);
+        }
     };
 
     __global__ void k_jacobi_dot(int64_t n, const double* __restrict__ r,
@@ -42,6 +53,22 @@ namespace lab
     static lab_status precond_apply(precond_impl* M, const double* r, double* z, cudaStream_t s,
                                     const int* skip, red_buf dot)
     {
+        if(M->kind >= 2)
+        {
+            // preconditioner.cpp: ILU(0) 452-467, IC(0) 527-542 (lower then upper
+            // solve of the factored copy), Gauss-Seidel 98-105 and SOR 149-156
+            // (one lower solve on A, SOR's diagonal scaled by 1 / omega)
+            if(M->kind == 2 || M->kind == 3)
+            {
+                LAB_TRY(tri_solve(M->F, true, M->kind == 2, 0.0, r, M->y, s, skip));
+                LAB_TRY(tri_solve(M->F, false, false, 0.0, M->y, z, s, skip));
+            }
+            else
+                LAB_TRY(tri_solve(M->F, true, false, M->dscale, r, z, s, skip));
+            if(dot.out)
+                LAB_TRY(dot_device(M->F->m, z, r, dot, s));
+            return LAB_OK;
+        }
         if(M->kind == 1)
         {
             int64_t n = M->A->m;
@@ -1495,6 +1522,67 @@ LAB_API lab_status lab_precond_create_jacobi(lab_csr A, lab_precond* out, lab_st
     M->diag = A->diag;
     *out    = M;
     return LAB_OK;
+}
+
+// ILU(0) / IC(0): factor a copy of A (ilu_precond::build, preconditioner.cpp:432-450;
+// ic_precond::build, 506-524).  Gauss-Seidel / SOR: solve with the lower part of
+// a copy of A (gauss_seidel_precond::build 90-96, SOR_precond::build 137-147).
+static lab_status create_tri_precond(lab_csr A, int kind, double omega, lab_precond* out,
+                                     lab_stream ls)
+{
+    LAB_ARG(A && out, "null argument");
+    LAB_ARG(A->m == A->n, "square matrix required");
+    LAB_TRY(ensure_init());
+    cudaStream_t   s = to_stream(ls);
+    lab_precond_s* M = new(std::nothrow) lab_precond_s();
+    if(!M)
+        return LAB_OOM;
+    M->kind       = kind;
+    M->A          = A;
+    M->dscale     = kind == 5 ? 1.0 / omega : 0.0; // SOR: scale_diagonal_by(1.0 / omega)
+    // like the reference's build(), every kind works on its own copy of A
+    lab_csr    F  = nullptr;
+    lab_status st = lab_csr_clone(A, &F, ls);
+    if(st == LAB_OK)
+    {
+        M->F = F;
+        st   = tri_analyse(M->F, s);
+    }
+    if(st == LAB_OK && (kind == 2 || kind == 3))
+    {
+        int sz = -1, nz = -1;
+        st = tri_factor(M->F, kind == 3, &sz, &nz, s);
+        if(st == LAB_OK)
+            st = dalloc(&M->y, (size_t)A->m + 1, s);
+    }
+    if(st != LAB_OK)
+    {
+        delete M;
+        return st;
+    }
+    *out = M;
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_precond_create_ilu0(lab_csr A, lab_precond* M, lab_stream s)
+{
+    return create_tri_precond(A, 2, 0.0, M, s);
+}
+
+LAB_API lab_status lab_precond_create_ic0(lab_csr A, lab_precond* M, lab_stream s)
+{
+    return create_tri_precond(A, 3, 0.0, M, s);
+}
+
+LAB_API lab_status lab_precond_create_gauss_seidel(lab_csr A, lab_precond* M, lab_stream s)
+{
+    return create_tri_precond(A, 4, 0.0, M, s);
+}
+
+LAB_API lab_status lab_precond_create_sor(lab_csr A, double omega, lab_precond* M, lab_stream s)
+{
+    LAB_ARG(omega > 0.0 && omega < 2.0, "SOR needs 0 < omega < 2");
+    return create_tri_precond(A, 5, omega, M, s);
 }
 
 LAB_API lab_status lab_precond_apply(lab_precond M, const double* r, double* z, lab_stream s)

@@ -1,0 +1,22 @@
+// Triangular path (tri.cu): level-scheduled triangular solves and in-place
+// ILU(0) / IC(0), bit-identical to the reference's sequential loops.
+#pragma once
+
+#include "internal.cuh"
+
+namespace lab
+{
+    // Levels of the lower and upper dependency of A's pattern and the diagonal
+    // positions (host analysis, cached on A until it is released).
+    lab_status tri_analyse(lab_csr_impl* A, cudaStream_t s);
+
+    // x = T^-1 b on the lower (columns < i) or upper (columns > i) part of A.
+    // dscale != 0 scales the diagonal (SOR); skip: early-exit flag (graphs).
+    lab_status tri_solve(lab_csr_impl* A, bool lower, bool unit, double dscale, const double* b,
+                         double* x, cudaStream_t s, const int* skip);
+
+    // In-place ILU(0) (ic = false) or IC(0); the smallest column of a missing /
+    // zero pivot goes to *structural_zero / *numeric_zero (-1: none).
+    lab_status tri_factor(lab_csr_impl* A, bool ic, int* structural_zero, int* numeric_zero,
+                          cudaStream_t s);
+}

@@ -4,6 +4,7 @@
 #include "oracle.h"
 
 #include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1168,4 +1169,222 @@ int orc_amg_solve(orc_hier* h, const double* b, double* x, int n1, int n2, int s
     }
     free(r);
     return cycle;
+}
+
+/* ======================================================================
+ * Triangular path
+ * ==================================================================== */
+
+/* get_diagonal_value_local (host_csrilu0.cpp:35-54, host_csric0.cpp:35-54): the
+ * pivot of column `col`, 1.0 for a missing or zero one (recorded). */
+static double tri_pivot(int col, int diag_index, const double* v, int* sz, int* nz)
+{
+    if(diag_index == -1)
+    {
+        if(sz && col < *sz)
+            *sz = col;
+        return 1.0;
+    }
+    double d = v[diag_index];
+    if(d == 0.0)
+    {
+        if(nz && col < *nz)
+            *nz = col;
+        return 1.0;
+    }
+    return d;
+}
+
+/* host_csrilu0_impl (host_csrilu0.cpp:57-102): row by row, every lower entry
+ * (CSR order, up to the diagonal) is divided by its column's pivot and then
+ * eliminates the matching entries of the row with the pivot row's part right of
+ * its diagonal (k from diag_index + 1, as the reference writes it). */
+void orc_csrilu0(orc_csr* A, int* structural_zero, int* numeric_zero)
+{
+    const int m = A->m;
+    int*      dp  = (int*)malloc(sizeof(int) * (m > 0 ? m : 1));
+    int*      map = (int*)malloc(sizeof(int) * (A->n > 0 ? A->n : 1));
+    if(structural_zero)
+        *structural_zero = INT_MAX;
+    if(numeric_zero)
+        *numeric_zero = INT_MAX;
+    for(int i = 0; i < m; i++)
+        dp[i] = -1;
+    for(int c = 0; c < A->n; c++)
+        map[c] = -1;
+    double* v = A->v;
+    for(int row = 0; row < m; row++)
+    {
+        const int a = A->rp[row], b = A->rp[row + 1];
+        for(int j = a; j < b; j++)
+            map[A->ci[j]] = j;
+        for(int j = a; j < b; j++)
+        {
+            const int cj = A->ci[j];
+            if(cj < row)
+            {
+                const int    di  = dp[cj];
+                const double piv = tri_pivot(cj, di, v, structural_zero, numeric_zero);
+                const int    end = A->rp[cj + 1];
+                v[j]             = v[j] / piv;
+                for(int k = di + 1; k < end; k++)
+                {
+                    const int t = map[A->ci[k]];
+                    if(t != -1)
+                        v[t] = v[t] - v[j] * v[k];
+                }
+            }
+            else if(cj == row)
+            {
+                dp[row] = j;
+                break;
+            }
+            else
+                break;
+        }
+        for(int j = a; j < b; j++)
+            map[A->ci[j]] = -1;
+    }
+    free(map);
+    free(dp);
+}
+
+/* host_csric0_impl (host_csric0.cpp:57-110): lower entries in CSR order become
+ * (a_ij - sum_k l_ik l_jk) / l_jj (fma-accumulated over the pivot row's part left
+ * of its diagonal), the diagonal sqrt(|a_ii - sum_j l_ij^2|); the upper part is
+ * left as it was. */
+void orc_csric0(orc_csr* A, int* structural_zero, int* numeric_zero)
+{
+    const int m = A->m;
+    int*      dp  = (int*)malloc(sizeof(int) * (m > 0 ? m : 1));
+    int*      map = (int*)malloc(sizeof(int) * (A->n > 0 ? A->n : 1));
+    if(structural_zero)
+        *structural_zero = INT_MAX;
+    if(numeric_zero)
+        *numeric_zero = INT_MAX;
+    for(int i = 0; i < m; i++)
+        dp[i] = -1;
+    for(int c = 0; c < A->n; c++)
+        map[c] = -1;
+    double* v = A->v;
+    for(int row = 0; row < m; row++)
+    {
+        const int a = A->rp[row], b = A->rp[row + 1];
+        for(int j = a; j < b; j++)
+            map[A->ci[j]] = j;
+        double sum = 0.0;
+        for(int j = a; j < b; j++)
+        {
+            const int cj = A->ci[j];
+            if(cj < row)
+            {
+                const int di = dp[cj];
+                double    s  = 0.0;
+                for(int k = A->rp[cj]; k < di; k++)
+                {
+                    const int t = map[A->ci[k]];
+                    if(t != -1)
+                        s = fma(v[t], v[k], s);
+                }
+                const double piv = tri_pivot(cj, di, v, structural_zero, numeric_zero);
+                const double val = (v[j] - s) / piv;
+                sum              = fma(val, val, sum);
+                v[j]             = val;
+            }
+            else if(cj == row)
+            {
+                dp[row] = j;
+                v[j]    = sqrt(fabs(v[j] - sum));
+                break;
+            }
+            else
+                break;
+        }
+        for(int j = a; j < b; j++)
+            map[A->ci[j]] = -1;
+    }
+    free(map);
+    free(dp);
+}
+
+/* host_forward_solve_impl / host_backward_solve_impl (host_csrtrsv.cpp:36-90):
+ * forward: fma over the entries left of the diagonal in CSR order, then
+ * (b - sum) / d; backward: x = b, subtract a_ij x_j walking the row right to
+ * left, then divide by the diagonal. unit_diag: d = 1. */
+void orc_trsv(const orc_csr* A, int lower, int unit_diag, const double* b, double* x)
+{
+    const int n = A->m;
+    if(lower)
+    {
+        for(int i = 0; i < n; i++)
+        {
+            double d = 1.0, sum = 0.0;
+            for(int j = A->rp[i]; j < A->rp[i + 1]; j++)
+            {
+                const int c = A->ci[j];
+                if(c < i)
+                    sum = fma(A->v[j], x[c], sum);
+                else if(!unit_diag && c == i)
+                    d = A->v[j];
+                else
+                    break;
+            }
+            x[i] = (b[i] - sum) / d;
+        }
+    }
+    else
+    {
+        for(int i = n - 1; i >= 0; i--)
+        {
+            double d  = 1.0;
+            double xi = b[i];
+            for(int j = A->rp[i + 1] - 1; j >= A->rp[i]; j--)
+            {
+                const int c = A->ci[j];
+                if(c > i)
+                    xi = xi - A->v[j] * x[c];
+                else if(!unit_diag && c == i)
+                    d = A->v[j];
+            }
+            x[i] = xi / d;
+        }
+    }
+}
+
+/* preconditioner.cpp: ilu_precond (432-468), ic_precond (506-543): factor a copy,
+ * lower solve (unit / non-unit), upper solve of the same matrix (non-unit; for
+ * IC(0) its upper part is A's, unchanged by the factorization);
+ * gauss_seidel_precond (90-105): lower non-unit solve on A's lower part;
+ * SOR_precond (137-156): the same with the diagonal scaled by 1 / omega. */
+void orc_precond_apply(int kind, double omega, const orc_csr* A, const double* rhs, double* x)
+{
+    const int nnz = A->rp[A->m];
+    orc_csr   F   = *A;
+    F.v         = (double*)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+    memcpy(F.v, A->v, sizeof(double) * nnz);
+    if(kind == 0 || kind == 1)
+    {
+        int sz, nz;
+        if(kind == 0)
+            orc_csrilu0(&F, &sz, &nz);
+        else
+            orc_csric0(&F, &sz, &nz);
+        double* y = (double*)malloc(sizeof(double) * (A->m > 0 ? A->m : 1));
+        orc_trsv(&F, 1, kind == 0, rhs, y);
+        orc_trsv(&F, 0, 0, y, x);
+        free(y);
+    }
+    else
+    {
+        if(kind == 3)
+        {
+            const double s = 1.0 / omega;
+            for(int i = 0; i < F.m; i++)
+                for(int j = F.rp[i]; j < F.rp[i + 1]; j++)
+                    if(F.ci[j] == i)
+                        F.v[j] = F.v[j] * s;
+        }
+        orc_trsv(&F, 1, 0, rhs, x);
+    }
+    free(F.v);
 }

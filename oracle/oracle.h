@@ -99,6 +99,16 @@ int  orc_cg(const orc_csr* A, const double* b, double* x, int jacobi, double rel
 int  orc_amg_solve(orc_hier* h, const double* b, double* x, int n1, int n2, int smoother,
                    double omega, int coarse, double rel_tol, double abs_tol, int max_cycle);
 
+/* triangular path: in-place ILU(0) / IC(0) (the factors overwrite A's values;
+ * *structural_zero / *numeric_zero get the smallest column of a missing / zero
+ * pivot, INT_MAX when none), triangular solves on the lower or upper part of A,
+ * and one application x = M^-1 rhs of the ILU(0), IC(0), Gauss-Seidel and SOR
+ * preconditioners (kind 0..3). */
+void orc_csrilu0(orc_csr* A, int* structural_zero, int* numeric_zero);
+void orc_csric0(orc_csr* A, int* structural_zero, int* numeric_zero);
+void orc_trsv(const orc_csr* A, int lower, int unit_diag, const double* b, double* x);
+void orc_precond_apply(int kind, double omega, const orc_csr* A, const double* rhs, double* x);
+
 #ifdef __cplusplus
 }
 #endif

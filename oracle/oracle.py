@@ -99,6 +99,10 @@ class Oracle:
         L.orc_amg_solve.argtypes = [C.POINTER(_Hier), _p, _p, _i, _i, _i, _d, _i, _d, _d, _i]
         L.orc_cg.argtypes = [P, _p, _p, _i, _d, _d, _i]
         L.orc_exclusive_scan_i64.argtypes = [_p, _i]
+        L.orc_csrilu0.argtypes = [P, _p, _p]
+        L.orc_csric0.argtypes = [P, _p, _p]
+        L.orc_trsv.argtypes = [P, _i, _i, _p, _p]
+        L.orc_precond_apply.argtypes = [_i, _d, P, _p, _p]
 
     # -- kernels
     def spmv(self, A, x, alpha=1.0, beta=0.0, y=None):
@@ -191,6 +195,35 @@ class Oracle:
     # -- hierarchy / solvers
     def amg_setup(self, A, kind=0, max_level=20):
         return OracleHierarchy(self, A, kind, max_level)
+
+    # -- triangular path
+    def _factor(self, fn, A):
+        s = _csr_in(A[0], A[1], np.array(A[2], dtype=np.float64))  # factored in place
+        sz, nz = _i(), _i()
+        fn(C.byref(s), C.byref(sz), C.byref(nz))
+        return s._keep[2].copy(), sz.value, nz.value
+
+    def csrilu0(self, A):
+        """(factored values, structural zero, numeric zero); INT_MAX = none."""
+        return self._factor(self.L.orc_csrilu0, A)
+
+    def csric0(self, A):
+        return self._factor(self.L.orc_csric0, A)
+
+    def trsv(self, A, b, lower=True, unit_diag=False):
+        s = _csr_in(*A[:3])
+        x = np.zeros(s.m)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.L.orc_trsv(C.byref(s), int(lower), int(unit_diag), _ptr(b), _ptr(x))
+        return x
+
+    def precond_apply(self, kind, A, rhs, omega=1.0):
+        """kind 0 ILU(0), 1 IC(0), 2 Gauss-Seidel, 3 SOR(omega)."""
+        s = _csr_in(*A[:3])
+        x = np.zeros(s.m)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        self.L.orc_precond_apply(kind, omega, C.byref(s), _ptr(rhs), _ptr(x))
+        return x
 
     def cg(self, A, b, x0=None, jacobi=False, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000):
         s = _csr_in(*A[:3])
@@ -289,6 +322,11 @@ class Reference:
         L.ref_classical_strength.argtypes = [_i, _i, _p, _p, _p, _d, _p]
         L.ref_cfpoints.argtypes = [_i, _i, _p, _p, _p, _p]
         L.ref_exclusive_scan_i64.argtypes = [_p, _i]
+        L.ref_csrilu0.argtypes = [_i, _i, _p, _p, _p, _p, _p]
+        L.ref_csric0.argtypes = [_i, _i, _p, _p, _p, _p, _p]
+        L.ref_trsv.argtypes = [_i, _i, _p, _p, _p, _i, _i, _p, _p]
+        L.ref_precond_apply.argtypes = [_i, _d, _i, _i, _p, _p, _p, _p, _p]
+        L.ref_precond_cg.argtypes = [_i, _d, _i, _i, _p, _p, _p, _p, _p, _d, _d, _i]
 
     @staticmethod
     def _arr(A):
@@ -381,6 +419,43 @@ class Reference:
         b = np.ascontiguousarray(b, dtype=np.float64)
         it = self.L.ref_cg(m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(b), _ptr(x), int(jacobi),
                            rel_tol, abs_tol, max_iter)
+        return x, it
+
+    # -- triangular path
+    def _factor(self, fn, A):
+        rp, ci, v, m, n, z = self._arr(A)
+        v = v.copy()
+        sz, nz = _i(2**31 - 1), _i(2**31 - 1)
+        fn(m, z, _ptr(rp), _ptr(ci), _ptr(v), C.byref(sz), C.byref(nz))
+        return v, sz.value, nz.value
+
+    def csrilu0(self, A):
+        return self._factor(self.L.ref_csrilu0, A)
+
+    def csric0(self, A):
+        return self._factor(self.L.ref_csric0, A)
+
+    def trsv(self, A, b, lower=True, unit_diag=False):
+        rp, ci, v, m, n, z = self._arr(A)
+        x = np.zeros(m)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        self.L.ref_trsv(m, z, _ptr(rp), _ptr(ci), _ptr(v), int(lower), int(unit_diag), _ptr(b),
+                        _ptr(x))
+        return x
+
+    def precond_apply(self, kind, A, rhs, omega=1.0):
+        rp, ci, v, m, n, z = self._arr(A)
+        x = np.zeros(m)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        self.L.ref_precond_apply(kind, omega, m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(rhs), _ptr(x))
+        return x
+
+    def precond_cg(self, kind, A, b, omega=1.0, rel_tol=1e-8, abs_tol=1e-300, max_iter=2000):
+        rp, ci, v, m, n, z = self._arr(A)
+        x = np.zeros(m)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        it = self.L.ref_precond_cg(kind, omega, m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(b),
+                                   _ptr(x), rel_tol, abs_tol, max_iter)
         return x, it
 
     # No gmres(): the reference's gmres_solver::build leaves its residual vectors

@@ -448,4 +448,104 @@ void ref_exclusive_scan_i64(int64_t* x, int n)
     exclusive_scan(v);
     std::memcpy(x, v.get_vec(), sizeof(int64_t) * n);
 }
+
+// In-place incomplete factorizations (linalg_math.h:95-109 -> host_csrilu0.cpp,
+// host_csric0.cpp); the factored values overwrite v.
+void ref_csrilu0(int m, int nnz, const int* rp, const int* ci, double* v, int* structural_zero,
+                 int* numeric_zero)
+{
+    quiet_scope        q;
+    csr_matrix<double> A;
+    to_csr(A, m, m, nnz, rp, ci, v);
+    csrilu0(A, structural_zero, numeric_zero);
+    std::memcpy(v, A.get_val(), sizeof(double) * nnz);
+}
+
+void ref_csric0(int m, int nnz, const int* rp, const int* ci, double* v, int* structural_zero,
+                int* numeric_zero)
+{
+    quiet_scope        q;
+    csr_matrix<double> A;
+    to_csr(A, m, m, nnz, rp, ci, v);
+    csric0(A, structural_zero, numeric_zero);
+    std::memcpy(v, A.get_val(), sizeof(double) * nnz);
+}
+
+// Triangular solve on the lower or upper part of A (csrtrsv_analysis/_solve,
+// linalg_math.h:229-254 -> host_csrtrsv.cpp).
+void ref_trsv(int m, int nnz, const int* rp, const int* ci, const double* v, int lower,
+              int unit_diag, const double* b, double* x)
+{
+    quiet_scope        q;
+    csr_matrix<double> A;
+    to_csr(A, m, m, nnz, rp, ci, v);
+    vector<double> vb(std::vector<double>(b, b + m));
+    vector<double> vx(m);
+    csrtrsv_descr* d = nullptr;
+    create_csrtrsv_descr(&d);
+    const triangular_type t = lower ? triangular_type::lower : triangular_type::upper;
+    const diagonal_type   g = unit_diag ? diagonal_type::unit : diagonal_type::non_unit;
+    csrtrsv_analysis(A, t, g, d);
+    csrtrsv_solve(A, vb, vx, 1.0, t, g, d);
+    destroy_csrtrsv_descr(d);
+    std::memcpy(x, vx.get_vec(), sizeof(double) * m);
+}
+
+// One application x = M^-1 rhs of the reference's triangular-solve
+// preconditioners (preconditioner.cpp): kind 0 ILU(0), 1 IC(0), 2 Gauss-Seidel,
+// 3 SOR(omega).
+void ref_precond_apply(int kind, double omega, int m, int nnz, const int* rp, const int* ci,
+                       const double* v, const double* rhs, double* x)
+{
+    quiet_scope        q;
+    csr_matrix<double> A;
+    to_csr(A, m, m, nnz, rp, ci, v);
+    preconditioner* P = nullptr;
+    if(kind == 0)
+        P = new ilu_precond();
+    else if(kind == 1)
+        P = new ic_precond();
+    else if(kind == 2)
+        P = new gauss_seidel_precond();
+    else
+        P = new SOR_precond(omega);
+    P->build(A);
+    vector<double> vr(std::vector<double>(rhs, rhs + m));
+    vector<double> vx(m);
+    P->solve(vr, vx);
+    std::memcpy(x, vx.get_vec(), sizeof(double) * m);
+    delete P;
+}
+
+// CG with one of the preconditioners above; returns the iteration count.
+int ref_precond_cg(int kind, double omega, int m, int nnz, const int* rp, const int* ci,
+                   const double* v, const double* b, double* x, double rel_tol, double abs_tol,
+                   int max_iter)
+{
+    quiet_scope        q;
+    csr_matrix<double> A;
+    to_csr(A, m, m, nnz, rp, ci, v);
+    preconditioner* P = nullptr;
+    if(kind == 0)
+        P = new ilu_precond();
+    else if(kind == 1)
+        P = new ic_precond();
+    else if(kind == 2)
+        P = new gauss_seidel_precond();
+    else
+        P = new SOR_precond(omega);
+    P->build(A);
+    vector<double> vb(std::vector<double>(b, b + m));
+    vector<double> vx(std::vector<double>(x, x + m));
+    iter_control   c;
+    c.rel_tol  = rel_tol;
+    c.abs_tol  = abs_tol;
+    c.max_iter = max_iter;
+    cg_solver cg;
+    cg.build(A);
+    int it = cg.solve(A, vx, vb, P, c);
+    std::memcpy(x, vx.get_vec(), sizeof(double) * m);
+    delete P;
+    return it;
+}
 }

@@ -1,6 +1,6 @@
-"""The C++ API as a reference user would call it: tests/cxx/pcg_amg_example.cpp
-is compiled against include/ with g++ and linked with liblinalg_b200.so, then
-run on the GPU and checked against the oracle."""
+"""The C++ API as a reference user would call it: the programs in tests/cxx/ are
+compiled against include/ with g++ and linked with liblinalg_b200.so, then run
+on the GPU and checked against the oracle."""
 import os
 import subprocess
 
@@ -12,17 +12,20 @@ from linalglib_b200 import problems as P
 pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-SRC = os.path.join(ROOT, "tests", "cxx", "pcg_amg_example.cpp")
 LIBDIR = os.path.join(ROOT, "linalglib_b200")
+
+
+def _compile(tmp_path_factory, name):
+    exe = str(tmp_path_factory.mktemp("cxx") / name)
+    subprocess.run(["/usr/bin/g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cxx", name + ".cpp"), "-o", exe, "-L", LIBDIR,
+                    "-llinalg_b200", f"-Wl,-rpath,{LIBDIR}"], check=True)
+    return exe
 
 
 @pytest.fixture(scope="module")
 def example(tmp_path_factory):
-    exe = str(tmp_path_factory.mktemp("cxx") / "pcg_amg_example")
-    subprocess.run(["/usr/bin/g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
-                    SRC, "-o", exe, "-L", LIBDIR, "-llinalg_b200", f"-Wl,-rpath,{LIBDIR}"],
-                   check=True)
-    return exe
+    return _compile(tmp_path_factory, "pcg_amg_example")
 
 
 def test_cxx_example_matches_oracle(gpu, oracle, example):
@@ -40,3 +43,27 @@ def test_cxx_example_matches_oracle(gpu, oracle, example):
     _, cyc_o = h.amg_solve(b, rel_tol=1e-8, abs_tol=0.0, max_cycle=300, coarse=1)
     assert abs(int(cycles) - cyc_o) <= 1
     assert int(conv) == 1 and float(rel) <= 1e-8
+
+
+def test_cxx_triangular_preconditioners(gpu, oracle, reference, tmp_path_factory):
+    exe = _compile(tmp_path_factory, "tri_precond_example")
+    n = 24
+    out = subprocess.run([exe, str(n)], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    lines = out.stdout.split("\n")
+    iters, conv, gs_cycles, sor_cycles, rel, sz, nz = lines[0].split()
+    A = P.poisson2d(n)
+    m, nnz = n * n, A[2].size
+    vals = np.array([float.fromhex(t) for t in lines[1:1 + nnz]])
+    y = np.array([float.fromhex(t) for t in lines[1 + nnz:1 + nnz + m]])
+    vo, so, no = oracle.csrilu0(A)
+    assert np.array_equal(vals.view(np.int64), vo.view(np.int64))
+    assert (int(sz), int(nz)) == (-1, -1) and (so, no) == (np.iinfo(np.int32).max,) * 2
+    y_o = oracle.trsv((A[0], A[1], vo), np.ones(m), True, True)
+    assert np.array_equal(y.view(np.int64), y_o.view(np.int64))
+    b = P.csr_matvec(*A[:3], np.ones(m))
+    _, itr = reference.precond_cg(0, A, b, rel_tol=1e-8, abs_tol=1e-300, max_iter=1000)
+    assert int(conv) == 1 and abs(int(iters) - itr) <= 1, (iters, itr)
+    # GMRES stops on the preconditioned 2-norm residual (1e-10 relative); the
+    # printed figure is the true inf-norm residual
+    assert float(rel) <= 1e-8

@@ -1,0 +1,131 @@
+"""Level-scheduled triangular path on the GPU: lab_csrtrsv, lab_csrilu0 /
+lab_csric0 and the ILU(0) / IC(0) / Gauss-Seidel / SOR preconditioners are
+bit-identical to the oracle (which is pinned bit-exact to the reference's
+host_csrtrsv.cpp, host_csrilu0.cpp, host_csric0.cpp and preconditioner.cpp), and
+PCG with them behaves as the reference's cg_solver does."""
+import numpy as np
+import pytest
+
+from linalglib_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "poisson2d_20": lambda: P.poisson2d(20),
+    "laplacian3d_8": lambda: P.graph_laplacian3d(8, seed=1),
+    "diffusion27_6": lambda: P.diffusion27(6, seed=2),
+    "poisson3d_24": lambda: P.poisson3d(24),
+}
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float64).view(np.int64)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("lower", [True, False])
+@pytest.mark.parametrize("unit", [True, False])
+def test_trsv_bit_exact(gpu, oracle, name, lower, unit):
+    A = CASES[name]()
+    b = np.random.default_rng(3).uniform(-1, 1, A[0].size - 1)
+    x = gpu.CsrMatrix.from_arrays(*A[:3]).trsv(gpu.vec(b), lower=lower, unit_diag=unit)
+    assert np.array_equal(_bits(x.cpu().numpy()), _bits(oracle.trsv(A, b, lower, unit)))
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("kind", ["ilu0", "ic0"])
+def test_factor_bit_exact(gpu, oracle, name, kind):
+    A = CASES[name]()
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    sz, nz = dA.factor(kind)
+    vo, so, no = getattr(oracle, "csr" + kind)(A)
+    big = np.iinfo(np.int32).max
+    assert (sz, nz) == (-1 if so == big else so, -1 if no == big else no)
+    assert np.array_equal(_bits(dA.to_numpy()[2]), _bits(vo))
+
+
+def test_factor_zero_pivots(gpu, oracle):
+    # numeric zero on row 3's diagonal, structural zero (no diagonal) in row 5:
+    # the level-parallel and sequential paths must both report the smallest column
+    rp, ci, v = P.poisson2d(4)
+    v = v.copy()
+    for j in range(rp[3], rp[4]):
+        if ci[j] == 3:
+            v[j] = 0.0
+    keep = np.ones(v.size, dtype=bool)
+    for j in range(rp[5], rp[6]):
+        if ci[j] == 5:
+            keep[j] = False
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))[keep]
+    A = (np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=rp.size - 1))]).astype(np.int32),
+         ci[keep].copy(), v[keep].copy())
+    for kind in ("ilu0", "ic0"):
+        dA = gpu.CsrMatrix.from_arrays(*A)
+        sz, nz = dA.factor(kind)
+        vo, so, no = getattr(oracle, "csr" + kind)(A)
+        big = np.iinfo(np.int32).max
+        assert (sz, nz) == (-1 if so == big else so, -1 if no == big else no), kind
+        assert np.array_equal(_bits(dA.to_numpy()[2]), _bits(vo)), kind
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+def test_precond_apply_bit_exact(gpu, oracle, name, kind):
+    A = CASES[name]()
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    M = [gpu.Preconditioner.ilu0, gpu.Preconditioner.ic0, gpu.Preconditioner.gauss_seidel,
+         lambda X: gpu.Preconditioner.sor(X, 1.3)][kind](dA)
+    r = np.random.default_rng(4).uniform(-1, 1, A[0].size - 1)
+    z = M.apply(gpu.vec(r)).cpu().numpy()
+    assert np.array_equal(_bits(z), _bits(oracle.precond_apply(kind, A, r, omega=1.3)))
+    # the preconditioner works on a copy: A itself is unchanged
+    assert np.array_equal(_bits(dA.to_numpy()[2]), _bits(A[2]))
+
+
+def test_ilu_pcg_matches_reference(gpu, reference):
+    A = P.poisson2d(24)
+    b, xt = P.rhs_from_solution(*A[:3], seed=0)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    x, info = gpu.pcg(dA, gpu.vec(b), M=gpu.Preconditioner.ilu0(dA),
+                      control=gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=1000))
+    xr, itr = reference.precond_cg(0, A, b, rel_tol=1e-8, abs_tol=1e-300)
+    assert itr == 24  # the reference's count on this problem
+    assert info.converged == 1
+    assert abs(info.iterations - itr) <= 1, (info.iterations, itr)
+    assert np.max(np.abs(x.cpu().numpy() - xr)) <= 1e-7 * np.max(np.abs(xr))
+    assert np.max(np.abs(x.cpu().numpy() - xt)) <= 1e-6
+
+
+@pytest.mark.parametrize("kind", [1, 2, 3])
+def test_nonsymmetric_precond_pcg_like_reference(gpu, reference, kind):
+    # The reference's IC(0) factor overwrites only the lower triangle and its
+    # upper solve reads the unfactored upper part (host_csric0.cpp:70-115,
+    # preconditioner.cpp:512-525); Gauss-Seidel and SOR are one-sided.  None is
+    # symmetric, so the reference's CG stagnates with them: the device path must
+    # do the same (not converged, the same iterate after 50 iterations).
+    A = P.poisson2d(24)
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    M = [None, gpu.Preconditioner.ic0, gpu.Preconditioner.gauss_seidel,
+         lambda X: gpu.Preconditioner.sor(X, 1.3)][kind](dA)
+    x, info = gpu.pcg(dA, gpu.vec(b), M=M,
+                      control=gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=50))
+    xr, itr = reference.precond_cg(kind, A, b, omega=1.3, rel_tol=1e-8, abs_tol=1e-300,
+                                   max_iter=50)
+    assert itr == 51 and info.converged == 0
+    assert np.max(np.abs(x.cpu().numpy() - xr)) <= 1e-6 * np.max(np.abs(xr))
+
+
+@pytest.mark.parametrize("name", ["poisson3d_24", "diffusion27_6"])
+def test_nonsymmetric_preconds_under_gmres(gpu, name):
+    # Gauss-Seidel and SOR are one-sided: they work under GMRES (the reference's
+    # IC(0), whose upper solve reads the unfactored upper part, does not converge
+    # under GMRES either: its application is checked bit for bit above)
+    A = CASES[name]()
+    b, xt = P.rhs_from_solution(*A[:3], seed=1)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    for M in (gpu.Preconditioner.gauss_seidel(dA), gpu.Preconditioner.sor(dA, 1.2)):
+        x, info = gpu.gmres(dA, gpu.vec(b), M=M, restart=30,
+                            control=gpu.iter_control(rel_tol=1e-10, abs_tol=0.0, max_iter=2000))
+        assert info.converged == 1
+        assert np.max(np.abs(x.cpu().numpy() - xt)) <= 1e-6 * np.max(np.abs(xt))
