@@ -61,13 +61,14 @@ def parse():
                          "27-point diffusion operator")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="full",
-                    choices=["full", "profile", "spmv", "mixed", "batched", "adjoint"],
+                    choices=["full", "profile", "spmv", "mixed", "batched", "adjoint", "tri"],
                     help="profile: only the warm-up and timed device-resident steps (the "
                          "command the ncu launch lists in profiles/ are taken from); "
                          "spmv: only the standalone level-0 SpMV timing (5 warm-up launches, "
                          "then 3 x 20 timed back-to-back launches); mixed / batched / "
-                         "adjoint: the mixed-precision, batched and adjoint workloads "
-                         "(one JSON line each, not the driver's bench line)")
+                         "adjoint / tri: the mixed-precision, batched, adjoint and "
+                         "ILU(0)-PCG workloads (one JSON line each, not the driver's "
+                         "bench line)")
     return ap.parse_args()
 
 
@@ -678,6 +679,117 @@ def run_adjoint(args, d):
     return 0
 
 
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def tri_bytes(rp, ci, lower):
+    """Algorithmic bytes of one triangular solve: the triangle's entries (value and
+    column, diagonal included), row pointers, b read and x written once."""
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+    nnz_t = int(np.count_nonzero(ci <= rows) if lower else np.count_nonzero(ci >= rows))
+    m = rp.size - 1
+    return 12 * nnz_t + 4 * (m + 1) + 16 * m, nnz_t
+
+
+def run_tri(args, d):
+    """ILU(0)-preconditioned CG on the 3D 7-point Poisson n^3 system (the reference's
+    ilu_precond with cg_solver).  A step is the preconditioner build (copy of A,
+    level analysis, in-place ILU(0)) plus the PCG solve to rtol, device-resident.
+    Also times one preconditioner application (unit-lower then upper solve of the
+    factor) and each triangular solve alone (CUDA events), and the oracle's CPU
+    ILU(0)-PCG (the C restatement, one core) on the same system."""
+    import torch
+    d.init(need_gpu=True)
+    import linalglib_b200.core as core
+    core.init()
+    n = args.n or 128
+    A, b, xt = problem(n)
+    m, nnz = A[0].size - 1, A[2].size
+    dA = core.CsrMatrix.from_arrays(*A)
+    dA.analyse()
+    bd = core.vec(b)
+    ctl = core.iter_control(rel_tol=args.rtol, abs_tol=0.0, max_iter=5000)
+    x = torch.zeros(m, dtype=torch.float64, device="cuda")
+    st = {}
+
+    def step():
+        M = core.Preconditioner.ilu0(dA)
+        x.zero_()
+        _, st["info"] = core.pcg(dA, bd, x=x, M=M, control=ctl)
+        del M
+
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    clocks.begin()
+    l0 = core.launch_count()
+    t_step, all_steps = _events_ms(torch, step, args.steps)
+    launches = (core.launch_count() - l0) / args.steps
+    clk = clocks.stop()
+    info = st["info"]
+    err = float(torch.max(torch.abs(x - core.vec(xt))))
+
+    M = core.Preconditioner.ilu0(dA)
+    r = core.vec(np.random.default_rng(3).uniform(-1, 1, m))
+    z = torch.empty_like(r)
+    for _ in range(3):
+        M.apply(r, z)
+    t_apply, _ = _events_ms(torch, lambda: M.apply(r, z), 20)
+    t_build, _ = _events_ms(torch, lambda: core.Preconditioner.ilu0(dA), 5)
+    # the build's parts on a fresh copy of A: level analysis (first solve minus a
+    # solve), then the in-place factorization alone
+    X = core.CsrMatrix.from_arrays(*A)
+    t_first, _ = _events_ms(torch, lambda: X.trsv(r, lower=True, unit_diag=True, x=z), 1)
+    t_fact, _ = _events_ms(torch, lambda: X.factor("ilu0"), 1)
+    del X
+    t_lo, _ = _events_ms(torch, lambda: dA.trsv(r, lower=True, unit_diag=False, x=z), 20)
+    t_up, _ = _events_ms(torch, lambda: dA.trsv(r, lower=False, unit_diag=False, x=z), 20)
+    b_lo, nnz_lo = tri_bytes(A[0], A[1], True)
+    b_up, nnz_up = tri_bytes(A[0], A[1], False)
+    peak, which = _hbm_peak()
+    levels = 3 * (n - 1) + 1  # dependency levels of either triangle of the 7-point stencil
+
+    cpu = None
+    if d.rank == 0 and not args.no_cpu_baseline:
+        from oracle.oracle import Oracle
+        t0 = time.perf_counter()
+        _, it_cpu = Oracle().precond_cg(0, A, b, rel_tol=args.rtol, abs_tol=0.0, max_iter=5000)
+        t_cpu = time.perf_counter() - t0
+        cpu = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": f"one full ILU(0)-PCG solve of the {n}^3 system ({it_cpu} iterations, "
+                         f"{t_cpu:.1f} s; the reference's own host ILU(0) allocates an n-sized "
+                         "column map per row, O(m^2) at this size)"}
+    line = {
+        "mode": "tri", "metric": "ILU(0)-PCG time-to-rtol", "value": 1e3 / t_step,
+        "unit": "solves/s", "ms_per_step": t_step, "steps_ms": all_steps, "dtype": "f64",
+        "config": {"workload": f"ILU(0)-PCG, 3D 7-point Poisson {n}^3, rtol {args.rtol:g}",
+                   "rows": int(m), "nnz": int(nnz), "levels_per_triangle": levels,
+                   "l2": "inputs larger than L2"},
+        "iterations": info.iterations, "converged": bool(info.converged),
+        "max_abs_err_vs_x_true": err, "build_ms": t_build, "apply_ms": t_apply,
+        "build_parts_ms": {"level_analysis": t_first - t_lo, "factorization": t_fact},
+        "trsv": {"lower_us": 1e3 * t_lo, "upper_us": 1e3 * t_up,
+                 "lower_bytes": b_lo, "upper_bytes": b_up,
+                 "lower_GBs": b_lo / (t_lo * 1e-3) / 1e9, "upper_GBs": b_up / (t_up * 1e-3) / 1e9,
+                 "frac_lower": b_lo / (t_lo * 1e-3) / 1e9 / peak,
+                 "frac_upper": b_up / (t_up * 1e-3) / 1e9 / peak,
+                 "peak": peak, "peak_source": which,
+                 "us_per_level": 1e3 * (t_lo + t_up) / (2 * levels)},
+        "gpu_launches_per_step": launches, "clocks": clk, "cpu_baseline": cpu,
+    }
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+    d.close()
+    return 0
+
+
 def main():
     args = parse()
     d = Dist()
@@ -690,6 +802,8 @@ def main():
         return run_batched(args, d)
     if args.mode == "adjoint":
         return run_adjoint(args, d)
+    if args.mode == "tri":
+        return run_tri(args, d)
     args.n = args.n or 128
     return run_ours(args, d)
 

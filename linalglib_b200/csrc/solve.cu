@@ -1524,6 +1524,14 @@ LAB_API lab_status lab_precond_create_jacobi(lab_csr A, lab_precond* out, lab_st
     return LAB_OK;
 }
 
+// A triangular preconditioner's solves give up only if a row's dependencies never
+// arrive (a bug, not an input property): report it over the solver's status.
+static lab_status tri_status(lab_precond_s* M, lab_status st, cudaStream_t s)
+{
+    const lab_status e = tri_check(M->F, s);
+    return e != LAB_OK ? e : st;
+}
+
 // ILU(0) / IC(0): factor a copy of A (ilu_precond::build, preconditioner.cpp:432-450;
 // ic_precond::build, 506-524).  Gauss-Seidel / SOR: solve with the lower part of
 // a copy of A (gauss_seidel_precond::build 90-96, SOR_precond::build 137-147).
@@ -1613,7 +1621,8 @@ LAB_API lab_status lab_pcg_solve(lab_csr A, lab_precond M, const double* b, doub
         return cg_plain(A, b, x, c, info, to_stream(s));
     if(M->kind == 0 && M->o.precision != LAB_PREC_FP64)
         return pcg_refine(A, M, b, x, c, info, to_stream(s));
-    return pcg_solve(A, M, b, x, c, info, to_stream(s));
+    lab_status st = pcg_solve(A, M, b, x, c, info, to_stream(s));
+    return M->kind >= 2 && st != LAB_BAD_ARG ? tri_status(M, st, to_stream(s)) : st;
 }
 
 LAB_API lab_status lab_pcg_solve_host(lab_csr A, lab_precond M, const double* bh, double* xh,
@@ -1631,6 +1640,8 @@ LAB_API lab_status lab_pcg_solve_host(lab_csr A, lab_precond M, const double* bh
                        : (M->kind == 0 && M->o.precision != LAB_PREC_FP64)
                              ? pcg_refine(A, M, b.get(), x.get(), c, info, s)
                              : pcg_solve(A, M, b.get(), x.get(), c, info, s);
+    if(M && M->kind >= 2 && st != LAB_BAD_ARG)
+        st = tri_status(M, st, s);
     if(st != LAB_OK && st != LAB_NOT_CONVERGED && st != LAB_NAN)
         return st;
     LAB_CUDA(cudaMemcpyAsync(xh, x.get(), sizeof(double) * A->m, cudaMemcpyDeviceToHost, s));
@@ -1646,7 +1657,8 @@ LAB_API lab_status lab_gmres_solve(lab_csr A, lab_precond M, int restart, const 
     LAB_ARG(A->m == A->n, "GMRES needs a square matrix");
     LAB_ARG(restart >= 1, "restart must be >= 1");
     LAB_TRY(ensure_init());
-    return gmres_solve(A, M, restart, b, x, c, info, to_stream(s));
+    lab_status st = gmres_solve(A, M, restart, b, x, c, info, to_stream(s));
+    return M && M->kind >= 2 && st != LAB_BAD_ARG ? tri_status(M, st, to_stream(s)) : st;
 }
 
 __global__ void k_block_copy(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,

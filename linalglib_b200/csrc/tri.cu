@@ -1,13 +1,18 @@
-// Triangular path: level-scheduled sparse triangular solves, in-place ILU(0) and
-// IC(0), behind the reference's csrtrsv / csrilu0 / csric0 and its ILU(0),
-// IC(0), Gauss-Seidel and SOR preconditioners.
+// Triangular path: sparse triangular solves, in-place ILU(0) and IC(0), behind
+// the reference's csrtrsv / csrilu0 / csric0 and its ILU(0), IC(0), Gauss-Seidel
+// and SOR preconditioners.
 //
 // Rows are grouped into dependency levels once per matrix pattern (on the host:
-// a row's level is one more than the deepest row it reads); a level's rows are
-// independent, so each level is one launch with a thread per row.  Every row is
-// computed by one thread in exactly the reference's operation order
-// (host_csrtrsv.cpp, host_csrilu0.cpp, host_csric0.cpp), so the results are
-// bit-identical to the reference's sequential loops.
+// a row's level is one more than the deepest row it reads).  A solve is one
+// launch (after one that marks x pending): warps claim 32-row chunks in level
+// order from an atomic counter, and each lane walks its row in the reference's
+// order, reading a dependency once its value is no longer marked pending.  A
+// chunk only waits on rows claimed before it, by warps that are running, so
+// every wait ends; the waits are still bounded (an error flag is set and the
+// kernel returns).  The factorizations run one launch per level.
+// Every row is computed by one thread in exactly the reference's operation
+// order (host_csrtrsv.cpp, host_csrilu0.cpp, host_csric0.cpp), so the results
+// are bit-identical to the reference's sequential loops.
 #include "internal.cuh"
 #include "tri.cuh"
 
@@ -27,6 +32,8 @@ namespace lab
     {
         tri_sched lower, upper;
         int32_t*  diag     = nullptr; // device: position of a_ii in row i, -1 if absent
+        int32_t*  ctl      = nullptr; // device: claim counter, error flag of the solves
+        double*   scratch  = nullptr; // device: copy of b for in-place solves
         bool      all_diag = true;
     };
 
@@ -40,6 +47,10 @@ namespace lab
             cudaFree(A->tri->upper.rows);
         if(A->tri->diag)
             cudaFree(A->tri->diag);
+        if(A->tri->ctl)
+            cudaFree(A->tri->ctl);
+        if(A->tri->scratch)
+            cudaFree(A->tri->scratch);
         delete A->tri;
         A->tri = nullptr;
     }
@@ -113,6 +124,10 @@ namespace lab
         level_sched(rp, ci, m, false, order, p->upper.ptr);
         up(&p->upper.rows, order);
         up(&p->diag, dpos);
+        if(st == LAB_OK)
+            st = dalloc(&p->ctl, 2, s);
+        if(st == LAB_OK && cudaMemsetAsync(p->ctl, 0, sizeof(int32_t) * 2, s) != cudaSuccess)
+            st = LAB_CUDA_ERROR;
         if(st == LAB_OK && cudaStreamSynchronize(s) != cudaSuccess) // host vectors go out of scope
             st = LAB_CUDA_ERROR;
         A->tri = p;
@@ -122,59 +137,185 @@ namespace lab
     }
 
     // ------------------------------------------------------------ solves
-    // host_forward_solve_impl (host_csrtrsv.cpp:36-64): fma over the entries left of
-    // the diagonal in CSR order, (b - sum) / d.  dscale != 0: d = a_ii * dscale (the
-    // diagonal of SOR_precond's M, preconditioner.cpp:137-147).
-    __global__ void k_trsv_lower(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                 const double* __restrict__ v, const int32_t* __restrict__ rows,
-                                 int n, int unit, double dscale, const double* __restrict__ b,
-                                 double* __restrict__ x, const int* skip)
+    // x is filled with kTriPending before a solve and every x_i is written once,
+    // by the row's lane, as the result of a double operation.  Such a result is
+    // never a signalling NaN (arithmetic returns a quiet NaN), so a value other
+    // than kTriPending is the solved x_i: the value is its own "solved" flag and
+    // a dependency costs one L2 round trip (relaxed 64-bit loads and stores at
+    // GPU scope, single-copy atomic).
+    constexpr uint64_t kTriPending = 0x7ff4d1b0c0de0001ull; // signalling NaN
+    constexpr int      kTriBlock   = 256;
+    constexpr int      kTriPf      = 8;        // entries of a row held in registers
+    constexpr unsigned kTriIdle    = 1u << 26; // idle rounds before a warp gives up
+
+    __device__ __forceinline__ uint64_t ld_relaxed(const double* p)
     {
-        if(skip && *skip)
-            return;
-        const int t = blockIdx.x * blockDim.x + threadIdx.x;
-        if(t >= n)
-            return;
-        const int i   = rows[t];
-        double    d   = 1.0;
-        double    sum = 0.0;
-        for(int j = rp[i]; j < rp[i + 1]; j++)
-        {
-            const int c = ci[j];
-            if(c < i)
-                sum = fma(v[j], x[c], sum);
-            else if(!unit && c == i)
-                d = dscale != 0.0 ? __dmul_rn(v[j], dscale) : v[j];
-            else
-                break;
-        }
-        x[i] = __ddiv_rn(__dsub_rn(b[i], sum), d);
+        uint64_t v;
+        asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+        return v;
+    }
+    __device__ __forceinline__ void st_relaxed(double* p, double v)
+    {
+        asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(__double_as_longlong(v))
+                     : "memory");
+    }
+    __device__ __forceinline__ int ld_acquire(const int32_t* p)
+    {
+        int v;
+        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        return v;
     }
 
-    // host_backward_solve_impl (host_csrtrsv.cpp:66-90): x = b, subtract a_ij x_j
-    // walking the row right to left (multiply, then subtract), divide by d.
-    __global__ void k_trsv_upper(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                 const double* __restrict__ v, const int32_t* __restrict__ rows,
-                                 int n, int unit, const double* __restrict__ b,
-                                 double* __restrict__ x, const int* skip)
+    __global__ void k_trsv_prep(double* x, int m, int32_t* counter, const int* skip)
     {
         if(skip && *skip)
             return;
-        const int t = blockIdx.x * blockDim.x + threadIdx.x;
-        if(t >= n)
-            return;
-        const int i  = rows[t];
-        double    d  = 1.0;
-        double    xi = b[i];
-        for(int j = rp[i + 1] - 1; j >= rp[i]; j--)
+        uint64_t* u = reinterpret_cast<uint64_t*>(x);
+        for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+            u[i] = kTriPending;
+        if(blockIdx.x == 0 && threadIdx.x == 0)
+            *counter = 0;
+    }
+
+    // One entry of a lane's row, in the reference's order, given the entry's
+    // dependency value xv (kTriPending: not solved yet -> false).  LOWER,
+    // host_forward_solve_impl (host_csrtrsv.cpp:36-64): fma over the entries left
+    // of the diagonal in CSR order, stop at the first entry right of it (or at the
+    // diagonal when unit); dscale != 0 scales the diagonal (SOR_precond's M,
+    // preconditioner.cpp:137-147).  Upper, host_backward_solve_impl (66-90): walk
+    // the row right to left subtracting a_ij x_j (multiply, then subtract), keep
+    // the diagonal.
+    template <bool LOWER>
+    __device__ __forceinline__ bool tri_entry(int c, double a, uint64_t xv, int i, int unit,
+                                              double dscale, int len, int& k, double& acc,
+                                              double& d)
+    {
+        if(LOWER ? c < i : c > i)
         {
-            const int c = ci[j];
-            if(c > i)
-                xi = __dsub_rn(xi, __dmul_rn(v[j], x[c]));
-            else if(!unit && c == i)
-                d = v[j];
+            if(xv == kTriPending)
+                return false;
+            const double xc = __longlong_as_double((long long)xv);
+            acc             = LOWER ? fma(a, xc, acc) : __dsub_rn(acc, __dmul_rn(a, xc));
+            k++;
         }
-        x[i] = __ddiv_rn(xi, d);
+        else if(c == i && !unit)
+        {
+            d = (LOWER && dscale != 0.0) ? __dmul_rn(a, dscale) : a;
+            k++;
+        }
+        else
+            k = LOWER ? len : k + 1; // the forward loop breaks here
+        return true;
+    }
+
+    // Warps claim 32-row chunks of `order` (rows by level) from ctl[0]; each lane
+    // polls the dependencies of its row's next entries at once, consumes the solved
+    // prefix in order, and writes x_i when the row is done.  ctl[1] is the error
+    // flag, set when a warp waited kTriIdle rounds without progress.
+    template <bool LOWER>
+    __global__ void __launch_bounds__(kTriBlock)
+        k_trsv(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+               const double* __restrict__ v, const int32_t* __restrict__ order, int m, int unit,
+               double dscale, const double* __restrict__ b, double* x, int32_t* ctl,
+               const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        const int lane = threadIdx.x & 31;
+        for(;;)
+        {
+            int base = 0;
+            if(lane == 0)
+                base = ld_acquire(ctl + 1) ? m : atomicAdd(ctl, 32);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if(base >= m)
+                return;
+            const int t    = base + lane;
+            bool      done = t >= m;
+            int       i = 0, a = 0, e = 0, len = 0, k = 0;
+            double    acc = 0.0, d = 1.0, bi = 0.0;
+            int       pc[kTriPf];
+            double    pv[kTriPf];
+            if(!done)
+            {
+                i   = order[t];
+                a   = rp[i];
+                e   = rp[i + 1];
+                len = e - a;
+#pragma unroll
+                for(int q = 0; q < kTriPf; q++)
+                {
+                    const int j = LOWER ? a + q : e - 1 - q;
+                    pc[q]       = q < len ? ci[j] : i;
+                    pv[q]       = q < len ? v[j] : 0.0;
+                }
+                if(LOWER)
+                    bi = b[i];
+                else
+                    acc = b[i];
+            }
+            unsigned idle = 0;
+            for(;;)
+            {
+                bool progress = false;
+                if(!done)
+                {
+                    const int k0 = k;
+                    // all outstanding dependencies of the held entries in flight at once
+                    uint64_t xv[kTriPf];
+#pragma unroll
+                    for(int q = 0; q < kTriPf; q++)
+                        xv[q] = (q >= k && q < len && (LOWER ? pc[q] < i : pc[q] > i))
+                                    ? ld_relaxed(x + pc[q])
+                                    : 0;
+                    bool blocked = false;
+#pragma unroll
+                    for(int q = 0; q < kTriPf; q++)
+                        if(!blocked && q == k && k < len)
+                            blocked = !tri_entry<LOWER>(pc[q], pv[q], xv[q], i, unit, dscale, len,
+                                                        k, acc, d);
+                    while(!blocked && k < len) // entries beyond the held ones
+                    {
+                        const int j  = LOWER ? a + k : e - 1 - k;
+                        const int c  = ci[j];
+                        uint64_t  xc = (LOWER ? c < i : c > i) ? ld_relaxed(x + c) : 0;
+                        blocked = !tri_entry<LOWER>(c, v[j], xc, i, unit, dscale, len, k, acc, d);
+                    }
+                    progress = k != k0;
+                    if(!blocked)
+                    {
+                        st_relaxed(x + i,
+                                   LOWER ? __ddiv_rn(__dsub_rn(bi, acc), d) : __ddiv_rn(acc, d));
+                        done     = true;
+                        progress = true;
+                    }
+                }
+                if(__all_sync(0xffffffffu, done))
+                    break;
+                if(__any_sync(0xffffffffu, progress))
+                    idle = 0;
+                else
+                {
+                    if(++idle >= kTriIdle)
+                    {
+                        if(lane == 0)
+                            atomicExch(ctl + 1, 1);
+                        return;
+                    }
+                    if((idle & 1023u) == 0 && __any_sync(0xffffffffu, ld_acquire(ctl + 1) != 0))
+                        return;
+                    __nanosleep(idle < 8 ? 0 : 64);
+                }
+            }
+        }
+    }
+
+    // One CTA (8 warps) per SM: 37,888 rows in flight on 148 SMs, more than the
+    // widest level of the 128^3 7-point solve; more warps only add polling traffic
+    // (measured: 740 us per 128^3 solve at 1 CTA per SM, 860 us at 3).
+    static int trsv_grid(int m)
+    {
+        return (int)std::max<int64_t>(1, std::min<int64_t>(num_sms(), ceil_div(m, kTriBlock)));
     }
 
     lab_status tri_solve(lab_csr_impl* A, bool lower, bool unit, double dscale, const double* b,
@@ -183,17 +324,39 @@ namespace lab
         if(A->m == 0)
             return LAB_OK;
         LAB_TRY(tri_analyse(A, s));
-        const tri_sched& sc = lower ? A->tri->lower : A->tri->upper;
-        for(size_t k = 0; k + 1 < sc.ptr.size(); k++)
+        tri_plan& p = *A->tri;
+        const int m = (int)A->m;
+        if(b < x + m && x < b + m) // in place: x is overwritten by the pending marks first
         {
-            const int      r0 = sc.ptr[k], n = sc.ptr[k + 1] - r0;
-            const unsigned g  = (unsigned)ceil_div(n, 128);
-            if(lower)
-                LAB_LAUNCH(k_trsv_lower, g, 128, 0, s, A->row_ptr, A->col_ind, (const double*)A->val,
-                           (const int32_t*)(sc.rows + r0), n, (int)unit, dscale, b, x, skip);
-            else
-                LAB_LAUNCH(k_trsv_upper, g, 128, 0, s, A->row_ptr, A->col_ind, (const double*)A->val,
-                           (const int32_t*)(sc.rows + r0), n, (int)unit, b, x, skip);
+            if(!p.scratch)
+                LAB_TRY(dalloc(&p.scratch, (size_t)m, s));
+            LAB_CUDA(cudaMemcpyAsync(p.scratch, b, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
+            b = p.scratch;
+        }
+        LAB_LAUNCH(k_trsv_prep, (unsigned)std::min<int64_t>(ceil_div(m, 256), 4 * num_sms()), 256,
+                   0, s, x, m, p.ctl, skip);
+        if(lower)
+            LAB_LAUNCH(k_trsv<true>, trsv_grid(m), kTriBlock, 0, s, A->row_ptr, A->col_ind,
+                       (const double*)A->val, (const int32_t*)p.lower.rows, m, (int)unit, dscale,
+                       b, x, p.ctl, skip);
+        else
+            LAB_LAUNCH(k_trsv<false>, trsv_grid(m), kTriBlock, 0, s, A->row_ptr,
+                       A->col_ind, (const double*)A->val, (const int32_t*)p.upper.rows, m,
+                       (int)unit, 0.0, b, x, p.ctl, skip);
+        return LAB_OK;
+    }
+
+    lab_status tri_check(lab_csr_impl* A, cudaStream_t s)
+    {
+        if(!A->tri || A->m == 0)
+            return LAB_OK;
+        int32_t e = 0;
+        LAB_TRY(copy_d2h_sync(&e, A->tri->ctl + 1, sizeof(e), s));
+        if(e)
+        {
+            LAB_CUDA(cudaMemsetAsync(A->tri->ctl + 1, 0, sizeof(int32_t), s));
+            set_error("triangular solve: a row waited too long for its dependencies");
+            return LAB_CUDA_ERROR;
         }
         return LAB_OK;
     }
@@ -374,7 +537,8 @@ LAB_API lab_status lab_csrtrsv(lab_csr A, int lower, int unit_diag, const double
     LAB_ARG(A && (A->m == 0 || (b && x)), "null argument");
     LAB_ARG(A->m == A->n, "triangular solve needs a square matrix");
     LAB_TRY(ensure_init());
-    return tri_solve(A, lower != 0, unit_diag != 0, 0.0, b, x, to_stream(s), nullptr);
+    LAB_TRY(tri_solve(A, lower != 0, unit_diag != 0, 0.0, b, x, to_stream(s), nullptr));
+    return tri_check(A, to_stream(s));
 }
 
 LAB_API lab_status lab_csrilu0(lab_csr A, int* structural_zero, int* numeric_zero, lab_stream s)

@@ -1,5 +1,6 @@
-// Triangular path (tri.cu): level-scheduled triangular solves and in-place
-// ILU(0) / IC(0), bit-identical to the reference's sequential loops.
+// Triangular path (tri.cu): one-launch triangular solves over a level order
+// (per-row solved flags) and in-place ILU(0) / IC(0), bit-identical to the
+// reference's sequential loops.
 #pragma once
 
 #include "internal.cuh"
@@ -14,6 +15,10 @@ namespace lab
     // dscale != 0 scales the diagonal (SOR); skip: early-exit flag (graphs).
     lab_status tri_solve(lab_csr_impl* A, bool lower, bool unit, double dscale, const double* b,
                          double* x, cudaStream_t s, const int* skip);
+
+    // Reads (and clears) the error flag of A's solves: LAB_CUDA_ERROR if a solve
+    // gave up waiting (synchronises the stream).
+    lab_status tri_check(lab_csr_impl* A, cudaStream_t s);
 
     // In-place ILU(0) (ic = false) or IC(0); the smallest column of a missing /
     // zero pivot goes to *structural_zero / *numeric_zero (-1: none).

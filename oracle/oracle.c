@@ -1355,36 +1355,91 @@ void orc_trsv(const orc_csr* A, int lower, int unit_diag, const double* b, doubl
  * lower solve (unit / non-unit), upper solve of the same matrix (non-unit; for
  * IC(0) its upper part is A's, unchanged by the factorization);
  * gauss_seidel_precond (90-105): lower non-unit solve on A's lower part;
- * SOR_precond (137-156): the same with the diagonal scaled by 1 / omega. */
-void orc_precond_apply(int kind, double omega, const orc_csr* A, const double* rhs, double* x)
+ * SOR_precond (137-156): the same with the diagonal scaled by 1 / omega.
+ * tri_prepare is the build() (F gets its own values), tri_apply the solve(). */
+static void tri_prepare(int kind, double omega, const orc_csr* A, orc_csr* F)
 {
     const int nnz = A->rp[A->m];
-    orc_csr   F   = *A;
-    F.v         = (double*)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
-    memcpy(F.v, A->v, sizeof(double) * nnz);
+    *F            = *A;
+    F->v          = (double*)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+    memcpy(F->v, A->v, sizeof(double) * nnz);
+    int sz, nz;
+    if(kind == 0)
+        orc_csrilu0(F, &sz, &nz);
+    else if(kind == 1)
+        orc_csric0(F, &sz, &nz);
+    else if(kind == 3)
+    {
+        const double s = 1.0 / omega;
+        for(int i = 0; i < F->m; i++)
+            for(int j = F->rp[i]; j < F->rp[i + 1]; j++)
+                if(F->ci[j] == i)
+                    F->v[j] = F->v[j] * s;
+    }
+}
+
+static void tri_apply(int kind, const orc_csr* F, const double* rhs, double* x, double* y)
+{
     if(kind == 0 || kind == 1)
     {
-        int sz, nz;
-        if(kind == 0)
-            orc_csrilu0(&F, &sz, &nz);
-        else
-            orc_csric0(&F, &sz, &nz);
-        double* y = (double*)malloc(sizeof(double) * (A->m > 0 ? A->m : 1));
-        orc_trsv(&F, 1, kind == 0, rhs, y);
-        orc_trsv(&F, 0, 0, y, x);
-        free(y);
+        orc_trsv(F, 1, kind == 0, rhs, y);
+        orc_trsv(F, 0, 0, y, x);
     }
     else
-    {
-        if(kind == 3)
-        {
-            const double s = 1.0 / omega;
-            for(int i = 0; i < F.m; i++)
-                for(int j = F.rp[i]; j < F.rp[i + 1]; j++)
-                    if(F.ci[j] == i)
-                        F.v[j] = F.v[j] * s;
-        }
-        orc_trsv(&F, 1, 0, rhs, x);
-    }
+        orc_trsv(F, 1, 0, rhs, x);
+}
+
+void orc_precond_apply(int kind, double omega, const orc_csr* A, const double* rhs, double* x)
+{
+    orc_csr F;
+    tri_prepare(kind, omega, A, &F);
+    double* y = (double*)malloc(sizeof(double) * (A->m > 0 ? A->m : 1));
+    tri_apply(kind, &F, rhs, x, y);
+    free(y);
     free(F.v);
+}
+
+/* cg_solver::solve_precond (cg.cpp:136-223) with one of the triangular
+ * preconditioners above (built once, as the reference's build()). */
+int orc_precond_cg(int kind, double omega, const orc_csr* A, const double* b, double* x,
+                   double rel_tol, double abs_tol, int max_iter)
+{
+    const int m = A->m;
+    orc_csr   F;
+    tri_prepare(kind, omega, A, &F);
+    double* r = (double*)malloc(sizeof(double) * ((size_t)m + 1));
+    double* z = (double*)malloc(sizeof(double) * ((size_t)m + 1));
+    double* p = (double*)malloc(sizeof(double) * ((size_t)m + 1));
+    double* y = (double*)malloc(sizeof(double) * ((size_t)m + 1));
+    orc_residual(A, x, b, r);
+    double r0 = orc_norm_inf(r, m);
+    tri_apply(kind, &F, r, z, y);
+    memcpy(p, z, sizeof(double) * (size_t)m);
+    double gamma = orc_dot(z, r, m);
+    int    iter  = 0;
+    while(!(iter > max_iter))
+    {
+        orc_spmv(A, 1.0, p, 0.0, z);
+        double alpha = gamma / orc_dot(z, p, m);
+        for(int i = 0; i < m; i++)
+            x[i] = alpha == 1.0 ? p[i] + x[i] : alpha * p[i] + x[i];
+        double na = -1.0 * alpha;
+        for(int i = 0; i < m; i++)
+            r[i] = na == 1.0 ? z[i] + r[i] : na * z[i] + r[i];
+        if(converges(orc_norm_inf(r, m), r0, rel_tol, abs_tol))
+            break;
+        tri_apply(kind, &F, r, z, y);
+        double old  = gamma;
+        gamma       = orc_dot(z, r, m);
+        double beta = gamma / old;
+        for(int i = 0; i < m; i++)
+            p[i] = beta == 0.0 ? 1.0 * z[i] : 1.0 * z[i] + beta * p[i];
+        iter++;
+    }
+    free(r);
+    free(z);
+    free(p);
+    free(y);
+    free(F.v);
+    return iter;
 }

@@ -108,6 +108,8 @@ void orc_csrilu0(orc_csr* A, int* structural_zero, int* numeric_zero);
 void orc_csric0(orc_csr* A, int* structural_zero, int* numeric_zero);
 void orc_trsv(const orc_csr* A, int lower, int unit_diag, const double* b, double* x);
 void orc_precond_apply(int kind, double omega, const orc_csr* A, const double* rhs, double* x);
+int  orc_precond_cg(int kind, double omega, const orc_csr* A, const double* b, double* x,
+                    double rel_tol, double abs_tol, int max_iter);
 
 #ifdef __cplusplus
 }

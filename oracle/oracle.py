@@ -103,6 +103,8 @@ class Oracle:
         L.orc_csric0.argtypes = [P, _p, _p]
         L.orc_trsv.argtypes = [P, _i, _i, _p, _p]
         L.orc_precond_apply.argtypes = [_i, _d, P, _p, _p]
+        L.orc_precond_cg.argtypes = [_i, _d, P, _p, _p, _d, _d, _i]
+        L.orc_precond_cg.restype = _i
 
     # -- kernels
     def spmv(self, A, x, alpha=1.0, beta=0.0, y=None):
@@ -224,6 +226,15 @@ class Oracle:
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
         self.L.orc_precond_apply(kind, omega, C.byref(s), _ptr(rhs), _ptr(x))
         return x
+
+    def precond_cg(self, kind, A, b, omega=1.0, rel_tol=1e-8, abs_tol=1e-300, max_iter=2000):
+        """CG with preconditioner kind (as precond_apply), built once; (x, iterations)."""
+        s = _csr_in(*A[:3])
+        x = np.zeros(s.m)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        it = self.L.orc_precond_cg(kind, omega, C.byref(s), _ptr(b), _ptr(x), rel_tol, abs_tol,
+                                   max_iter)
+        return x, it
 
     def cg(self, A, b, x0=None, jacobi=False, rel_tol=1e-6, abs_tol=1e-6, max_iter=1000):
         s = _csr_in(*A[:3])

@@ -64,3 +64,18 @@ def test_zero_pivots_reported_like_reference(oracle, reference):
         vr, sr, nr = getattr(reference, fn)(A)
         assert np.array_equal(vo.view(np.int64), vr.view(np.int64)), fn
         assert (so, no) == (sr, nr), fn
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+def test_precond_cg_oracle_vs_reference(oracle, reference, kind):
+    # the whole preconditioned CG (ILU(0) converges; IC(0) as the reference
+    # applies it, Gauss-Seidel and SOR are not symmetric and stagnate).  The
+    # reference's dot products are OpenMP reductions, so the iterates agree to
+    # rounding, not bit for bit.
+    A = P.poisson2d(24)
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    xo, io = oracle.precond_cg(kind, A, b, omega=1.3, max_iter=60)
+    xr, ir = reference.precond_cg(kind, A, b, omega=1.3, max_iter=60)
+    assert io == ir
+    tol = 1e-9 if kind == 0 else 1e-6
+    assert np.max(np.abs(xo - xr)) <= tol * np.max(np.abs(xr))
