@@ -1,5 +1,5 @@
 // Preconditioner plug-in point (library/include/iterative_solvers/preconditioner/preconditioner.h:59-99)
-// with the reference's Jacobi, Gauss-Seidel, SOR, ILU(0) and IC(0)
+// with the reference's Jacobi, Gauss-Seidel, SOR, SSOR, ILU(0) and IC(0)
 // preconditioners (preconditioner.cpp:33-545) and the AMG preconditioner the
 // reference lacks: one multigrid cycle from a zero guess per application.
 #ifndef LINALG_B200_PRECONDITIONER_H
@@ -88,6 +88,21 @@ namespace linalg
 
     public:
         SOR_precond(double omega)
+            : omega(omega)
+        {
+        }
+        void build(const csr_matrix<double>& A) override;
+    };
+
+    // x = U^-1 L^-1 rhs with L = (beta D - E) D^-1, U = beta D - F built from A
+    // (preconditioner.cpp:270-395)
+    class SSOR_precond : public tri_precond_base
+    {
+    private:
+        double omega;
+
+    public:
+        SSOR_precond(double omega)
             : omega(omega)
         {
         }

@@ -177,8 +177,8 @@ LAB_API lab_status lab_exclusive_scan_i64_noalloc(int64_t n, int64_t* x, lab_str
 
 /* Sparse triangular solve x = T^-1 b on the lower (columns < i) or upper part
  * of A, unit or stored diagonal (csrtrsv_analysis / csrtrsv_solve,
- * linalg_math.h:229-254; host_csrtrsv.cpp).  The level schedule is built on first
- * use and kept with A. */
+ * linalg_math.h:229-254; host_csrtrsv.cpp).  The dependency levels of A's pattern
+ * are computed on first use and kept with A; b and x may be the same array. */
 LAB_API lab_status lab_csrtrsv(lab_csr A, int lower, int unit_diag, const double* b, double* x,
                                lab_stream s);
 /* In-place incomplete factorizations of A's values: ILU(0) (csrilu0,
@@ -359,12 +359,15 @@ LAB_API lab_status lab_precond_create_amg(lab_hierarchy h, const lab_amg_options
 LAB_API lab_status lab_precond_create_jacobi(lab_csr A, lab_precond* M, lab_stream s);
 /* Triangular-solve preconditioners (preconditioner.h:172-580): ILU(0) and IC(0)
  * factor a copy of A (ilu_precond / ic_precond::build), Gauss-Seidel and SOR(omega)
- * solve with A's lower part (gauss_seidel_precond, SOR_precond).  Each application
- * runs the reference's triangular solves, level-scheduled, bit-identical. */
+ * solve with the lower part of a copy of A (gauss_seidel_precond, SOR_precond),
+ * SSOR(omega) with the two triangles SSOR_precond::build makes from A.  Each
+ * application runs the reference's triangular solves, bit-identical.  All need
+ * 0 < omega < 2 where they take one. */
 LAB_API lab_status lab_precond_create_ilu0(lab_csr A, lab_precond* M, lab_stream s);
 LAB_API lab_status lab_precond_create_ic0(lab_csr A, lab_precond* M, lab_stream s);
 LAB_API lab_status lab_precond_create_gauss_seidel(lab_csr A, lab_precond* M, lab_stream s);
 LAB_API lab_status lab_precond_create_sor(lab_csr A, double omega, lab_precond* M, lab_stream s);
+LAB_API lab_status lab_precond_create_ssor(lab_csr A, double omega, lab_precond* M, lab_stream s);
 /* z = M^{-1} r.  preconditioner::solve (preconditioner.h:78). */
 LAB_API lab_status lab_precond_apply(lab_precond M, const double* r, double* z, lab_stream s);
 LAB_API lab_status lab_precond_destroy(lab_precond M);

@@ -106,6 +106,7 @@ _SIGS = {
     "lab_precond_create_ic0": [_p, C.POINTER(_p), _p],
     "lab_precond_create_gauss_seidel": [_p, C.POINTER(_p), _p],
     "lab_precond_create_sor": [_p, _d, C.POINTER(_p), _p],
+    "lab_precond_create_ssor": [_p, _d, C.POINTER(_p), _p],
     "lab_spmv_autotune": [_p, _i, C.POINTER(_d), _p],
     "lab_hierarchy_autotune": [_p, _i, _p],
     "lab_hierarchy_save": [_p, C.c_char_p, _p],

@@ -168,7 +168,7 @@ class CsrMatrix:
         return self._new("lab_transpose", self.h)
 
     def trsv(self, b, lower=True, unit_diag=False, x=None):
-        """x = T^-1 b on the lower or upper part (level-scheduled, reference order)."""
+        """x = T^-1 b on the lower or upper part (reference order, bit-identical)."""
         if x is None:
             x = torch.empty_like(b)
         call("lab_csrtrsv", self.h, int(bool(lower)), int(bool(unit_diag)), ptr(b), ptr(x),
@@ -360,6 +360,10 @@ class Preconditioner:
     @classmethod
     def sor(cls, A: CsrMatrix, omega: float):
         return cls._tri("lab_precond_create_sor", A, C.c_double(omega))
+
+    @classmethod
+    def ssor(cls, A: CsrMatrix, omega: float):
+        return cls._tri("lab_precond_create_ssor", A, C.c_double(omega))
 
     def apply(self, r, z=None):
         if z is None:

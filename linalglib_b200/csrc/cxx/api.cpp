@@ -1235,6 +1235,12 @@ namespace linalg
         ok(lab_precond_create_sor(A.device(), omega, &P, nullptr), "SOR_precond::build");
         rebuild(P);
     }
+    void SSOR_precond::build(const csr_matrix<double>& A)
+    {
+        lab_precond P = nullptr;
+        ok(lab_precond_create_ssor(A.device(), omega, &P, nullptr), "SSOR_precond::build");
+        rebuild(P);
+    }
     void ilu_precond::build(const csr_matrix<double>& A)
     {
         lab_precond P = nullptr;

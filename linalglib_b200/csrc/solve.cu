@@ -14,18 +14,22 @@ namespace lab
     struct precond_impl
     {
         uint64_t         uid  = next_uid();
-        int              kind = 0; // 0 AMG, 1 Jacobi, 2 ILU(0), 3 IC(0), 4 Gauss-Seidel, 5 SOR
+        // 0 AMG, 1 Jacobi, 2 ILU(0), 3 IC(0), 4 Gauss-Seidel, 5 SOR, 6 SSOR
+        int              kind = 0;
         hierarchy_impl*  h    = nullptr;
         lab_amg_options  o;
-        lab_csr_impl*    A    = nullptr; // Jacobi, Gauss-Seidel, SOR: the operator
+        lab_csr_impl*    A    = nullptr; // the operator
         double*          diag = nullptr; // Jacobi: the reference divides by the diagonal
-        lab_csr_impl*    F    = nullptr; // ILU(0) / IC(0): factored copy of the operator
-        double*          y    = nullptr; // ILU(0) / IC(0): intermediate of the two solves
+        lab_csr_impl*    F    = nullptr; // kinds 2-5: factored / copied operator; SSOR: L
+        lab_csr_impl*    G    = nullptr; // SSOR: U
+        double*          y    = nullptr; // intermediate of the two solves (kinds 2, 3, 6)
         double           dscale = 0.0;   // SOR: diagonal scale 1 / omega
         ~precond_impl()
         {
             if(F)
                 csr_release(F);
+            if(G)
+                csr_release(G);
             if(y)
                 cudaFree(y);
         }
@@ -57,11 +61,17 @@ namespace lab
         {
             // preconditioner.cpp: ILU(0) 452-467, IC(0) 527-542 (lower then upper
             // solve of the factored copy), Gauss-Seidel 98-105 and SOR 149-156
-            // (one lower solve on A, SOR's diagonal scaled by 1 / omega)
+            // (one lower solve on A, SOR's diagonal scaled by 1 / omega), SSOR
+            // (lower solve with L, upper solve with U)
             if(M->kind == 2 || M->kind == 3)
             {
                 LAB_TRY(tri_solve(M->F, true, M->kind == 2, 0.0, r, M->y, s, skip));
                 LAB_TRY(tri_solve(M->F, false, false, 0.0, M->y, z, s, skip));
+            }
+            else if(M->kind == 6) // SSOR_precond::solve 355-395 (host trsv: alpha unused)
+            {
+                LAB_TRY(tri_solve(M->F, true, false, 0.0, r, M->y, s, skip));
+                LAB_TRY(tri_solve(M->G, false, false, 0.0, M->y, z, s, skip));
             }
             else
                 LAB_TRY(tri_solve(M->F, true, false, M->dscale, r, z, s, skip));
@@ -1528,13 +1538,16 @@ LAB_API lab_status lab_precond_create_jacobi(lab_csr A, lab_precond* out, lab_st
 // arrive (a bug, not an input property): report it over the solver's status.
 static lab_status tri_status(lab_precond_s* M, lab_status st, cudaStream_t s)
 {
-    const lab_status e = tri_check(M->F, s);
+    lab_status e = tri_check(M->F, s);
+    if(e == LAB_OK && M->G)
+        e = tri_check(M->G, s);
     return e != LAB_OK ? e : st;
 }
 
 // ILU(0) / IC(0): factor a copy of A (ilu_precond::build, preconditioner.cpp:432-450;
 // ic_precond::build, 506-524).  Gauss-Seidel / SOR: solve with the lower part of
 // a copy of A (gauss_seidel_precond::build 90-96, SOR_precond::build 137-147).
+// SSOR: the two triangles L and U of SSOR_precond::build (283-353).
 static lab_status create_tri_precond(lab_csr A, int kind, double omega, lab_precond* out,
                                      lab_stream ls)
 {
@@ -1548,14 +1561,26 @@ static lab_status create_tri_precond(lab_csr A, int kind, double omega, lab_prec
     M->kind       = kind;
     M->A          = A;
     M->dscale     = kind == 5 ? 1.0 / omega : 0.0; // SOR: scale_diagonal_by(1.0 / omega)
-    // like the reference's build(), every kind works on its own copy of A
+    // like the reference's build(), every kind works on its own copy of A (SSOR:
+    // on the two triangles built from it)
     lab_csr    F  = nullptr;
-    lab_status st = lab_csr_clone(A, &F, ls);
-    if(st == LAB_OK)
+    lab_status st = LAB_OK;
+    if(kind == 6)
     {
-        M->F = F;
-        st   = tri_analyse(M->F, s);
+        st = ssor_split(A, omega, &M->F, &M->G, s);
+        if(st == LAB_OK)
+            st = tri_analyse(M->G, s);
+        if(st == LAB_OK)
+            st = dalloc(&M->y, (size_t)A->m + 1, s);
     }
+    else
+    {
+        st = lab_csr_clone(A, &F, ls);
+        if(st == LAB_OK)
+            M->F = F;
+    }
+    if(st == LAB_OK)
+        st = tri_analyse(M->F, s);
     if(st == LAB_OK && (kind == 2 || kind == 3))
     {
         int sz = -1, nz = -1;
@@ -1591,6 +1616,12 @@ LAB_API lab_status lab_precond_create_sor(lab_csr A, double omega, lab_precond* 
 {
     LAB_ARG(omega > 0.0 && omega < 2.0, "SOR needs 0 < omega < 2");
     return create_tri_precond(A, 5, omega, M, s);
+}
+
+LAB_API lab_status lab_precond_create_ssor(lab_csr A, double omega, lab_precond* M, lab_stream s)
+{
+    LAB_ARG(omega > 0.0 && omega < 2.0, "SSOR needs 0 < omega < 2");
+    return create_tri_precond(A, 6, omega, M, s);
 }
 
 LAB_API lab_status lab_precond_apply(lab_precond M, const double* r, double* z, lab_stream s)

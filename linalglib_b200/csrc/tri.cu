@@ -527,6 +527,126 @@ namespace lab
     }
 }
 
+namespace lab
+{
+    // ------------------------------------------------------------ SSOR split
+    // SSOR_precond::build (preconditioner.cpp:283-353): L = (beta D - E) D^-1 holds
+    // a_ij / d_j left of the diagonal and beta on it; U = beta D - F holds a_ij
+    // right of it and beta * a_ii on it (host_ssor.cpp:52-142; d = the row's first
+    // diagonal entry, 0 if none).  Entries keep A's order within each row.
+    __global__ void k_ssor_count(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                 const double* __restrict__ v, int m, int32_t* cl, int32_t* cu,
+                                 double* d)
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int    nl = 0, nu = 0;
+        double di = 0.0;
+        bool   found = false;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+        {
+            const int c = ci[j];
+            nl += c <= i;
+            nu += c >= i;
+            if(c == i && !found)
+            {
+                di    = v[j];
+                found = true;
+            }
+        }
+        cl[i] = nl;
+        cu[i] = nu;
+        d[i]  = di;
+    }
+
+    __global__ void k_ssor_fill(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                const double* __restrict__ v, int m, const double* __restrict__ d,
+                                double beta, const int32_t* __restrict__ lrp, int32_t* lci,
+                                double* lv, const int32_t* __restrict__ urp, int32_t* uci,
+                                double* uv)
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int kl = lrp[i], ku = urp[i];
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+        {
+            const int    c = ci[j];
+            const double a = v[j];
+            if(c < i)
+            {
+                lci[kl]  = c;
+                lv[kl++] = __ddiv_rn(a, d[c]);
+            }
+            else if(c > i)
+            {
+                uci[ku]  = c;
+                uv[ku++] = a;
+            }
+            else
+            {
+                lci[kl]  = c;
+                lv[kl++] = beta;
+                uci[ku]  = c;
+                uv[ku++] = __dmul_rn(beta, a);
+            }
+        }
+    }
+
+    lab_status ssor_split(lab_csr_impl* A, double omega, lab_csr_impl** L, lab_csr_impl** U,
+                          cudaStream_t s)
+    {
+        const int m = (int)A->m;
+        // build() hands 1 / omega to the fill routines, which take its inverse again
+        const double beta_in = 1.0 / omega;
+        const double beta    = 1.0 / beta_in;
+        dbuf<int32_t> cl, cu;
+        dbuf<double>  d;
+        LAB_TRY(cl.alloc((size_t)m + 1, s));
+        LAB_TRY(cu.alloc((size_t)m + 1, s));
+        LAB_TRY(d.alloc((size_t)m, s));
+        LAB_CUDA(cudaMemsetAsync(cl.get() + m, 0, sizeof(int32_t), s));
+        LAB_CUDA(cudaMemsetAsync(cu.get() + m, 0, sizeof(int32_t), s));
+        if(m > 0)
+            LAB_LAUNCH(k_ssor_count, (unsigned)ceil_div(m, 256), 256, 0, s, A->row_ptr, A->col_ind,
+                       (const double*)A->val, m, cl.get(), cu.get(), d.get());
+        LAB_TRY(scan_i32(cl.get(), (int64_t)m + 1, s));
+        LAB_TRY(scan_i32(cu.get(), (int64_t)m + 1, s));
+        int32_t nl = 0, nu = 0;
+        LAB_TRY(copy_d2h_sync(&nl, cl.get() + m, sizeof(nl), s));
+        LAB_TRY(copy_d2h_sync(&nu, cu.get() + m, sizeof(nu), s));
+        lab_csr_impl *l = nullptr, *u = nullptr;
+        LAB_TRY(csr_alloc(&l, A->m, A->n, nl, s));
+        lab_status st = csr_alloc(&u, A->m, A->n, nu, s);
+        if(st == LAB_OK &&
+           (cudaMemcpyAsync(l->row_ptr, cl.get(), sizeof(int32_t) * ((size_t)m + 1),
+                            cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(u->row_ptr, cu.get(), sizeof(int32_t) * ((size_t)m + 1),
+                            cudaMemcpyDeviceToDevice, s) != cudaSuccess))
+            st = LAB_CUDA_ERROR;
+        if(st == LAB_OK && m > 0)
+        {
+            k_ssor_fill<<<(unsigned)ceil_div(m, 256), 256, 0, s>>>(
+                A->row_ptr, A->col_ind, (const double*)A->val, m, d.get(), beta, l->row_ptr,
+                l->col_ind, (double*)l->val, u->row_ptr, u->col_ind, (double*)u->val);
+            g_launches.fetch_add(1);
+            if(cudaGetLastError() != cudaSuccess)
+                st = LAB_CUDA_ERROR;
+        }
+        if(st != LAB_OK)
+        {
+            csr_release(l);
+            if(u)
+                csr_release(u);
+            return st;
+        }
+        *L = l;
+        *U = u;
+        return LAB_OK;
+    }
+}
+
 using namespace lab;
 
 extern "C" {

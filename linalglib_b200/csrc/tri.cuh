@@ -16,6 +16,11 @@ namespace lab
     lab_status tri_solve(lab_csr_impl* A, bool lower, bool unit, double dscale, const double* b,
                          double* x, cudaStream_t s, const int* skip);
 
+    // The two triangles of the reference's SSOR preconditioner built from A
+    // (new matrices owned by the caller).
+    lab_status ssor_split(lab_csr_impl* A, double omega, lab_csr_impl** L, lab_csr_impl** U,
+                          cudaStream_t s);
+
     // Reads (and clears) the error flag of A's solves: LAB_CUDA_ERROR if a solve
     // gave up waiting (synchronises the stream).
     lab_status tri_check(lab_csr_impl* A, cudaStream_t s);

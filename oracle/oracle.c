@@ -1355,10 +1355,80 @@ void orc_trsv(const orc_csr* A, int lower, int unit_diag, const double* b, doubl
  * lower solve (unit / non-unit), upper solve of the same matrix (non-unit; for
  * IC(0) its upper part is A's, unchanged by the factorization);
  * gauss_seidel_precond (90-105): lower non-unit solve on A's lower part;
- * SOR_precond (137-156): the same with the diagonal scaled by 1 / omega.
- * tri_prepare is the build() (F gets its own values), tri_apply the solve(). */
-static void tri_prepare(int kind, double omega, const orc_csr* A, orc_csr* F)
+ * SOR_precond (137-156): the same with the diagonal scaled by 1 / omega;
+ * SSOR_precond (kind 4, below).  tri_prepare is the build() (F gets its own
+ * values), tri_apply the solve(). */
+/* SSOR_precond::build (preconditioner.cpp:283-353) with host_ssor_fill_lower_precond
+ * / host_ssor_fill_upper_precond (host_ssor.cpp:52-142): L holds a_ij / d_j left of
+ * the diagonal and "beta" on it, U holds a_ij right of it and beta * a_ii on it, d
+ * the first stored diagonal entry (0 if none).  build() passes 1 / omega as the
+ * fill routines' omega, which compute beta = 1 / omega again, so beta is
+ * 1 / (1 / omega) (rounded twice), not 1 / omega. */
+static void ssor_split(double omega, const orc_csr* A, orc_csr* L, orc_csr* U)
 {
+    const int m     = A->m;
+    double*   d     = (double*)calloc((size_t)(m > 0 ? m : 1), sizeof(double));
+    const double b1 = 1.0 / omega;
+    const double beta = 1.0 / b1;
+    for(int i = 0; i < m; i++)
+        for(int j = A->rp[i]; j < A->rp[i + 1]; j++)
+            if(A->ci[j] == i)
+            {
+                d[i] = A->v[j];
+                break;
+            }
+    orc_csr* T[2] = {L, U};
+    for(int t = 0; t < 2; t++)
+    {
+        orc_csr* X = T[t];
+        X->m       = m;
+        X->n       = A->n;
+        X->rp      = (int*)malloc(sizeof(int) * ((size_t)m + 1));
+        X->rp[0]   = 0;
+        for(int i = 0; i < m; i++)
+        {
+            int c = 0;
+            for(int j = A->rp[i]; j < A->rp[i + 1]; j++)
+                if(t == 0 ? A->ci[j] <= i : A->ci[j] >= i)
+                    c++;
+            X->rp[i + 1] = X->rp[i] + c;
+        }
+        const int nz = X->rp[m];
+        X->nnz       = nz;
+        X->ci        = (int*)malloc(sizeof(int) * (size_t)(nz > 0 ? nz : 1));
+        X->v         = (double*)malloc(sizeof(double) * (size_t)(nz > 0 ? nz : 1));
+        for(int i = 0; i < m; i++)
+        {
+            int k = X->rp[i];
+            for(int j = A->rp[i]; j < A->rp[i + 1]; j++)
+            {
+                const int c = A->ci[j];
+                if(t == 0 && c < i)
+                    X->ci[k] = c, X->v[k++] = A->v[j] / d[c];
+                else if(t == 1 && c > i)
+                    X->ci[k] = c, X->v[k++] = A->v[j];
+                else if(c == i)
+                    X->ci[k] = c, X->v[k++] = t == 0 ? beta : beta * A->v[j];
+            }
+        }
+    }
+    free(d);
+}
+
+static void csr_free_all(orc_csr* X)
+{
+    free(X->rp);
+    free(X->ci);
+    free(X->v);
+}
+
+static void tri_prepare(int kind, double omega, const orc_csr* A, orc_csr* F, orc_csr* G)
+{
+    if(kind == 4)
+    {
+        ssor_split(omega, A, F, G);
+        return;
+    }
     const int nnz = A->rp[A->m];
     *F            = *A;
     F->v          = (double*)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
@@ -1378,12 +1448,31 @@ static void tri_prepare(int kind, double omega, const orc_csr* A, orc_csr* F)
     }
 }
 
-static void tri_apply(int kind, const orc_csr* F, const double* rhs, double* x, double* y)
+static void tri_release_pc(int kind, orc_csr* F, orc_csr* G)
+{
+    if(kind == 4)
+    {
+        csr_free_all(F);
+        csr_free_all(G);
+    }
+    else
+        free(F->v);
+}
+
+/* SSOR_precond::solve (preconditioner.cpp:355-395): lower solve with L (the host
+ * csrtrsv_solve ignores its alpha argument), upper solve with U. */
+static void tri_apply(int kind, const orc_csr* F, const orc_csr* G, const double* rhs, double* x,
+                      double* y)
 {
     if(kind == 0 || kind == 1)
     {
         orc_trsv(F, 1, kind == 0, rhs, y);
         orc_trsv(F, 0, 0, y, x);
+    }
+    else if(kind == 4)
+    {
+        orc_trsv(F, 1, 0, rhs, y);
+        orc_trsv(G, 0, 0, y, x);
     }
     else
         orc_trsv(F, 1, 0, rhs, x);
@@ -1391,12 +1480,12 @@ static void tri_apply(int kind, const orc_csr* F, const double* rhs, double* x, 
 
 void orc_precond_apply(int kind, double omega, const orc_csr* A, const double* rhs, double* x)
 {
-    orc_csr F;
-    tri_prepare(kind, omega, A, &F);
+    orc_csr F, G;
+    tri_prepare(kind, omega, A, &F, &G);
     double* y = (double*)malloc(sizeof(double) * (A->m > 0 ? A->m : 1));
-    tri_apply(kind, &F, rhs, x, y);
+    tri_apply(kind, &F, &G, rhs, x, y);
     free(y);
-    free(F.v);
+    tri_release_pc(kind, &F, &G);
 }
 
 /* cg_solver::solve_precond (cg.cpp:136-223) with one of the triangular
@@ -1405,15 +1494,15 @@ int orc_precond_cg(int kind, double omega, const orc_csr* A, const double* b, do
                    double rel_tol, double abs_tol, int max_iter)
 {
     const int m = A->m;
-    orc_csr   F;
-    tri_prepare(kind, omega, A, &F);
+    orc_csr   F, G;
+    tri_prepare(kind, omega, A, &F, &G);
     double* r = (double*)malloc(sizeof(double) * ((size_t)m + 1));
     double* z = (double*)malloc(sizeof(double) * ((size_t)m + 1));
     double* p = (double*)malloc(sizeof(double) * ((size_t)m + 1));
     double* y = (double*)malloc(sizeof(double) * ((size_t)m + 1));
     orc_residual(A, x, b, r);
     double r0 = orc_norm_inf(r, m);
-    tri_apply(kind, &F, r, z, y);
+    tri_apply(kind, &F, &G, r, z, y);
     memcpy(p, z, sizeof(double) * (size_t)m);
     double gamma = orc_dot(z, r, m);
     int    iter  = 0;
@@ -1428,7 +1517,7 @@ int orc_precond_cg(int kind, double omega, const orc_csr* A, const double* b, do
             r[i] = na == 1.0 ? z[i] + r[i] : na * z[i] + r[i];
         if(converges(orc_norm_inf(r, m), r0, rel_tol, abs_tol))
             break;
-        tri_apply(kind, &F, r, z, y);
+        tri_apply(kind, &F, &G, r, z, y);
         double old  = gamma;
         gamma       = orc_dot(z, r, m);
         double beta = gamma / old;
@@ -1440,6 +1529,6 @@ int orc_precond_cg(int kind, double omega, const orc_csr* A, const double* b, do
     free(z);
     free(p);
     free(y);
-    free(F.v);
+    tri_release_pc(kind, &F, &G);
     return iter;
 }

@@ -220,7 +220,7 @@ class Oracle:
         return x
 
     def precond_apply(self, kind, A, rhs, omega=1.0):
-        """kind 0 ILU(0), 1 IC(0), 2 Gauss-Seidel, 3 SOR(omega)."""
+        """kind 0 ILU(0), 1 IC(0), 2 Gauss-Seidel, 3 SOR(omega), 4 SSOR(omega)."""
         s = _csr_in(*A[:3])
         x = np.zeros(s.m)
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)

@@ -493,7 +493,7 @@ void ref_trsv(int m, int nnz, const int* rp, const int* ci, const double* v, int
 
 // One application x = M^-1 rhs of the reference's triangular-solve
 // preconditioners (preconditioner.cpp): kind 0 ILU(0), 1 IC(0), 2 Gauss-Seidel,
-// 3 SOR(omega).
+// 3 SOR(omega), 4 SSOR(omega).
 void ref_precond_apply(int kind, double omega, int m, int nnz, const int* rp, const int* ci,
                        const double* v, const double* rhs, double* x)
 {
@@ -507,8 +507,10 @@ void ref_precond_apply(int kind, double omega, int m, int nnz, const int* rp, co
         P = new ic_precond();
     else if(kind == 2)
         P = new gauss_seidel_precond();
-    else
+    else if(kind == 3)
         P = new SOR_precond(omega);
+    else
+        P = new SSOR_precond(omega);
     P->build(A);
     vector<double> vr(std::vector<double>(rhs, rhs + m));
     vector<double> vx(m);
@@ -532,8 +534,10 @@ int ref_precond_cg(int kind, double omega, int m, int nnz, const int* rp, const 
         P = new ic_precond();
     else if(kind == 2)
         P = new gauss_seidel_precond();
-    else
+    else if(kind == 3)
         P = new SOR_precond(omega);
+    else
+        P = new SSOR_precond(omega);
     P->build(A);
     vector<double> vb(std::vector<double>(b, b + m));
     vector<double> vx(std::vector<double>(x, x + m));

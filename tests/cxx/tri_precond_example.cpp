@@ -1,8 +1,10 @@
 // The reference's triangular-solve preconditioners and free functions
-// (preconditioner.h: ilu_precond, ic_precond, gauss_seidel_precond, SOR_precond;
+// (preconditioner.h: ilu_precond, ic_precond, gauss_seidel_precond, SOR_precond,
+// SSOR_precond;
 // linalg_math.h: csrilu0, csrtrsv_*) through this library's C++ API.
 // Usage: tri_precond_example <grid n>.  Prints one line
-//   "<ilu cg iters> <converged> <gs gmres cycles> <sor gmres cycles> <gmres rel res>"
+//   "<ilu cg iters> <converged> <gs gmres cycles> <sor gmres cycles> <gmres rel res>
+//    <structural zero> <numeric zero> <ssor cg iters>"
 // then the ILU(0) factor values and the unit-lower solve of ones, one hex float
 // per line, for a bit-for-bit comparison.
 #include "linalg.h"
@@ -60,6 +62,13 @@ int main(int argc, char** argv)
     int iters = cg.solve(A, x, b, &ilu, control);
     int conv  = cg.last_info().converged;
 
+    // SSOR(1.3)-preconditioned CG
+    SSOR_precond ssor(1.3);
+    ssor.build(A);
+    x.zeros();
+    int ssor_iters = cg.solve(A, x, b, &ssor, control);
+    conv           = conv && cg.last_info().converged;
+
     // Gauss-Seidel and SOR under restarted GMRES
     gmres_solver gm;
     gm.build(A, 20);
@@ -88,8 +97,8 @@ int main(int argc, char** argv)
     csrtrsv_solve(LU, e, y, 1.0, triangular_type::lower, diagonal_type::unit, d);
     destroy_csrtrsv_descr(d);
 
-    std::printf("%d %d %d %d %.3e %d %d\n", iters, conv, gs_cycles, sor_cycles, rel,
-                sz == INT_MAX ? -1 : sz, nz == INT_MAX ? -1 : nz);
+    std::printf("%d %d %d %d %.3e %d %d %d\n", iters, conv, gs_cycles, sor_cycles, rel,
+                sz == INT_MAX ? -1 : sz, nz == INT_MAX ? -1 : nz, ssor_iters);
     const double* lv = LU.get_val();
     for(int j = 0; j < LU.get_nnz(); j++)
         std::printf("%a\n", lv[j]);

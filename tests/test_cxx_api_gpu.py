@@ -51,7 +51,7 @@ def test_cxx_triangular_preconditioners(gpu, oracle, reference, tmp_path_factory
     out = subprocess.run([exe, str(n)], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     lines = out.stdout.split("\n")
-    iters, conv, gs_cycles, sor_cycles, rel, sz, nz = lines[0].split()
+    iters, conv, gs_cycles, sor_cycles, rel, sz, nz, ssor_iters = lines[0].split()
     A = P.poisson2d(n)
     m, nnz = n * n, A[2].size
     vals = np.array([float.fromhex(t) for t in lines[1:1 + nnz]])
@@ -64,6 +64,8 @@ def test_cxx_triangular_preconditioners(gpu, oracle, reference, tmp_path_factory
     b = P.csr_matvec(*A[:3], np.ones(m))
     _, itr = reference.precond_cg(0, A, b, rel_tol=1e-8, abs_tol=1e-300, max_iter=1000)
     assert int(conv) == 1 and abs(int(iters) - itr) <= 1, (iters, itr)
+    _, its = reference.precond_cg(4, A, b, omega=1.3, rel_tol=1e-8, abs_tol=1e-300, max_iter=1000)
+    assert abs(int(ssor_iters) - its) <= 1, (ssor_iters, its)
     # GMRES stops on the preconditioned 2-norm residual (1e-10 relative); the
     # printed figure is the true inf-norm residual
     assert float(rel) <= 1e-8

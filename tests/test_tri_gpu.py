@@ -1,5 +1,5 @@
 """Level-scheduled triangular path on the GPU: lab_csrtrsv, lab_csrilu0 /
-lab_csric0 and the ILU(0) / IC(0) / Gauss-Seidel / SOR preconditioners are
+lab_csric0 and the ILU(0) / IC(0) / Gauss-Seidel / SOR / SSOR preconditioners are
 bit-identical to the oracle (which is pinned bit-exact to the reference's
 host_csrtrsv.cpp, host_csrilu0.cpp, host_csric0.cpp and preconditioner.cpp), and
 PCG with them behaves as the reference's cg_solver does."""
@@ -68,13 +68,18 @@ def test_factor_zero_pivots(gpu, oracle):
         assert np.array_equal(_bits(dA.to_numpy()[2]), _bits(vo)), kind
 
 
+def _precond(gpu, kind, dA, omega=1.3):
+    return [gpu.Preconditioner.ilu0, gpu.Preconditioner.ic0, gpu.Preconditioner.gauss_seidel,
+            lambda X: gpu.Preconditioner.sor(X, omega),
+            lambda X: gpu.Preconditioner.ssor(X, omega)][kind](dA)
+
+
 @pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
 def test_precond_apply_bit_exact(gpu, oracle, name, kind):
     A = CASES[name]()
     dA = gpu.CsrMatrix.from_arrays(*A[:3])
-    M = [gpu.Preconditioner.ilu0, gpu.Preconditioner.ic0, gpu.Preconditioner.gauss_seidel,
-         lambda X: gpu.Preconditioner.sor(X, 1.3)][kind](dA)
+    M = _precond(gpu, kind, dA)
     r = np.random.default_rng(4).uniform(-1, 1, A[0].size - 1)
     z = M.apply(gpu.vec(r)).cpu().numpy()
     assert np.array_equal(_bits(z), _bits(oracle.precond_apply(kind, A, r, omega=1.3)))
@@ -82,14 +87,15 @@ def test_precond_apply_bit_exact(gpu, oracle, name, kind):
     assert np.array_equal(_bits(dA.to_numpy()[2]), _bits(A[2]))
 
 
-def test_ilu_pcg_matches_reference(gpu, reference):
+@pytest.mark.parametrize("kind,omega,expected", [(0, 1.0, 24), (4, 1.3, 32), (4, 1.0, 26)])
+def test_ilu_ssor_pcg_matches_reference(gpu, reference, kind, omega, expected):
     A = P.poisson2d(24)
     b, xt = P.rhs_from_solution(*A[:3], seed=0)
     dA = gpu.CsrMatrix.from_arrays(*A[:3])
-    x, info = gpu.pcg(dA, gpu.vec(b), M=gpu.Preconditioner.ilu0(dA),
+    x, info = gpu.pcg(dA, gpu.vec(b), M=_precond(gpu, kind, dA, omega),
                       control=gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=1000))
-    xr, itr = reference.precond_cg(0, A, b, rel_tol=1e-8, abs_tol=1e-300)
-    assert itr == 24  # the reference's count on this problem
+    xr, itr = reference.precond_cg(kind, A, b, omega=omega, rel_tol=1e-8, abs_tol=1e-300)
+    assert itr == expected  # the reference's count on this problem
     assert info.converged == 1
     assert abs(info.iterations - itr) <= 1, (info.iterations, itr)
     assert np.max(np.abs(x.cpu().numpy() - xr)) <= 1e-7 * np.max(np.abs(xr))
@@ -106,8 +112,7 @@ def test_nonsymmetric_precond_pcg_like_reference(gpu, reference, kind):
     A = P.poisson2d(24)
     b, _ = P.rhs_from_solution(*A[:3], seed=0)
     dA = gpu.CsrMatrix.from_arrays(*A[:3])
-    M = [None, gpu.Preconditioner.ic0, gpu.Preconditioner.gauss_seidel,
-         lambda X: gpu.Preconditioner.sor(X, 1.3)][kind](dA)
+    M = _precond(gpu, kind, dA)
     x, info = gpu.pcg(dA, gpu.vec(b), M=M,
                       control=gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=50))
     xr, itr = reference.precond_cg(kind, A, b, omega=1.3, rel_tol=1e-8, abs_tol=1e-300,
@@ -129,3 +134,17 @@ def test_nonsymmetric_preconds_under_gmres(gpu, name):
                             control=gpu.iter_control(rel_tol=1e-10, abs_tol=0.0, max_iter=2000))
         assert info.converged == 1
         assert np.max(np.abs(x.cpu().numpy() - xt)) <= 1e-6 * np.max(np.abs(xt))
+
+
+def test_trsv_in_place_and_ssor_arg_check(gpu, oracle):
+    A = P.poisson3d(12)
+    b = np.random.default_rng(7).uniform(-1, 1, A[0].size - 1)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    for lower in (True, False):
+        xb = gpu.vec(b)
+        dA.trsv(xb, lower=lower, unit_diag=False, x=xb)  # b and x the same array
+        assert np.array_equal(_bits(xb.cpu().numpy()), _bits(oracle.trsv(A, b, lower, False)))
+    from linalglib_b200 import _lib as L
+    for bad in (0.0, 2.0, -1.0):
+        with pytest.raises(L.LabError):
+            gpu.Preconditioner.ssor(dA, bad)

@@ -1,7 +1,7 @@
 """Triangular path on the CPU: the C restatement (oracle/oracle.c) against the
 compiled reference -- ILU(0), IC(0), lower/upper triangular solves and the
-ILU(0) / IC(0) / Gauss-Seidel / SOR preconditioner applications must agree bit
-for bit (host_csrilu0.cpp, host_csric0.cpp, host_csrtrsv.cpp, preconditioner.cpp)."""
+ILU(0) / IC(0) / Gauss-Seidel / SOR / SSOR preconditioner applications must agree
+bit for bit (host_csrilu0.cpp, host_csric0.cpp, host_csrtrsv.cpp, preconditioner.cpp)."""
 import numpy as np
 import pytest
 
@@ -34,7 +34,7 @@ def test_trsv_oracle_vs_reference(oracle, reference, name, lower, unit):
 
 
 @pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
 def test_precond_apply_oracle_vs_reference(oracle, reference, name, kind):
     A = CASES[name]()
     r = np.random.default_rng(4).uniform(-1, 1, A[0].size - 1)
@@ -66,10 +66,10 @@ def test_zero_pivots_reported_like_reference(oracle, reference):
         assert (so, no) == (sr, nr), fn
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
 def test_precond_cg_oracle_vs_reference(oracle, reference, kind):
-    # the whole preconditioned CG (ILU(0) converges; IC(0) as the reference
-    # applies it, Gauss-Seidel and SOR are not symmetric and stagnate).  The
+    # the whole preconditioned CG (ILU(0) and SSOR converge; IC(0) as the
+    # reference applies it, Gauss-Seidel and SOR are not symmetric and stagnate).  The
     # reference's dot products are OpenMP reductions, so the iterates agree to
     # rounding, not bit for bit.
     A = P.poisson2d(24)
@@ -77,5 +77,5 @@ def test_precond_cg_oracle_vs_reference(oracle, reference, kind):
     xo, io = oracle.precond_cg(kind, A, b, omega=1.3, max_iter=60)
     xr, ir = reference.precond_cg(kind, A, b, omega=1.3, max_iter=60)
     assert io == ir
-    tol = 1e-9 if kind == 0 else 1e-6
+    tol = 1e-9 if kind in (0, 4) else 1e-6
     assert np.max(np.abs(xo - xr)) <= tol * np.max(np.abs(xr))
