@@ -314,6 +314,36 @@ def dominant_kernel_roofline(core, dA, m, nnz, torch, profiled=True):
             "launch_us": t * 1e6}
 
 
+def pcg_iteration_roofline(core, dA, solve_ms, iters, peak):
+    """Whole PCG iteration against HBM: algorithmic bytes of one iteration on the
+    built hierarchy, B_spmv(A_0) + B_vcycle + 8 m_0 k (k = 10 vector passes), with
+    B_vcycle = sum over levels l < L of 2 B_jac(l) + B_spmv(A_l) + |R_l| + |P_l|
+    + 8 (4 m_l + 2 m_l+1), B_jac(l) = |A_l| + 24 m_l, |X| = 8 nnz + 4 (nnz + m + 1),
+    plus the coarsest dense solve (8 m_L^2); time = median PCG time / iterations."""
+    H = core.Hierarchy(dA)
+
+    def size(X):
+        mm, nn, zz = X.info()
+        return mm, nn, zz, 8 * zz + 4 * (zz + mm + 1)
+
+    L = H.levels
+    b_cycle = 0
+    for l in range(L):
+        ml, nl, zl, al = size(H.A(l))
+        mc = H.A(l + 1).info()[0]
+        b_cycle += (2 * (al + 24 * ml) + spmv_bytes(ml, nl, zl) + size(H.R(l))[3]
+                    + size(H.P(l))[3] + 8 * (4 * ml + 2 * mc))
+    mL = H.A(L).info()[0]
+    b_cycle += 8 * mL * mL
+    m0, n0, z0, _ = size(H.A(0))
+    b_iter = spmv_bytes(m0, n0, z0) + b_cycle + 8 * m0 * 10
+    t_iter = statistics.median(solve_ms) * 1e-3 / max(1, iters[-1])
+    achieved = b_iter / t_iter / 1e9
+    del H
+    return {"bound": "hbm", "bytes_per_iteration": int(b_iter), "us_per_iteration": t_iter * 1e6,
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak}
+
+
 def run_ours(args, d):
     import torch
 
@@ -435,6 +465,7 @@ def run_ours(args, d):
     d2h = 8 * m
 
     roof = dominant_kernel_roofline(core, dA, m, nnz, torch, profiled=args.n == 128)
+    pcg_roof = pcg_iteration_roofline(core, dA, solves, iters, roof["peak"])
 
     if d.rank == 0:
         cpu = None
@@ -454,6 +485,7 @@ def run_ours(args, d):
             "e2e": {"value": d.world * args.steps / e2e_t, "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "roofline": roof,
+            "pcg_iteration_roofline": pcg_roof,
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": int(launches),
