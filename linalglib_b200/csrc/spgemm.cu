@@ -364,10 +364,12 @@ namespace lab
     constexpr int kHashACap    = 64; // A entries staged per piece
     constexpr int kHashU       = 4;  // products in flight per lane
     constexpr int kHashClasses = 8;
+    static_assert(kHashU == 4, "the chunk's slot map is one int4 per lane");
 
     template <int MODE, int HS>
-    struct hash_smem
+    struct alignas(16) hash_smem
     {
+        int      jmap[32 * kHashU]; // A entry of each product slot of the current chunk
         int      key[HS];
         double   val[MODE == 1 ? HS : 1];
         uint64_t sk[MODE == 1 ? HS / 2 : 1];
@@ -469,8 +471,49 @@ namespace lab
                 sm.aoff[lane]      = inc0 - len[0];
                 sm.aoff[lane + 32] = tot0 + inc1 - len[1];
                 __syncwarp();
+                int jcarry = 0; // A entry of the product just before the chunk
                 for(int t0 = 0; t0 < T && !ovf; t0 += 32 * kHashU)
                 {
+                    // Map the chunk's product slots t0 .. t0 + 127 to their A entries
+                    // (the largest j with aoff[j] <= t): each non-empty A entry marks the
+                    // slot where its products start, then an inclusive max-scan over the
+                    // slots (lane k owns slots 4k .. 4k + 3) fills the rest.
+                    reinterpret_cast<int4*>(sm.jmap)[lane] = make_int4(-1, -1, -1, -1);
+                    __syncwarp();
+#pragma unroll
+                    for(int h = 0; h < 2; h++)
+                    {
+                        const int j = lane + 32 * h;
+                        if(j < nA)
+                        {
+                            const int o   = sm.aoff[j];
+                            const int nxt = j + 1 < nA ? sm.aoff[j + 1] : T;
+                            if(nxt > o && o >= t0 && o < t0 + 32 * kHashU)
+                                sm.jmap[o - t0] = j;
+                        }
+                    }
+                    __syncwarp();
+                    int4 q4 = reinterpret_cast<const int4*>(sm.jmap)[lane];
+                    q4.y    = max(q4.x, q4.y);
+                    q4.z    = max(q4.y, q4.z);
+                    q4.w    = max(q4.z, q4.w);
+                    int run = q4.w;
+#pragma unroll
+                    for(int o = 1; o < 32; o <<= 1)
+                    {
+                        const int t = __shfl_up_sync(full, run, o);
+                        if(lane >= o)
+                            run = max(run, t);
+                    }
+                    int before = __shfl_up_sync(full, run, 1);
+                    before     = lane == 0 ? jcarry : max(jcarry, before);
+                    q4.x       = max(before, q4.x);
+                    q4.y       = max(before, q4.y);
+                    q4.z       = max(before, q4.z);
+                    q4.w       = max(before, q4.w);
+                    reinterpret_cast<int4*>(sm.jmap)[lane] = q4;
+                    jcarry = __shfl_sync(full, q4.w, 31);
+                    __syncwarp();
                     int    c[kHashU];
                     int    jj[kHashU];
                     double bv[kHashU];
@@ -483,18 +526,9 @@ namespace lab
                         bv[u]       = 0.0;
                         if(t < T)
                         {
-                            // the A entry j with aoff[j] <= t < aoff[j] + len_j
-                            int lo = 0, hi = nA - 1;
-                            while(lo < hi)
-                            {
-                                const int mid = (lo + hi + 1) >> 1;
-                                if(sm.aoff[mid] <= t)
-                                    lo = mid;
-                                else
-                                    hi = mid - 1;
-                            }
-                            const int p = sm.ab0[lo] + (t - sm.aoff[lo]);
-                            jj[u]       = lo;
+                            const int j = sm.jmap[32 * u + lane];
+                            const int p = sm.ab0[j] + (t - sm.aoff[j]);
+                            jj[u]       = j;
                             c[u]        = __ldg(B.ci + p);
                             if(MODE == 1)
                                 bv[u] = __ldg(B.v + p);
