@@ -618,8 +618,8 @@ namespace lab
     }
 
     // Row classes.  Symbolic (by the product bound ub): 0 = lane tier (ub <= 32),
-    // 1..6 = hash tables of 128..4096 slots (ub <= slots / 2; class 6 takes every
-    // larger row and checks for overflow).  Numeric (by the exact column count of
+    // 1..4 = hash tables of 128..1024 slots (ub <= slots / 2; class 4 takes every
+    // larger row and checks for overflow, and its overflow rows get 4096 slots).  Numeric (by the exact column count of
     // rows with ub > 32): 1..6 = tables of 64..2048 slots (count <= slots / 2),
     // 7 = global sort tier.
     __device__ __forceinline__ int gemm_class(int phase, int ub, int cnt)
@@ -628,8 +628,11 @@ namespace lab
             return 0;
         if(phase == 0)
         {
+            // the bound is loose for Galerkin products (many products per column):
+            // rows bounded above 512 start in the 1024-slot table and only the ones
+            // that fill it are retried with 4096 slots (then the global sort tier)
             int c = 1, hs = 128;
-            while(c < 6 && 2 * ub > hs)
+            while(c < 4 && 2 * ub > hs)
             {
                 c++;
                 hs <<= 1;
@@ -763,8 +766,6 @@ namespace lab
             LAB_HASH_CLS(2, 256, 8);
             LAB_HASH_CLS(3, 512, 8);
             LAB_HASH_CLS(4, 1024, 8);
-            LAB_HASH_CLS(5, 2048, 8);
-            LAB_HASH_CLS(6, 4096, 4);
         }
         else
         {
@@ -855,12 +856,12 @@ namespace lab
         // ---- symbolic: lane tier (<= 32 products), hash classes, overflow -> global sort
         gemm_classes gs;
         LAB_TRY(gemm_classify(0, upper.get(), nullptr, m, gs, s));
-        dbuf<int32_t> counts, ovf_rows, rp;
+        dbuf<int32_t> counts, ovf_rows, ovf2_rows, rp;
         dbuf<int>     novf_d;
         LAB_TRY(counts.alloc((size_t)m + 1, s));
-        LAB_TRY(ovf_rows.alloc((size_t)std::max(gs.count(6), 1), s));
-        LAB_TRY(novf_d.alloc(1, s));
-        LAB_CUDA(cudaMemsetAsync(novf_d.get(), 0, sizeof(int), s));
+        LAB_TRY(ovf_rows.alloc((size_t)std::max(gs.count(4), 1), s));
+        LAB_TRY(novf_d.alloc(2, s));
+        LAB_CUDA(cudaMemsetAsync(novf_d.get(), 0, 2 * sizeof(int), s));
         LAB_CUDA(cudaMemsetAsync(counts.get(), 0, sizeof(int32_t) * (m + 1), s));
         esc_tiers tl;
         LAB_TRY(lane_tiers(gs, tl, s));
@@ -868,13 +869,23 @@ namespace lab
         LAB_TRY(launch_hash_classes<0>(gs, Ar, Br, counts.get(), nullptr, nullptr, nullptr,
                                        ovf_rows.get(), novf_d.get(), s));
         int novf = 0;
-        if(gs.count(6))
+        if(gs.count(4))
             LAB_TRY(copy_d2h_sync(&novf, novf_d.get(), sizeof(int), s));
         if(novf)
         {
-            esc_tiers tg;
-            LAB_TRY(tiers_for_rows(ovf_rows.get(), novf, upper.get(), tg, s));
-            LAB_TRY((esc_run<exp_gemm, 0>(e, m, tg, counts.get(), nullptr, nullptr, s)));
+            // rows that filled 3/4 of the 1024-slot table: 4096 slots, then global sort
+            LAB_TRY(ovf2_rows.alloc((size_t)novf, s));
+            LAB_TRY((launch_hash_cls<0, 4096, 4>(Ar, Br, ovf_rows.get(), novf, counts.get(), nullptr,
+                                                 nullptr, nullptr, ovf2_rows.get(),
+                                                 novf_d.get() + 1, s)));
+            int novf2 = 0;
+            LAB_TRY(copy_d2h_sync(&novf2, novf_d.get() + 1, sizeof(int), s));
+            if(novf2)
+            {
+                esc_tiers tg;
+                LAB_TRY(tiers_for_rows(ovf2_rows.get(), novf2, upper.get(), tg, s));
+                LAB_TRY((esc_run<exp_gemm, 0>(e, m, tg, counts.get(), nullptr, nullptr, s)));
+            }
         }
 
         // ---- row pointer and allocation
