@@ -439,14 +439,48 @@ namespace lab
         {
             __shared__ int s_pref[32];
             const int      a0 = rp[row], a1 = rp[row + 1];
-            // saamg.cpp:145-163, sequential in CSR order (every thread computes it)
+            // saamg.cpp:145-163: the diagonal plus the weak entries' negated values,
+            // summed in CSR order.  A warp loads 32 entries at once and every lane
+            // runs the same ordered chain over the contributing ones (shuffles);
+            // larger groups sum sequentially (every thread computes it).
             double dg = 0.0;
-            for(int j = a0; j < a1; j++)
+            if constexpr(G::size == 32)
             {
-                if(ci[j] == row)
-                    dg = __dadd_rn(dg, v[j]);
-                else if(conn[j] == 0)
-                    dg = __dsub_rn(dg, v[j]);
+                const unsigned full = 0xffffffffu;
+                const int      lane = G::rank();
+                for(int base = a0; base < a1; base += 32)
+                {
+                    const int j    = base + lane;
+                    double    t    = 0.0;
+                    bool      add  = false, sub = false;
+                    if(j < a1)
+                    {
+                        const int c = ci[j];
+                        add         = c == row;
+                        sub         = !add && conn[j] == 0;
+                        if(add || sub)
+                            t = v[j];
+                    }
+                    unsigned       mask = __ballot_sync(full, add || sub);
+                    const unsigned subs = __ballot_sync(full, sub);
+                    while(mask)
+                    {
+                        const int    l = __ffs(mask) - 1;
+                        const double x = __shfl_sync(full, t, l);
+                        dg             = ((subs >> l) & 1u) ? __dsub_rn(dg, x) : __dadd_rn(dg, x);
+                        mask &= mask - 1u;
+                    }
+                }
+            }
+            else
+            {
+                for(int j = a0; j < a1; j++)
+                {
+                    if(ci[j] == row)
+                        dg = __dadd_rn(dg, v[j]);
+                    else if(conn[j] == 0)
+                        dg = __dsub_rn(dg, v[j]);
+                }
             }
             const double inv  = __ddiv_rn(1.0, dg);
             const double coef = __dmul_rn(-relax, inv);
