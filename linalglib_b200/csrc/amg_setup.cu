@@ -32,30 +32,13 @@ namespace lab
         }
     }
 
-    __global__ void k_diag_only(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                const double* __restrict__ v, int64_t m, double* __restrict__ d)
-    {
-        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-        if(i >= m)
-            return;
-        double dd = 0.0;
-        for(int j = rp[i]; j < rp[i + 1]; j++)
-            if(ci[j] == i)
-            {
-                dd = v[j];
-                break;
-            }
-        d[i] = dd;
-    }
-
     lab_status amg_strength(const lab_csr_impl* A, double eps, int32_t* conn, cudaStream_t s)
     {
         if(A->m == 0)
             return LAB_OK;
         dbuf<double> d;
         LAB_TRY(d.alloc((size_t)A->m, s));
-        LAB_LAUNCH(k_diag_only, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, s, A->row_ptr,
-                   A->col_ind, A->val, A->m, d.get());
+        LAB_TRY(diag_into(A, d.get(), nullptr, s));
         double avg = (double)A->nnz / (double)A->m;
         if(avg <= 12.0)
             LAB_LAUNCH(k_strength<1>, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, s,
@@ -92,6 +75,28 @@ namespace lab
                 break;
             }
         state[i] = s;
+        hash[i]  = (int32_t)pmis_hash((unsigned int)i);
+        agg[i]   = 0;
+    }
+
+    // k_pmis_init with a warp per row (long rows): any strong entry makes the
+    // state 0 (the reference stops at the first one; the result is the same).
+    __global__ void k_pmis_init_warp(const int32_t* __restrict__ rp,
+                                     const int32_t* __restrict__ conn, int64_t m,
+                                     int32_t* __restrict__ state, int32_t* __restrict__ hash,
+                                     int64_t* __restrict__ agg)
+    {
+        const int64_t i    = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        const int     lane = threadIdx.x & 31;
+        if(i >= m)
+            return;
+        bool strong = false;
+        for(int j = rp[i] + lane; j < rp[i + 1] && !strong; j += 32)
+            strong = conn[j] == 1;
+        strong = __any_sync(0xffffffffu, strong);
+        if(lane != 0)
+            return;
+        state[i] = strong ? 0 : -2;
         hash[i]  = (int32_t)pmis_hash((unsigned int)i);
         agg[i]   = 0;
     }
@@ -378,12 +383,17 @@ namespace lab
         LAB_TRY(flags.alloc(24, s));
         LAB_CUDA(cudaMemsetAsync(flags.get(), 0, sizeof(int32_t) * 24, s));
         const unsigned g = (unsigned)ceil_div<int64_t>(m, 256);
-        LAB_LAUNCH(k_pmis_init, g, 256, 0, s, A->row_ptr, conn, m, state.get(), hash.get(), agg);
+        const bool     wide = A->nnz > 12 * m;
+        const unsigned gw   = (unsigned)ceil_div<int64_t>(m * 32, 256);
+        if(wide)
+            LAB_LAUNCH(k_pmis_init_warp, gw, 256, 0, s, A->row_ptr, conn, m, state.get(),
+                       hash.get(), agg);
+        else
+            LAB_LAUNCH(k_pmis_init, g, 256, 0, s, A->row_ptr, conn, m, state.get(), hash.get(),
+                       agg);
         // ping-pong: round r reads buffer r & 1 of {state, snap} and writes the other
         int32_t* buf[2] = {state.get(), snap.get()};
         // long rows (coarse levels): a warp per row
-        const bool     wide = A->nnz > 12 * m;
-        const unsigned gw   = (unsigned)ceil_div<int64_t>(m * 32, 256);
         for(int r = 0; r < 20; r++)
         {
             if(wide)

@@ -130,6 +130,76 @@ namespace lab
         return LAB_OK;
     }
 
+    // ------------------------------------------------------------ stream fork
+    static cudaStream_t* side_pool()
+    {
+        static cudaStream_t pool[8] = {};
+        static bool         ok      = [] {
+            for(auto& x : pool)
+                if(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking) != cudaSuccess)
+                {
+                    cudaGetLastError();
+                    return false;
+                }
+            return true;
+        }();
+        return ok ? pool : nullptr;
+    }
+
+    cudaStream_t stream_fork::next()
+    {
+        const int k = used_++;
+        if(k == 0 || !on_)
+            return s_;
+        cudaStream_t* pool = side_pool();
+        if(!pool || k > kSides)
+            return s_; // serial fallback
+        if(!fork_)
+        {
+            if(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming) != cudaSuccess ||
+               cudaEventRecord(fork_, s_) != cudaSuccess)
+            {
+                cudaGetLastError();
+                if(fork_)
+                    cudaEventDestroy(fork_);
+                fork_ = nullptr;
+                used_ = kSides + 1; // everything else on s_
+                return s_;
+            }
+        }
+        cudaStream_t side = pool[k - 1];
+        if(cudaEventCreateWithFlags(&done_[k - 1], cudaEventDisableTiming) != cudaSuccess)
+        {
+            cudaGetLastError();
+            done_[k - 1] = nullptr;
+            return s_;
+        }
+        if(cudaStreamWaitEvent(side, fork_, 0) != cudaSuccess)
+        {
+            cudaGetLastError();
+            cudaEventDestroy(done_[k - 1]);
+            done_[k - 1] = nullptr;
+            return s_;
+        }
+        return side;
+    }
+
+    stream_fork::~stream_fork()
+    {
+        cudaStream_t* pool = side_pool();
+        for(int k = 0; k < kSides; k++)
+            if(done_[k])
+            {
+                if(pool && cudaEventRecord(done_[k], pool[k]) == cudaSuccess)
+                    cudaStreamWaitEvent(s_, done_[k], 0);
+                else
+                    cudaStreamSynchronize(pool ? pool[k] : s_);
+                cudaEventDestroy(done_[k]);
+            }
+        if(fork_)
+            cudaEventDestroy(fork_);
+    }
+
     // ------------------------------------------------------------ CSR containers
     lab_status csr_alloc(lab_csr_impl** out, int64_t m, int64_t n, int64_t nnz, cudaStream_t s)
     {
@@ -247,16 +317,55 @@ namespace lab
             invd[i] = 1.0 / dd;
     }
 
+    // Warp per row for long rows: the first diagonal entry in CSR order is the
+    // lowest lane of the first 32-entry window that holds one.
+    __global__ void k_diag_warp(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                const double* __restrict__ v, int64_t m, double* __restrict__ d,
+                                double* __restrict__ invd)
+    {
+        const int64_t i    = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        const int     lane = threadIdx.x & 31;
+        if(i >= m)
+            return;
+        double dd = 0.0;
+        for(int base = rp[i]; base < rp[i + 1]; base += 32)
+        {
+            const int      j   = base + lane;
+            const unsigned hit = __ballot_sync(0xffffffffu, j < rp[i + 1] && ci[j] == i);
+            if(hit)
+            {
+                dd = v[base + __ffs(hit) - 1];
+                break;
+            }
+        }
+        if(lane != 0)
+            return;
+        if(d)
+            d[i] = dd;
+        if(invd)
+            invd[i] = 1.0 / dd;
+    }
+
+    lab_status diag_into(const lab_csr_impl* A, double* d, double* invd, cudaStream_t s)
+    {
+        if(A->m == 0)
+            return LAB_OK;
+        if(A->nnz > 12 * A->m)
+            LAB_LAUNCH(k_diag_warp, (unsigned)ceil_div<int64_t>(A->m * 32, 256), 256, 0, s,
+                       A->row_ptr, A->col_ind, (const double*)A->val, A->m, d, invd);
+        else
+            LAB_LAUNCH(k_diag, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, s, A->row_ptr,
+                       A->col_ind, (const double*)A->val, A->m, d, invd);
+        return LAB_OK;
+    }
+
     lab_status csr_ensure_invdiag(lab_csr_impl* A, cudaStream_t s)
     {
         if(A->invdiag)
             return LAB_OK;
         LAB_TRY(dalloc(&A->diag, (size_t)A->m + 1, s));
         LAB_TRY(dalloc(&A->invdiag, (size_t)A->m + 1, s));
-        if(A->m > 0)
-            LAB_LAUNCH(k_diag, ceil_div<int64_t>(A->m, 256), 256, 0, s, A->row_ptr, A->col_ind,
-                       A->val, A->m, A->diag, A->invdiag);
-        return LAB_OK;
+        return diag_into(A, A->diag, A->invdiag, s);
     }
 
     // ------------------------------------------------------------ reductions
@@ -882,9 +991,7 @@ LAB_API lab_status lab_diagonal(lab_csr A, double* d, lab_stream s)
     LAB_ARG(A && d, "null argument");
     if(A->m == 0)
         return LAB_OK;
-    LAB_LAUNCH(k_diag, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, to_stream(s), A->row_ptr,
-               A->col_ind, A->val, A->m, d, (double*)nullptr);
-    return LAB_OK;
+    return diag_into(A, d, nullptr, to_stream(s));
 }
 
 LAB_API lab_status lab_jacobi_solve(int64_t n, const double* r, const double* d, double* x,

@@ -353,11 +353,12 @@ namespace lab
     lab_status esc_run(const Exp& e, int64_t m, esc_tiers& t, int32_t* counts, int32_t* out_col,
                        double* out_val, cudaStream_t s)
     {
+        stream_fork f(s, m); // the tiers are disjoint row sets: they run side by side
         if(t.nl > 0)
         {
             unsigned grid = (unsigned)std::min<int64_t>(
                 ceil_div<int64_t>(t.nl, 32 * kEscLaneWarps), (int64_t)num_sms() * 16);
-            LAB_LAUNCH((k_esc_lane<Exp, MODE>), grid, 32 * kEscLaneWarps, 0, s, e, t.rows.get(),
+            LAB_LAUNCH((k_esc_lane<Exp, MODE>), grid, 32 * kEscLaneWarps, 0, f.next(), e, t.rows.get(),
                        t.nl, counts, out_col, out_val);
         }
         const int32_t* wrows = t.rows.get() + t.nl;
@@ -365,7 +366,7 @@ namespace lab
         {
             unsigned grid = (unsigned)std::min<int64_t>(
                 ceil_div<int64_t>(t.nw, kEscWarpsPerCta), (int64_t)num_sms() * 8);
-            LAB_LAUNCH((k_esc_warp<Exp, MODE>), grid, 32 * kEscWarpsPerCta, 0, s, e, wrows, t.nw,
+            LAB_LAUNCH((k_esc_warp<Exp, MODE>), grid, 32 * kEscWarpsPerCta, 0, f.next(), e, wrows, t.nw,
                        counts, out_col, out_val);
         }
         if(t.nb > 0)
@@ -375,13 +376,13 @@ namespace lab
                 k_esc_cta<Exp, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             LAB_CUDA(attr);
             unsigned grid = (unsigned)std::min<int64_t>(t.nb, (int64_t)num_sms() * 3);
-            LAB_LAUNCH((k_esc_cta<Exp, MODE>), grid, kEscCtaNT, smem, s, e, wrows + t.nw, t.nb,
+            LAB_LAUNCH((k_esc_cta<Exp, MODE>), grid, kEscCtaNT, smem, f.next(), e, wrows + t.nw, t.nb,
                        counts, out_col, out_val);
         }
         if(t.ng > 0)
         {
             unsigned grid = (unsigned)std::min<int64_t>(t.ng, (int64_t)num_sms() * 2);
-            LAB_LAUNCH((k_esc_big<Exp, MODE>), grid, kEscBigNT, 0, s, e, wrows + t.nw + t.nb,
+            LAB_LAUNCH((k_esc_big<Exp, MODE>), grid, kEscBigNT, 0, f.next(), e, wrows + t.nw + t.nb,
                        t.ng, t.g_offsets.get(), t.g_keys.get(), t.g_vals.get(), counts, out_col,
                        out_val);
         }

@@ -175,6 +175,34 @@ namespace lab
         upper[i] = (int32_t)u;
     }
 
+    // Warp-per-row form for long A rows (coarse levels): the lanes take strided
+    // entries and the 64-bit sum is reduced by shuffles (integer: exact).
+    __global__ void k_gemm_upper_warp(csr_ref A, const int32_t* __restrict__ Brp, int64_t m,
+                                      int32_t* upper, int* overflow)
+    {
+        const int64_t i    = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        const int     lane = threadIdx.x & 31;
+        if(i >= m)
+            return;
+        long long u = 0;
+        for(int j = A.rp[i] + lane; j < A.rp[i + 1]; j += 32)
+        {
+            const int k = A.ci[j];
+            u += Brp[k + 1] - Brp[k];
+        }
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            u += __shfl_xor_sync(0xffffffffu, u, o);
+        if(lane != 0)
+            return;
+        if(u > (1 << 30))
+        {
+            atomicOr(overflow, 1);
+            u = 0;
+        }
+        upper[i] = (int32_t)u;
+    }
+
     // C = alpha*A + beta*B: A's entries then B's (host_csrgeam.cpp).
     struct exp_geam
     {
@@ -755,11 +783,13 @@ namespace lab
     static lab_status launch_hash_classes(const gemm_classes& g, csr_ref Ar, csr_ref Br,
                                           int32_t* counts, const int32_t* out_rp, int32_t* out_ci,
                                           double* out_v, int32_t* ovf_rows, int* n_ovf,
-                                          cudaStream_t s)
+                                          stream_fork& f)
     {
+        // the classes are independent row sets: they run side by side
 #define LAB_HASH_CLS(C, HS, W)                                                                    \
-    LAB_TRY((launch_hash_cls<MODE, HS, W>(Ar, Br, g.of(C), g.count(C), counts, out_rp, out_ci,    \
-                                          out_v, ovf_rows, n_ovf, s)))
+    if(g.count(C))                                                                                \
+        LAB_TRY((launch_hash_cls<MODE, HS, W>(Ar, Br, g.of(C), g.count(C), counts, out_rp, out_ci,\
+                                              out_v, ovf_rows, n_ovf, f.next())))
         if constexpr(MODE == 0)
         {
             LAB_HASH_CLS(1, 128, 8);
@@ -838,7 +868,10 @@ namespace lab
         LAB_TRY(ovf.alloc(1, s));
         LAB_CUDA(cudaMemsetAsync(ovf.get(), 0, sizeof(int), s));
         csr_ref Ar{A->row_ptr, A->col_ind, A->val}, Br{B->row_ptr, B->col_ind, B->val};
-        if(A->m > 0)
+        if(A->m > 0 && A->nnz > 12 * A->m)
+            LAB_LAUNCH(k_gemm_upper_warp, (unsigned)ceil_div<int64_t>(A->m * 32, 256), 256, 0, s,
+                       Ar, B->row_ptr, A->m, upper.get(), ovf.get());
+        else if(A->m > 0)
             LAB_LAUNCH(k_gemm_upper, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, s, Ar,
                        B->row_ptr, A->m, upper.get(), ovf.get());
         int h = 0;
@@ -865,9 +898,12 @@ namespace lab
         LAB_CUDA(cudaMemsetAsync(counts.get(), 0, sizeof(int32_t) * (m + 1), s));
         esc_tiers tl;
         LAB_TRY(lane_tiers(gs, tl, s));
-        LAB_TRY((esc_run<exp_gemm, 0>(e, m, tl, counts.get(), nullptr, nullptr, s)));
-        LAB_TRY(launch_hash_classes<0>(gs, Ar, Br, counts.get(), nullptr, nullptr, nullptr,
-                                       ovf_rows.get(), novf_d.get(), s));
+        {
+            stream_fork f(s, m); // lane tier and hash classes side by side
+            LAB_TRY((esc_run<exp_gemm, 0>(e, m, tl, counts.get(), nullptr, nullptr, f.next())));
+            LAB_TRY(launch_hash_classes<0>(gs, Ar, Br, counts.get(), nullptr, nullptr, nullptr,
+                                           ovf_rows.get(), novf_d.get(), f));
+        }
         int novf = 0;
         if(gs.count(4))
             LAB_TRY(copy_d2h_sync(&novf, novf_d.get(), sizeof(int), s));
@@ -904,12 +940,15 @@ namespace lab
         e2.out_rp   = out->row_ptr;
         gemm_classes gn;
         if(st == LAB_OK)
-            st = esc_run<exp_gemm, 1>(e2, m, tl, nullptr, out->col_ind, out->val, s);
-        if(st == LAB_OK)
             st = gemm_classify(1, upper.get(), out->row_ptr, m, gn, s);
         if(st == LAB_OK)
-            st = launch_hash_classes<1>(gn, Ar, Br, nullptr, out->row_ptr, out->col_ind, out->val,
-                                        nullptr, nullptr, s);
+        {
+            stream_fork f(s, m); // lane tier and hash classes side by side
+            st = esc_run<exp_gemm, 1>(e2, m, tl, nullptr, out->col_ind, out->val, f.next());
+            if(st == LAB_OK)
+                st = launch_hash_classes<1>(gn, Ar, Br, nullptr, out->row_ptr, out->col_ind,
+                                            out->val, nullptr, nullptr, f);
+        }
         if(st == LAB_OK && gn.count(7))
         {
             esc_tiers tg;
