@@ -69,7 +69,7 @@ namespace lab
             return;
         int s = -2;
         for(int j = rp[i]; j < rp[i + 1]; j++)
-            if(conn[j] == 1)
+            if(!conn || conn[j] == 1)
             {
                 s = 0;
                 break;
@@ -92,7 +92,7 @@ namespace lab
             return;
         bool strong = false;
         for(int j = rp[i] + lane; j < rp[i + 1] && !strong; j += 32)
-            strong = conn[j] == 1;
+            strong = !conn || conn[j] == 1;
         strong = __any_sync(0xffffffffu, strong);
         if(lane != 0)
             return;
@@ -129,7 +129,7 @@ namespace lab
         int bs = st[i], bh = hash[i], br = (int)i;
         for(int j = rp[i]; j < rp[i + 1]; j++)
         {
-            if(conn[j] != 1)
+            if(conn && conn[j] != 1)
                 continue;
             int c = ci[j], cs = st[c], chh = hash[c];
             if(cs > bs || (cs == bs && chh > bh))
@@ -142,7 +142,7 @@ namespace lab
         const int r = br;
         for(int j = rp[r]; j < rp[r + 1]; j++)
         {
-            if(conn[j] != 1)
+            if(conn && conn[j] != 1)
                 continue;
             int c = ci[j], cs = st[c], chh = hash[c];
             if(cs > bs || (cs == bs && chh > bh))
@@ -215,7 +215,7 @@ namespace lab
         const int a = rp[r], b = rp[r + 1];
         for(int j = a + lane; j < b; j += 32)
         {
-            if(conn[j] != 1)
+            if(conn && conn[j] != 1)
                 continue;
             const int c = ci[j];
             pmis_best w{st[c], hash[c], j - a, c};
@@ -296,7 +296,7 @@ namespace lab
         {
             for(int j = rp[i]; j < rp[i + 1]; j++)
             {
-                if(conn[j] == 1 && st[ci[j]] == 1)
+                if((!conn || conn[j] == 1) && st[ci[j]] == 1)
                 {
                     agg[i] = agg[ci[j]];
                     s      = 1;
@@ -331,7 +331,7 @@ namespace lab
             for(int base = a; base < b; base += 32)
             {
                 const int      j   = base + lane;
-                const bool     hit = j < b && conn[j] == 1 && st[ci[j]] == 1;
+                const bool     hit = j < b && (!conn || conn[j] == 1) && st[ci[j]] == 1;
                 const unsigned bal = __ballot_sync(0xffffffffu, hit);
                 if(bal)
                 {
@@ -365,6 +365,47 @@ namespace lab
             roots[i] = agg[i] == 1 ? 1 : -1;
     }
 
+    // Strong-neighbour lists of long rows (coarse SA levels keep only 10-20 % of
+    // their entries strong): the PMIS passes then scan the strong columns alone,
+    // in CSR order (the scans' tie rules depend on that order only).
+    __global__ void k_strong_count(const int32_t* __restrict__ rp,
+                                   const int32_t* __restrict__ conn, int64_t m,
+                                   int32_t* __restrict__ cnt)
+    {
+        const int64_t i    = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        const int     lane = threadIdx.x & 31;
+        if(i >= m)
+            return;
+        int c = 0;
+        for(int j = rp[i] + lane; j < rp[i + 1]; j += 32)
+            c += conn[j] == 1;
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            c += __shfl_xor_sync(0xffffffffu, c, o);
+        if(lane == 0)
+            cnt[i] = c;
+    }
+
+    __global__ void k_strong_fill(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                  const int32_t* __restrict__ conn, int64_t m,
+                                  const int32_t* __restrict__ srp, int32_t* __restrict__ sci)
+    {
+        const int64_t i    = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        const int     lane = threadIdx.x & 31;
+        if(i >= m)
+            return;
+        int o = srp[i];
+        for(int base = rp[i]; base < rp[i + 1]; base += 32)
+        {
+            const int      j   = base + lane;
+            const bool     st  = j < rp[i + 1] && conn[j] == 1;
+            const unsigned bal = __ballot_sync(0xffffffffu, st);
+            if(st)
+                sci[o + __popc(bal & ((1u << lane) - 1u))] = ci[j];
+            o += __popc(bal);
+        }
+    }
+
     // compute_aggregates_using_pmis (amg_aggregation.cpp:106-215)
     lab_status amg_pmis(const lab_csr_impl* A, const int32_t* conn, int64_t* agg, int* rounds,
                         cudaStream_t s, int64_t* roots = nullptr)
@@ -376,6 +417,26 @@ namespace lab
                 *rounds = 0;
             return LAB_OK;
         }
+        // the passes read (prp, pci, pconn): A with its conn flags, or, for long
+        // rows, the strong-neighbour lists (pconn = null: every entry strong)
+        const int32_t* prp   = A->row_ptr;
+        const int32_t* pci   = A->col_ind;
+        const int32_t* pconn = conn;
+        int64_t        pnnz  = A->nnz;
+        dbuf<int32_t>  srp, sci;
+        if(conn && A->nnz > 12 * m)
+        {
+            const unsigned gw = (unsigned)ceil_div<int64_t>(m * 32, 256);
+            LAB_TRY(srp.alloc((size_t)m + 1, s));
+            LAB_TRY(sci.alloc((size_t)std::max<int64_t>(A->nnz, 1), s));
+            LAB_LAUNCH(k_strong_count, gw, 256, 0, s, A->row_ptr, conn, m, srp.get());
+            LAB_TRY(counts_to_rowptr(srp.get(), srp.get(), m, &pnnz, s));
+            LAB_LAUNCH(k_strong_fill, gw, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                       (const int32_t*)srp.get(), sci.get());
+            prp   = srp.get();
+            pci   = sci.get();
+            pconn = nullptr;
+        }
         dbuf<int32_t> state, snap, hash, flags;
         LAB_TRY(state.alloc((size_t)m, s));
         LAB_TRY(snap.alloc((size_t)m, s));
@@ -383,13 +444,13 @@ namespace lab
         LAB_TRY(flags.alloc(24, s));
         LAB_CUDA(cudaMemsetAsync(flags.get(), 0, sizeof(int32_t) * 24, s));
         const unsigned g = (unsigned)ceil_div<int64_t>(m, 256);
-        const bool     wide = A->nnz > 12 * m;
+        const bool     wide = pnnz > 12 * m;
         const unsigned gw   = (unsigned)ceil_div<int64_t>(m * 32, 256);
         if(wide)
-            LAB_LAUNCH(k_pmis_init_warp, gw, 256, 0, s, A->row_ptr, conn, m, state.get(),
+            LAB_LAUNCH(k_pmis_init_warp, gw, 256, 0, s, prp, pconn, m, state.get(),
                        hash.get(), agg);
         else
-            LAB_LAUNCH(k_pmis_init, g, 256, 0, s, A->row_ptr, conn, m, state.get(), hash.get(),
+            LAB_LAUNCH(k_pmis_init, g, 256, 0, s, prp, pconn, m, state.get(), hash.get(),
                        agg);
         // ping-pong: round r reads buffer r & 1 of {state, snap} and writes the other
         int32_t* buf[2] = {state.get(), snap.get()};
@@ -397,11 +458,11 @@ namespace lab
         for(int r = 0; r < 20; r++)
         {
             if(wide)
-                LAB_LAUNCH(k_pmis_round_warp, gw, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                LAB_LAUNCH(k_pmis_round_warp, gw, 256, 0, s, prp, pci, pconn, m,
                            (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg,
                            flags.get(), r);
             else
-                LAB_LAUNCH(k_pmis_round, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                LAB_LAUNCH(k_pmis_round, g, 256, 0, s, prp, pci, pconn, m,
                            (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg,
                            flags.get(), r);
         }
@@ -418,10 +479,10 @@ namespace lab
         for(int k = 0; k < 2; k++)
         {
             if(wide)
-                LAB_LAUNCH(k_pmis_attach_warp, gw, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                LAB_LAUNCH(k_pmis_attach_warp, gw, 256, 0, s, prp, pci, pconn, m,
                            state.get(), snap.get(), (const int32_t*)flags.get(), k, agg);
             else
-                LAB_LAUNCH(k_pmis_attach, g, 256, 0, s, A->row_ptr, A->col_ind, conn, m,
+                LAB_LAUNCH(k_pmis_attach, g, 256, 0, s, prp, pci, pconn, m,
                            state.get(), snap.get(), (const int32_t*)flags.get(), k, agg);
         }
         return LAB_OK;
