@@ -109,17 +109,15 @@ namespace lab
     // larger (state, hash), so the CSR scan order decides ties exactly as in the
     // reference (lines 77-93).
     // Rounds after the first complete one return at once (amg_aggregation.cpp:154).
-    __global__ void k_pmis_round(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                 const int32_t* __restrict__ conn, int64_t m,
-                                 const int32_t* __restrict__ st, const int32_t* __restrict__ hash,
-                                 int32_t* __restrict__ out, int64_t* __restrict__ agg,
-                                 int32_t* flags, int round)
+    __device__ __forceinline__ void pmis_round_row(int64_t i, const int32_t* __restrict__ rp,
+                                                   const int32_t* __restrict__ ci,
+                                                   const int32_t* __restrict__ conn,
+                                                   const int32_t* __restrict__ st,
+                                                   const int32_t* __restrict__ hash,
+                                                   int32_t* __restrict__ out,
+                                                   int64_t* __restrict__ agg, int32_t* flags,
+                                                   int round)
     {
-        if(round > 0 && flags[round - 1] == 0)
-            return;
-        int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-        if(i >= m)
-            return;
         if(st[i] != 0)
         {
             // decided rows keep their state; their scans would change nothing
@@ -169,6 +167,21 @@ namespace lab
                 flags[round] = 1;
         }
         out[i] = ns;
+    }
+
+    // Persistent grid (grid-stride): the 20 round launches are made unconditionally
+    // and the ones after convergence must cost next to nothing.
+    __global__ void k_pmis_round(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                 const int32_t* __restrict__ conn, int64_t m,
+                                 const int32_t* __restrict__ st, const int32_t* __restrict__ hash,
+                                 int32_t* __restrict__ out, int64_t* __restrict__ agg,
+                                 int32_t* flags, int round)
+    {
+        if(round > 0 && flags[round - 1] == 0)
+            return;
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+            i += (int64_t)gridDim.x * blockDim.x)
+            pmis_round_row(i, rp, ci, conn, st, hash, out, agg, flags, round);
     }
 
     // Warp-per-row form of k_pmis_round for long rows (coarse levels).  The
@@ -225,18 +238,12 @@ namespace lab
         return pmis_warp_max(v);
     }
 
-    __global__ void k_pmis_round_warp(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                      const int32_t* __restrict__ conn, int64_t m,
-                                      const int32_t* __restrict__ st,
-                                      const int32_t* __restrict__ hash, int32_t* __restrict__ out,
-                                      int64_t* __restrict__ agg, int32_t* flags, int round)
+    __device__ __forceinline__ void pmis_round_row_warp(
+        int64_t i, int lane, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+        const int32_t* __restrict__ conn, const int32_t* __restrict__ st,
+        const int32_t* __restrict__ hash, int32_t* __restrict__ out, int64_t* __restrict__ agg,
+        int32_t* flags, int round)
     {
-        if(round > 0 && flags[round - 1] == 0)
-            return;
-        const int64_t i    = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-        const int     lane = threadIdx.x & 31;
-        if(i >= m)
-            return;
         if(st[i] != 0)
         {
             if(lane == 0)
@@ -266,6 +273,20 @@ namespace lab
                 flags[round] = 1;
         }
         out[i] = ns;
+    }
+
+    __global__ void k_pmis_round_warp(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                      const int32_t* __restrict__ conn, int64_t m,
+                                      const int32_t* __restrict__ st,
+                                      const int32_t* __restrict__ hash, int32_t* __restrict__ out,
+                                      int64_t* __restrict__ agg, int32_t* flags, int round)
+    {
+        if(round > 0 && flags[round - 1] == 0)
+            return;
+        const int lane = threadIdx.x & 31;
+        for(int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < m;
+            i += ((int64_t)gridDim.x * blockDim.x) >> 5)
+            pmis_round_row_warp(i, lane, rp, ci, conn, st, hash, out, agg, flags, round);
     }
 
     // Rounds that ran: round r runs iff r == 0 or round r-1 left a row undecided.
@@ -458,11 +479,13 @@ namespace lab
         for(int r = 0; r < 20; r++)
         {
             if(wide)
-                LAB_LAUNCH(k_pmis_round_warp, gw, 256, 0, s, prp, pci, pconn, m,
+                LAB_LAUNCH(k_pmis_round_warp, std::min<unsigned>(gw, num_sms() * 8), 256, 0, s,
+                           prp, pci, pconn, m,
                            (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg,
                            flags.get(), r);
             else
-                LAB_LAUNCH(k_pmis_round, g, 256, 0, s, prp, pci, pconn, m,
+                LAB_LAUNCH(k_pmis_round, std::min<unsigned>(g, num_sms() * 8), 256, 0, s, prp, pci,
+                           pconn, m,
                            (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg,
                            flags.get(), r);
         }
