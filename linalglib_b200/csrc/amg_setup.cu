@@ -641,6 +641,128 @@ namespace lab
         }
     };
 
+    // Long rows (coarse levels): one warp per row computes the row's diagonal-plus-
+    // weak sum (saamg.cpp:145-163, in CSR order, as exp_sap::expand) and compacts
+    // the candidate entries (the diagonal and the strong ones, in CSR order) to the
+    // front of the row's slot range, so the expansion then walks ~10 candidates
+    // instead of the whole row.
+    __global__ void k_sap_prep(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                               const double* __restrict__ v, const int32_t* __restrict__ conn,
+                               int64_t m, int32_t* __restrict__ sci, double* __restrict__ sv,
+                               int32_t* __restrict__ cnt, double* __restrict__ dgs)
+    {
+        const int64_t  i    = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+        const int      lane = threadIdx.x & 31;
+        const unsigned full = 0xffffffffu;
+        if(i >= m)
+            return;
+        const int a0 = rp[i], a1 = rp[i + 1];
+        double    dg = 0.0;
+        int       o  = a0;
+        for(int base = a0; base < a1; base += 32)
+        {
+            const int j    = base + lane;
+            int       c    = -1, cn = 0;
+            double    x    = 0.0;
+            if(j < a1)
+            {
+                c  = ci[j];
+                cn = conn[j];
+                x  = v[j];
+            }
+            const bool     add  = j < a1 && c == i;
+            const bool     sub  = j < a1 && !add && cn == 0;
+            const bool     cand = j < a1 && (add || cn == 1);
+            unsigned       mask = __ballot_sync(full, add || sub);
+            const unsigned subs = __ballot_sync(full, sub);
+            while(mask)
+            {
+                const int    l = __ffs(mask) - 1;
+                const double t = __shfl_sync(full, x, l);
+                dg             = ((subs >> l) & 1u) ? __dsub_rn(dg, t) : __dadd_rn(dg, t);
+                mask &= mask - 1u;
+            }
+            const unsigned cb = __ballot_sync(full, cand);
+            if(cand)
+            {
+                const int q = o + __popc(cb & ((1u << lane) - 1u));
+                sci[q]      = c;
+                sv[q]       = x;
+            }
+            o += __popc(cb);
+        }
+        if(lane == 0)
+        {
+            cnt[i] = o - a0;
+            dgs[i] = dg;
+        }
+    }
+
+    // exp_sap over the compacted candidates of k_sap_prep (row r: slots
+    // rp[r] .. rp[r] + cnt[r]) with the precomputed diagonal sums.
+    struct exp_sap_c
+    {
+        const int32_t* rp;
+        const int32_t* cnt;
+        const int32_t* ci;
+        const double*  v;
+        const double*  dgs;
+        const int64_t* agg;
+        double         relax;
+        const int32_t* out_rp = nullptr;
+
+        template <class G>
+        __device__ int expand(int row, uint64_t* keys, double* vals) const
+        {
+            __shared__ int s_pref[32];
+            const int      a0   = rp[row], a1 = a0 + cnt[row];
+            const double   coef = __dmul_rn(-relax, __ddiv_rn(1.0, dgs[row]));
+            const double   dval = __dsub_rn(1.0, relax);
+            int            n    = 0;
+            for(int base = a0; base < a1; base += G::size)
+            {
+                const int j  = base + G::rank();
+                bool      q  = false;
+                int       c  = 0;
+                int64_t   ag = -1;
+                if(j < a1)
+                {
+                    c  = ci[j];
+                    ag = agg[c];
+                    q  = ag >= 0;
+                }
+                int tot;
+                int pos = n + group_prefix<G>(q, s_pref, tot);
+                if(q)
+                {
+                    keys[pos] = make_key((int)ag, pos);
+                    vals[pos] = (c == row) ? dval : __dmul_rn(coef, v[j]);
+                }
+                n += tot;
+            }
+            G::sync();
+            return n;
+        }
+        template <bool VALS, class F>
+        __device__ void emit_seq(int row, F&& f) const
+        {
+            const int    a0   = rp[row], a1 = a0 + cnt[row];
+            const double coef = VALS ? __dmul_rn(-relax, __ddiv_rn(1.0, dgs[row])) : 0.0;
+            const double dval = __dsub_rn(1.0, relax);
+            for(int j = a0; j < a1; j++)
+            {
+                const int     c  = ci[j];
+                const int64_t ag = agg[c];
+                if(ag >= 0)
+                    f((int)ag, VALS ? ((c == row) ? dval : __dmul_rn(coef, v[j])) : 0.0);
+            }
+        }
+        __device__ int32_t out_start(int row) const
+        {
+            return out_rp[row];
+        }
+    };
+
     lab_status amg_sa_prolongation(const lab_csr_impl* A, const int32_t* conn, const int64_t* agg,
                                    double relax, lab_csr_impl** P, cudaStream_t s)
     {
@@ -648,6 +770,20 @@ namespace lab
         if(A->m > 0)
             LAB_TRY(max_i64(agg, A->m, &mx, s));
         int64_t nc = (mx > -1 ? mx : -1) + 1; // saamg.cpp:68-76
+        if(A->m > 0 && A->nnz > 12 * A->m)
+        {
+            dbuf<int32_t> cnt, sci;
+            dbuf<double>  sv, dgs;
+            LAB_TRY(cnt.alloc((size_t)A->m + 1, s));
+            LAB_TRY(sci.alloc((size_t)A->nnz, s));
+            LAB_TRY(sv.alloc((size_t)A->nnz, s));
+            LAB_TRY(dgs.alloc((size_t)A->m, s));
+            LAB_LAUNCH(k_sap_prep, (unsigned)ceil_div<int64_t>(A->m * 32, 256), 256, 0, s,
+                       A->row_ptr, A->col_ind, (const double*)A->val, conn, A->m, sci.get(),
+                       sv.get(), cnt.get(), dgs.get());
+            exp_sap_c e{A->row_ptr, cnt.get(), sci.get(), sv.get(), dgs.get(), agg, relax};
+            return esc_build(e, cnt.get(), A->m, nc, P, s);
+        }
         dbuf<int32_t> upper;
         LAB_TRY(upper.alloc((size_t)A->m + 1, s));
         LAB_TRY(row_lengths(A->row_ptr, A->m, upper.get(), s));
