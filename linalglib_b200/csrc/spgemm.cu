@@ -141,12 +141,45 @@ namespace lab
         template <bool VALS, class F>
         __device__ void emit_seq(int row, F&& f) const
         {
-            for(int j = A.rp[row]; j < A.rp[row + 1]; j++)
+            // canonical order (A entry, then B entry); the loads of four A entries,
+            // their B-row bounds and four B entries at a time are issued together
+            const int a0 = A.rp[row], a1 = A.rp[row + 1];
+            for(int j0 = a0; j0 < a1; j0 += 4)
             {
-                const int    k = A.ci[j];
-                const double a = VALS ? A.v[j] : 0.0;
-                for(int p = B.rp[k]; p < B.rp[k + 1]; p++)
-                    f(B.ci[p], VALS ? __dmul_rn(a, B.v[p]) : 0.0);
+                int    kk[4], lo[4], hi[4];
+                double av[4];
+#pragma unroll
+                for(int u = 0; u < 4; u++)
+                {
+                    const bool ok = j0 + u < a1;
+                    kk[u]         = ok ? A.ci[j0 + u] : 0;
+                    av[u]         = (VALS && ok) ? A.v[j0 + u] : 0.0;
+                }
+#pragma unroll
+                for(int u = 0; u < 4; u++)
+                {
+                    const bool ok = j0 + u < a1;
+                    lo[u]         = ok ? B.rp[kk[u]] : 0;
+                    hi[u]         = ok ? B.rp[kk[u] + 1] : 0;
+                }
+#pragma unroll
+                for(int u = 0; u < 4; u++)
+                    for(int p0 = lo[u]; p0 < hi[u]; p0 += 4)
+                    {
+                        int    cc[4];
+                        double bv[4];
+#pragma unroll
+                        for(int t = 0; t < 4; t++)
+                        {
+                            const bool ok = p0 + t < hi[u];
+                            cc[t]         = ok ? B.ci[p0 + t] : 0;
+                            bv[t]         = (VALS && ok) ? B.v[p0 + t] : 0.0;
+                        }
+#pragma unroll
+                        for(int t = 0; t < 4; t++)
+                            if(p0 + t < hi[u])
+                                f(cc[t], VALS ? __dmul_rn(av[u], bv[t]) : 0.0);
+                    }
             }
         }
         __device__ int32_t out_start(int row) const
