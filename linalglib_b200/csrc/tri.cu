@@ -55,82 +55,261 @@ namespace lab
         A->tri = nullptr;
     }
 
-    // Levels of the lower (reads columns < i) or upper (columns > i) dependency.
-    static void level_sched(const std::vector<int32_t>& rp, const std::vector<int32_t>& ci,
-                            int m, bool lower, std::vector<int>& order, std::vector<int>& ptr)
+    // ------------------------------------------------------------ level analysis
+    // Dependency levels of the lower (row i reads columns < i) or upper (columns > i)
+    // triangle, on the device, by Kahn's algorithm: the rows with no dependency are
+    // level 0; processing level L decrements the pending-dependency count of every
+    // row that reads one of its rows, and a row whose count reaches 0 joins level
+    // L + 1.  One cooperative launch runs all levels, separated by a grid barrier;
+    // order[] receives the rows level by level (any order within a level: a
+    // level's rows are independent, so results do not depend on it).
+    __global__ void k_dep_count(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                int m, int lower, int32_t* __restrict__ indeg,
+                                int32_t* __restrict__ tcnt)
     {
-        std::vector<int> lev(m, 0);
-        int              nlev = 0;
-        for(int t = 0; t < m; t++)
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int d = 0;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
         {
-            const int i = lower ? t : m - 1 - t;
-            int       l = 0;
-            for(int j = rp[i]; j < rp[i + 1]; j++)
+            const int c = ci[j];
+            if(lower ? c < i : c > i)
             {
-                const int c = ci[j];
-                if(lower ? c < i : c > i)
-                    l = std::max(l, lev[c] + 1);
+                d++;
+                atomicAdd(&tcnt[c], 1);
             }
-            lev[i] = l;
-            nlev   = std::max(nlev, l + 1);
         }
-        ptr.assign(nlev + 1, 0);
-        for(int i = 0; i < m; i++)
-            ptr[lev[i] + 1]++;
-        for(int k = 0; k < nlev; k++)
-            ptr[k + 1] += ptr[k];
-        order.assign(m, 0);
-        std::vector<int> cur(ptr.begin(), ptr.end() - 1);
-        for(int i = 0; i < m; i++) // ascending rows within a level
-            order[cur[lev[i]]++] = i;
+        indeg[i] = d;
+    }
+
+    __global__ void k_dep_fill(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                               int m, int lower, int32_t* __restrict__ tcur,
+                               int32_t* __restrict__ tadj)
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+        {
+            const int c = ci[j];
+            if(lower ? c < i : c > i)
+                tadj[atomicAdd(&tcur[c], 1)] = i;
+        }
+    }
+
+    __global__ void k_diag_pos(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                               int m, int32_t* __restrict__ dpos, int* missing)
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int d = -1;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+            if(ci[j] == i)
+            {
+                d = j;
+                break;
+            }
+        dpos[i] = d;
+        if(d < 0)
+            atomicExch(missing, 1);
+    }
+
+    struct kahn_ctl
+    {
+        unsigned arrive, gen;
+        int      tail, err, nlev;
+    };
+
+    __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+    {
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        return v;
+    }
+    __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v)
+    {
+        asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+    }
+
+    constexpr unsigned kKahnSpin = 1u << 22; // bounded barrier wait (then the error flag)
+
+    // Grid barrier (all blocks are co-resident: cooperative launch).  The last
+    // block to arrive records the level boundary lptr[slot] = rows appended so far
+    // and releases the others; a block that waits kKahnSpin rounds sets the error
+    // flag.  Returns false on error.
+    __device__ bool kahn_barrier(kahn_ctl* c, int slot, int32_t* lptr)
+    {
+        __shared__ int ok;
+        __syncthreads();
+        if(threadIdx.x == 0)
+        {
+            __threadfence();
+            const unsigned g = ld_acquire_u32(&c->gen);
+            ok               = 1;
+            if(atomicAdd(&c->arrive, 1u) == gridDim.x - 1)
+            {
+                atomicExch(&c->arrive, 0u);
+                lptr[slot] = atomicAdd(&c->tail, 0);
+                __threadfence();
+                st_release_u32(&c->gen, g + 1u);
+            }
+            else
+            {
+                unsigned it = 0;
+                while(ld_acquire_u32(&c->gen) == g)
+                {
+                    if(++it > kKahnSpin)
+                    {
+                        atomicExch(&c->err, 1);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            if(atomicAdd(&c->err, 0))
+                ok = 0;
+        }
+        __syncthreads();
+        return ok != 0;
+    }
+
+    __global__ void __launch_bounds__(512)
+        k_kahn(const int32_t* __restrict__ tptr, const int32_t* __restrict__ tadj,
+               int32_t* indeg, int m, int32_t* order, int32_t* lptr, kahn_ctl* c)
+    {
+        const int nt  = gridDim.x * blockDim.x;
+        const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+        for(int i = tid; i < m; i += nt)
+            if(indeg[i] == 0)
+                order[atomicAdd(&c->tail, 1)] = i;
+        int L = 0, lo = 0;
+        if(!kahn_barrier(c, 1, lptr))
+            return;
+        for(;;)
+        {
+            const int hi = __ldcg(lptr + L + 1);
+            if(hi == lo)
+            {
+                if(tid == 0)
+                    c->nlev = L;
+                return;
+            }
+            for(int t = lo + tid; t < hi; t += nt)
+            {
+                const int r = __ldcg(order + t);
+                for(int q = tptr[r]; q < tptr[r + 1]; q++)
+                {
+                    const int j = tadj[q];
+                    if(atomicSub(&indeg[j], 1) == 1)
+                        order[atomicAdd(&c->tail, 1)] = j;
+                }
+            }
+            lo = hi;
+            L++;
+            if(!kahn_barrier(c, L + 1, lptr))
+                return;
+        }
+    }
+
+    static lab_status level_sched_dev(const lab_csr_impl* A, bool lower, tri_sched& out,
+                                      cudaStream_t s)
+    {
+        const int      m = (int)A->m;
+        dbuf<int32_t>  indeg, tptr, tcur, tadj, lptr;
+        dbuf<kahn_ctl> ctl;
+        int64_t        ndep = 0;
+        LAB_TRY(indeg.alloc((size_t)m, s));
+        LAB_TRY(tptr.alloc((size_t)m + 1, s));
+        LAB_CUDA(cudaMemsetAsync(tptr.get(), 0, sizeof(int32_t) * ((size_t)m + 1), s));
+        const unsigned g = (unsigned)ceil_div(m, 256);
+        LAB_LAUNCH(k_dep_count, g, 256, 0, s, A->row_ptr, A->col_ind, m, (int)lower, indeg.get(),
+                   tptr.get());
+        LAB_TRY(counts_to_rowptr(tptr.get(), tptr.get(), m, &ndep, s));
+        LAB_TRY(tcur.alloc((size_t)m + 1, s));
+        LAB_TRY(tadj.alloc((size_t)std::max<int64_t>(ndep, 1), s));
+        LAB_CUDA(cudaMemcpyAsync(tcur.get(), tptr.get(), sizeof(int32_t) * ((size_t)m + 1),
+                                 cudaMemcpyDeviceToDevice, s));
+        LAB_LAUNCH(k_dep_fill, g, 256, 0, s, A->row_ptr, A->col_ind, m, (int)lower, tcur.get(),
+                   tadj.get());
+        LAB_TRY(dalloc(&out.rows, (size_t)std::max(m, 1), s));
+        LAB_TRY(lptr.alloc((size_t)m + 2, s));
+        LAB_TRY(ctl.alloc(1, s));
+        LAB_CUDA(cudaMemsetAsync(lptr.get(), 0, sizeof(int32_t) * ((size_t)m + 2), s));
+        LAB_CUDA(cudaMemsetAsync(ctl.get(), 0, sizeof(kahn_ctl), s));
+        static int occ = 0;
+        if(!occ)
+        {
+            if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_kahn, 512, 0) != cudaSuccess ||
+               occ < 1)
+            {
+                cudaGetLastError();
+                occ = 1;
+            }
+        }
+        const int32_t* tp     = tptr.get();
+        const int32_t* ta     = tadj.get();
+        int32_t*       id     = indeg.get();
+        int32_t*       od     = out.rows;
+        int32_t*       lp     = lptr.get();
+        kahn_ctl*      cp     = ctl.get();
+        int            mm     = m;
+        void*          args[] = {(void*)&tp, (void*)&ta, (void*)&id, (void*)&mm,
+                                 (void*)&od, (void*)&lp, (void*)&cp};
+        const unsigned grid =
+            (unsigned)std::max(1, std::min(num_sms() * occ, (int)ceil_div(m, 512)));
+        LAB_CUDA(cudaLaunchCooperativeKernel((const void*)k_kahn, dim3(grid), dim3(512), args, 0,
+                                             s));
+        g_launches.fetch_add(1);
+        kahn_ctl hc{};
+        LAB_TRY(copy_d2h_sync(&hc, ctl.get(), sizeof(hc), s));
+        if(hc.err || hc.tail != m)
+        {
+            set_error("triangular analysis: level computation failed (%s)",
+                      hc.err ? "barrier wait" : "a row never became ready");
+            return LAB_CUDA_ERROR;
+        }
+        out.ptr.assign((size_t)hc.nlev + 1, 0);
+        LAB_TRY(copy_d2h_sync(out.ptr.data(), lptr.get(), sizeof(int32_t) * out.ptr.size(), s));
+        return LAB_OK;
     }
 
     lab_status tri_analyse(lab_csr_impl* A, cudaStream_t s)
     {
         if(A->tri)
             return LAB_OK;
-        const int            m = (int)A->m;
-        std::vector<int32_t> rp((size_t)m + 1), ci((size_t)std::max<int64_t>(A->nnz, 1));
-        LAB_TRY(copy_d2h_sync(rp.data(), A->row_ptr, sizeof(int32_t) * rp.size(), s));
-        if(A->nnz)
-            LAB_TRY(copy_d2h_sync(ci.data(), A->col_ind, sizeof(int32_t) * A->nnz, s));
+        const int m = (int)A->m;
         tri_plan* p = new(std::nothrow) tri_plan();
         if(!p)
             return LAB_OOM;
-        std::vector<int> dpos(m, -1), order;
-        for(int i = 0; i < m; i++)
+        A->tri        = p;
+        lab_status st = dalloc(&p->diag, (size_t)std::max(m, 1), s);
+        dbuf<int>  missing;
+        if(st == LAB_OK)
+            st = missing.alloc(1, s);
+        if(st == LAB_OK && cudaMemsetAsync(missing.get(), 0, sizeof(int), s) != cudaSuccess)
+            st = LAB_CUDA_ERROR;
+        if(st == LAB_OK && m > 0)
         {
-            for(int j = rp[i]; j < rp[i + 1]; j++)
-                if(ci[j] == i)
-                {
-                    dpos[i] = j;
-                    break;
-                }
-            if(dpos[i] < 0)
-                p->all_diag = false;
-        }
-        lab_status st = LAB_OK;
-        auto       up = [&](int32_t** dst, const std::vector<int>& src) {
-            if(st != LAB_OK)
-                return;
-            st = dalloc(dst, std::max<size_t>(src.size(), 1), s);
-            if(st == LAB_OK && !src.empty() &&
-               cudaMemcpyAsync(*dst, src.data(), sizeof(int32_t) * src.size(),
-                               cudaMemcpyHostToDevice, s) != cudaSuccess)
+            k_diag_pos<<<(unsigned)ceil_div(m, 256), 256, 0, s>>>(A->row_ptr, A->col_ind, m,
+                                                                 p->diag, missing.get());
+            g_launches.fetch_add(1);
+            if(cudaGetLastError() != cudaSuccess)
                 st = LAB_CUDA_ERROR;
-        };
-        level_sched(rp, ci, m, true, order, p->lower.ptr);
-        up(&p->lower.rows, order);
-        level_sched(rp, ci, m, false, order, p->upper.ptr);
-        up(&p->upper.rows, order);
-        up(&p->diag, dpos);
+        }
+        if(st == LAB_OK && m > 0)
+            st = level_sched_dev(A, true, p->lower, s);
+        if(st == LAB_OK && m > 0)
+            st = level_sched_dev(A, false, p->upper, s);
         if(st == LAB_OK)
             st = dalloc(&p->ctl, 2, s);
         if(st == LAB_OK && cudaMemsetAsync(p->ctl, 0, sizeof(int32_t) * 2, s) != cudaSuccess)
             st = LAB_CUDA_ERROR;
-        if(st == LAB_OK && cudaStreamSynchronize(s) != cudaSuccess) // host vectors go out of scope
-            st = LAB_CUDA_ERROR;
-        A->tri = p;
+        int miss = 0;
+        if(st == LAB_OK)
+            st = copy_d2h_sync(&miss, missing.get(), sizeof(int), s);
+        p->all_diag = miss == 0;
         if(st != LAB_OK)
             tri_release(A);
         return st;
