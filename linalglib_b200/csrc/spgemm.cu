@@ -433,7 +433,7 @@ namespace lab
         int      jmap[32 * kHashU]; // A entry of each product slot of the current chunk
         int      key[HS];
         double   val[MODE == 1 ? HS : 1];
-        uint64_t sk[MODE == 1 ? HS / 2 : 1];
+        uint64_t sk[MODE == 1 ? HS : 1]; // the filled slots (<= 3/4 of HS) padded to a power of 2
         double   aa[MODE == 1 ? kHashACap : 1];
         double   sp[MODE == 1 ? 32 : 1];
         int      ab0[kHashACap];
@@ -681,8 +681,8 @@ namespace lab
     // Row classes.  Symbolic (by the product bound ub): 0 = lane tier (ub <= 32),
     // 1..4 = hash tables of 128..1024 slots (ub <= slots / 2; class 4 takes every
     // larger row and checks for overflow, and its overflow rows get 4096 slots).  Numeric (by the exact column count of
-    // rows with ub > 32): 1..6 = tables of 64..2048 slots (count <= slots / 2),
-    // 7 = global sort tier.
+    // rows with ub > 32): 1..6 = tables of 64..2048 slots (count <= 3/4 of the
+    // slots), 7 = global sort tier.
     __device__ __forceinline__ int gemm_class(int phase, int ub, int cnt)
     {
         if(ub <= kEscLaneCap)
@@ -700,10 +700,12 @@ namespace lab
             }
             return c;
         }
-        if(cnt > 1024)
+        // exact counts: a table may fill to 3/4 (fewer slots to clear and compact,
+        // twice the occupancy of a half-full table, a few more probes)
+        if(4 * cnt > 3 * 2048)
             return 7;
         int c = 1, hs = 64;
-        while(2 * cnt > hs)
+        while(4 * cnt > 3 * hs)
         {
             c++;
             hs <<= 1;
