@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=None,
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=None,
                     help="grid side (default: 128 for the Poisson step, 160 for mixed, "
                          "96 for adjoint, 64 for the multi-RHS batch)")
     ap.add_argument("--rtol", type=float, default=1e-8)
@@ -94,6 +94,7 @@ class Dist:
 
     def init(self, need_gpu=True):
         import torch
+        self.dev = "cuda" if need_gpu else "cpu"
         if need_gpu:
             torch.cuda.set_device(self.local)
         if self.world > 1:
@@ -111,7 +112,7 @@ class Dist:
         if not self.pg:
             return v
         import torch
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        t = torch.tensor([v], dtype=torch.float64, device=getattr(self, "dev", "cuda"))
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
