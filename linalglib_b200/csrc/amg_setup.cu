@@ -289,6 +289,34 @@ namespace lab
             pmis_round_row_warp(i, lane, rp, ci, conn, st, hash, out, agg, flags, round);
     }
 
+    // All rounds in one CTA for small levels (the per-round launches dominate
+    // there): round r reads buffer r & 1 and writes the other, as the launches do,
+    // and stops after the first round that left no row undecided.
+    constexpr int kPmisSmallRows = 4096;
+
+    __global__ void __launch_bounds__(1024)
+        k_pmis_rounds_small(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                            const int32_t* __restrict__ conn, int64_t m, int32_t* b0, int32_t* b1,
+                            const int32_t* __restrict__ hash, int64_t* __restrict__ agg,
+                            int32_t* flags, int wide)
+    {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for(int r = 0; r < 20; r++)
+        {
+            if(r > 0 && flags[r - 1] == 0)
+                break;
+            const int32_t* st  = (r & 1) ? b1 : b0;
+            int32_t*       out = (r & 1) ? b0 : b1;
+            if(wide)
+                for(int64_t i = wid; i < m; i += nw)
+                    pmis_round_row_warp(i, lane, rp, ci, conn, st, hash, out, agg, flags, r);
+            else
+                for(int64_t i = threadIdx.x; i < m; i += blockDim.x)
+                    pmis_round_row(i, rp, ci, conn, st, hash, out, agg, flags, r);
+            __syncthreads();
+        }
+    }
+
     // Rounds that ran: round r runs iff r == 0 or round r-1 left a row undecided.
     __device__ __forceinline__ int pmis_rounds_run(const int32_t* flags)
     {
@@ -476,18 +504,22 @@ namespace lab
         // ping-pong: round r reads buffer r & 1 of {state, snap} and writes the other
         int32_t* buf[2] = {state.get(), snap.get()};
         // long rows (coarse levels): a warp per row
-        for(int r = 0; r < 20; r++)
+        if(m <= kPmisSmallRows)
+            LAB_LAUNCH(k_pmis_rounds_small, 1, 1024, 0, s, prp, pci, pconn, m, buf[0], buf[1],
+                       (const int32_t*)hash.get(), agg, flags.get(), (int)wide);
+        else
         {
-            if(wide)
-                LAB_LAUNCH(k_pmis_round_warp, std::min<unsigned>(gw, num_sms() * 8), 256, 0, s,
-                           prp, pci, pconn, m,
-                           (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg,
-                           flags.get(), r);
-            else
-                LAB_LAUNCH(k_pmis_round, std::min<unsigned>(g, num_sms() * 8), 256, 0, s, prp, pci,
-                           pconn, m,
-                           (const int32_t*)buf[r & 1], hash.get(), buf[(r + 1) & 1], agg,
-                           flags.get(), r);
+            for(int r = 0; r < 20; r++)
+            {
+                if(wide)
+                    LAB_LAUNCH(k_pmis_round_warp, std::min<unsigned>(gw, num_sms() * 8), 256, 0,
+                               s, prp, pci, pconn, m, (const int32_t*)buf[r & 1], hash.get(),
+                               buf[(r + 1) & 1], agg, flags.get(), r);
+                else
+                    LAB_LAUNCH(k_pmis_round, std::min<unsigned>(g, num_sms() * 8), 256, 0, s, prp,
+                               pci, pconn, m, (const int32_t*)buf[r & 1], hash.get(),
+                               buf[(r + 1) & 1], agg, flags.get(), r);
+            }
         }
         if(rounds)
         {
