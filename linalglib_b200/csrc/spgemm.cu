@@ -766,24 +766,45 @@ namespace lab
         }
     };
 
-    static lab_status gemm_classify(int phase, const int32_t* upper, const int32_t* rp, int64_t m,
-                                    gemm_classes& g, cudaStream_t s)
+    // Classification in two halves around a synchronisation the caller makes
+    // anyway: the count kernel and an asynchronous copy of the histogram into
+    // pinned host memory, then (after the sync) the class starts and the fill.
+    static lab_status gemm_class_count(int phase, const int32_t* upper, const int32_t* rp,
+                                       int64_t m, int* dev_hist, int* host_hist, cudaStream_t s)
     {
-        dbuf<int> cnt;
-        LAB_TRY(cnt.alloc(2 * kHashClasses, s));
-        LAB_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * kHashClasses, s));
+        LAB_CUDA(cudaMemsetAsync(dev_hist, 0, sizeof(int) * kHashClasses, s));
         const unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(m, 256), 4096);
-        LAB_LAUNCH(k_gemm_class_count, grid, 256, 0, s, phase, upper, rp, m, cnt.get());
-        int h[kHashClasses];
-        LAB_TRY(copy_d2h_sync(h, cnt.get(), sizeof(h), s));
+        LAB_LAUNCH(k_gemm_class_count, grid, 256, 0, s, phase, upper, rp, m, dev_hist);
+        LAB_CUDA(cudaMemcpyAsync(host_hist, dev_hist, sizeof(int) * kHashClasses,
+                                 cudaMemcpyDeviceToHost, s));
+        return LAB_OK;
+    }
+
+    static lab_status gemm_class_fill(int phase, const int32_t* upper, const int32_t* rp,
+                                      int64_t m, const int* host_hist, int* dev_start,
+                                      gemm_classes& g, cudaStream_t s)
+    {
         for(int c = 0; c < kHashClasses; c++)
-            g.start[c + 1] = g.start[c] + h[c];
-        LAB_CUDA(cudaMemcpyAsync(cnt.get() + kHashClasses, g.start, sizeof(int) * kHashClasses,
+            g.start[c + 1] = g.start[c] + host_hist[c];
+        LAB_CUDA(cudaMemcpyAsync(dev_start, g.start, sizeof(int) * kHashClasses,
                                  cudaMemcpyHostToDevice, s));
         LAB_TRY(g.rows.alloc((size_t)m + 1, s));
-        LAB_LAUNCH(k_gemm_class_fill, grid, 256, 0, s, phase, upper, rp, m,
-                   cnt.get() + kHashClasses, g.rows.get());
+        const unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(m, 256), 4096);
+        LAB_LAUNCH(k_gemm_class_fill, grid, 256, 0, s, phase, upper, rp, m, dev_start,
+                   g.rows.get());
         return LAB_OK;
+    }
+
+    // Small pinned host buffer of this thread for the asynchronous copies above.
+    static int* gemm_pinned()
+    {
+        static thread_local int* p = nullptr;
+        if(!p && cudaMallocHost(&p, 64 * sizeof(int)) != cudaSuccess)
+        {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return p;
     }
 
     template <int MODE, int HS, int WARPS>
@@ -909,21 +930,28 @@ namespace lab
         else if(A->m > 0)
             LAB_LAUNCH(k_gemm_upper, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, s, Ar,
                        B->row_ptr, A->m, upper.get(), ovf.get());
-        int h = 0;
-        LAB_TRY(copy_d2h_sync(&h, ovf.get(), sizeof(int), s));
-        if(h)
+        exp_gemm      e{Ar, Br};
+        const int64_t m  = A->m;
+        int*          hp = gemm_pinned(); // [0] overflow, [1..] phase-0 classes, [16..] phase 1
+        if(!hp)
+            return LAB_OOM;
+        dbuf<int> dh;
+        LAB_TRY(dh.alloc(4 * kHashClasses, s));
+        if(m > 0)
+            LAB_TRY(gemm_class_count(0, upper.get(), nullptr, m, dh.get(), hp + 1, s));
+        LAB_CUDA(cudaMemcpyAsync(hp, ovf.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        LAB_CUDA(cudaStreamSynchronize(s)); // the overflow flag and the class counts
+        if(hp[0])
         {
             set_error("spgemm: a row has more than 2^30 intermediate products");
             return LAB_NOT_SUPPORTED;
         }
-        exp_gemm      e{Ar, Br};
-        const int64_t m = A->m;
         if(m == 0)
             return esc_build(e, upper.get(), m, B->n, C, s);
 
         // ---- symbolic: lane tier (<= 32 products), hash classes, overflow -> global sort
         gemm_classes gs;
-        LAB_TRY(gemm_classify(0, upper.get(), nullptr, m, gs, s));
+        LAB_TRY(gemm_class_fill(0, upper.get(), nullptr, m, hp + 1, dh.get() + kHashClasses, gs, s));
         dbuf<int32_t> counts, ovf_rows, ovf2_rows, rp;
         dbuf<int>     novf_d;
         LAB_TRY(counts.alloc((size_t)m + 1, s));
@@ -961,8 +989,19 @@ namespace lab
 
         // ---- row pointer and allocation
         LAB_TRY(rp.alloc((size_t)m + 1, s));
-        int64_t nnz = 0;
-        LAB_TRY(counts_to_rowptr(counts.get(), rp.get(), m, &nnz, s));
+        LAB_TRY(counts_to_rowptr(counts.get(), rp.get(), m, nullptr, s));
+        // the numeric classes (by exact count) are counted before the one sync that
+        // reads the nonzero total
+        LAB_TRY(gemm_class_count(1, upper.get(), rp.get(), m, dh.get() + 2 * kHashClasses,
+                                 hp + 16, s));
+        int32_t nnz32 = 0;
+        LAB_TRY(copy_d2h_sync(&nnz32, rp.get() + m, sizeof(int32_t), s));
+        if(nnz32 < 0)
+        {
+            set_error("nonzero count exceeds int32 range");
+            return LAB_NOT_SUPPORTED;
+        }
+        const int64_t nnz = nnz32;
         lab_csr_impl* out = nullptr;
         LAB_TRY(csr_alloc(&out, m, B->n, nnz, s));
         lab_status st = LAB_OK;
@@ -975,7 +1014,8 @@ namespace lab
         e2.out_rp   = out->row_ptr;
         gemm_classes gn;
         if(st == LAB_OK)
-            st = gemm_classify(1, upper.get(), out->row_ptr, m, gn, s);
+            st = gemm_class_fill(1, upper.get(), rp.get(), m, hp + 16, dh.get() + 3 * kHashClasses,
+                                 gn, s);
         if(st == LAB_OK)
         {
             stream_fork f(s, m); // lane tier and hash classes side by side
