@@ -8,7 +8,7 @@
 namespace lab
 {
     // Levels of the lower and upper dependency of A's pattern and the diagonal
-    // positions (host analysis, cached on A until it is released).
+    // positions (device analysis, cached on A until it is released).
     lab_status tri_analyse(lab_csr_impl* A, cudaStream_t s);
 
     // x = T^-1 b on the lower (columns < i) or upper (columns > i) part of A.
