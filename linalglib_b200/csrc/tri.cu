@@ -15,6 +15,7 @@
 // are bit-identical to the reference's sequential loops.
 #include "internal.cuh"
 #include "tri.cuh"
+#include "amg.cuh"
 
 #include <algorithm>
 #include <climits>
@@ -63,6 +64,13 @@ namespace lab
     // L + 1.  One cooperative launch runs all levels, separated by a grid barrier;
     // order[] receives the rows level by level (any order within a level: a
     // level's rows are independent, so results do not depend on it).
+    __global__ void k_iota(int32_t* __restrict__ p, int n)
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i < n)
+            p[i] = i;
+    }
+
     __global__ void k_dep_count(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                 int m, int lower, int32_t* __restrict__ indeg,
                                 int32_t* __restrict__ tcnt)
@@ -213,6 +221,60 @@ namespace lab
         }
     }
 
+    // Row -> level of the level order.
+    __global__ void k_row_level(const int32_t* __restrict__ order, const int32_t* __restrict__ lptr,
+                                int m, int nlev, int32_t* __restrict__ lev)
+    {
+        const int t = blockIdx.x * blockDim.x + threadIdx.x;
+        if(t >= m)
+            return;
+        int lo = 0, hi = nlev - 1; // the level L with lptr[L] <= t < lptr[L + 1]
+        while(lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if(lptr[mid] <= t)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        lev[order[t]] = lo;
+    }
+
+    // Rows of each level in ascending order (neighbouring rows of a level then load
+    // neighbouring matrix rows): the level order is the transpose of the m x nlev
+    // row -> level incidence, and the library's transpose keeps each output row in
+    // source-row order.
+    static lab_status order_levels(tri_sched& out, const int32_t* lptr, int m, int nlev,
+                                   cudaStream_t s)
+    {
+        if(m == 0 || nlev <= 1)
+            return LAB_OK;
+        lab_csr_impl* T = nullptr;
+        LAB_TRY(csr_alloc(&T, m, nlev, m, s));
+        lab_status st = LAB_OK;
+        k_iota<<<(unsigned)ceil_div(m + 1, 256), 256, 0, s>>>(T->row_ptr, m + 1);
+        k_row_level<<<(unsigned)ceil_div(m, 256), 256, 0, s>>>(out.rows, lptr, m, nlev, T->col_ind);
+        g_launches.fetch_add(2);
+        if(cudaGetLastError() != cudaSuccess ||
+           cudaMemsetAsync(T->val, 0, sizeof(double) * (size_t)m, s) != cudaSuccess)
+            st = LAB_CUDA_ERROR;
+        lab_csr_impl* Tt = nullptr;
+        if(st == LAB_OK)
+            st = transpose(T, &Tt, s);
+        if(st == LAB_OK &&
+           cudaMemcpyAsync(out.rows, Tt->col_ind, sizeof(int32_t) * (size_t)m,
+                           cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            st = LAB_CUDA_ERROR;
+        if(Tt)
+        {
+            cudaStreamSynchronize(s);
+            csr_release(Tt);
+        }
+        cudaStreamSynchronize(s);
+        csr_release(T);
+        return st;
+    }
+
     static lab_status level_sched_dev(const lab_csr_impl* A, bool lower, tri_sched& out,
                                       cudaStream_t s)
     {
@@ -272,7 +334,7 @@ namespace lab
         }
         out.ptr.assign((size_t)hc.nlev + 1, 0);
         LAB_TRY(copy_d2h_sync(out.ptr.data(), lptr.get(), sizeof(int32_t) * out.ptr.size(), s));
-        return LAB_OK;
+        return order_levels(out, lptr.get(), m, hc.nlev, s);
     }
 
     lab_status tri_analyse(lab_csr_impl* A, cudaStream_t s)
