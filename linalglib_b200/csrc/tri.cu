@@ -319,10 +319,19 @@ namespace lab
         int            mm     = m;
         void*          args[] = {(void*)&tp, (void*)&ta, (void*)&id, (void*)&mm,
                                  (void*)&od, (void*)&lp, (void*)&cp};
-        const unsigned grid =
-            (unsigned)std::max(1, std::min(num_sms() * occ, (int)ceil_div(m, 512)));
-        LAB_CUDA(cudaLaunchCooperativeKernel((const void*)k_kahn, dim3(grid), dim3(512), args, 0,
-                                             s));
+        unsigned grid = (unsigned)std::max(1, std::min(num_sms() * occ, (int)ceil_div(m, 512)));
+        // every block must be resident at once: a device shared with other work may
+        // not fit the occupancy-derived grid, so halve it until the launch is accepted
+        cudaError_t le = cudaErrorCooperativeLaunchTooLarge;
+        while(true)
+        {
+            le = cudaLaunchCooperativeKernel((const void*)k_kahn, dim3(grid), dim3(512), args, 0, s);
+            if(le != cudaErrorCooperativeLaunchTooLarge || grid == 1)
+                break;
+            cudaGetLastError();
+            grid = std::max(1u, grid / 2);
+        }
+        LAB_CUDA(le);
         g_launches.fetch_add(1);
         kahn_ctl hc{};
         LAB_TRY(copy_d2h_sync(&hc, ctl.get(), sizeof(hc), s));
