@@ -56,9 +56,9 @@ def parse():
                     help="grid side (default: 128 for the Poisson step, 160 for mixed, "
                          "96 for adjoint, 64 for the multi-RHS batch)")
     ap.add_argument("--rtol", type=float, default=1e-8)
-    ap.add_argument("--matrix", default="poisson", choices=["poisson", "diffusion27"],
-                    help="operator of --mode spmv: 3D 7-point Poisson (default) or the "
-                         "27-point diffusion operator")
+    ap.add_argument("--matrix", default=None, choices=["poisson", "diffusion27"],
+                    help="operator of --mode spmv (default 3D 7-point Poisson) and --mode "
+                         "mixed (default the 27-point diffusion operator)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="full",
                     choices=["full", "profile", "spmv", "mixed", "batched", "adjoint", "tri"],
@@ -364,9 +364,11 @@ def run_ours(args, d):
     dA.analyse()
     if args.mode == "spmv":
         roof = dominant_kernel_roofline(core, dA, m, nnz, torch,
-                                        profiled=args.matrix == "poisson" and args.n == 128)
+                                        profiled=(args.matrix or "poisson") == "poisson"
+                                        and args.n == 128)
         if d.rank == 0:
-            print(json.dumps({"mode": "spmv", "matrix": f"{args.matrix} {args.n}^3", "rows": int(m),
+            print(json.dumps({"mode": "spmv", "matrix": f"{args.matrix or 'poisson'} {args.n}^3",
+                              "rows": int(m),
                               "nnz": int(nnz), "roofline": roof}), flush=True)
         d.close()
         return 0
@@ -522,16 +524,25 @@ def _rel_res(torch, dA, x, b):
 
 def run_mixed(args, d):
     """27-point variable-coefficient diffusion (lognormal sigma 1.5, z x100) on an
-    n^3 grid: one FP64 SA hierarchy, PCG (omega 2/3) with the FP64, FP32 and
-    FP32+BF16 cycles to rtol 1e-8 and 1e-10; error of each against the FP64 solve."""
+    n^3 grid (default; --matrix poisson: the 3D 7-point Poisson problem, omega 1):
+    one FP64 SA hierarchy, PCG with the FP64, FP32 and FP32+BF16 cycles to rtol
+    1e-8 and 1e-10; error of each against the FP64 solve."""
     import torch
     d.init(need_gpu=True)
     import linalglib_b200.core as core
     from linalglib_b200 import _lib as L
     from linalglib_b200 import problems as P
     core.init()
-    n = args.n or 160
-    A = P.diffusion27(n, sigma=1.5, zscale=100.0, seed=0)
+    if args.matrix == "poisson":
+        # the 7-point Poisson problem with the reference's smoother weight
+        n = args.n or 128
+        A = P.poisson3d(n)
+        omega, wl = 1.0, f"SA-AMG-PCG, 3D 7-point Poisson {n}^3, omega 1"
+    else:
+        n = args.n or 160
+        A = P.diffusion27(n, sigma=1.5, zscale=100.0, seed=0)
+        omega, wl = 2.0 / 3.0, (f"SA-AMG-PCG, 27-point diffusion {n}^3 (lognormal sigma 1.5, "
+                                "z x100), omega 2/3")
     b, xt = P.rhs_from_solution(*A, seed=0)
     dA = core.CsrMatrix.from_arrays(*A)
     dA.analyse()
@@ -539,8 +550,7 @@ def run_mixed(args, d):
     xtd = core.vec(xt)
     H = core.Hierarchy(dA)  # warm-up (module loading, pool growth)
     t_setup, _ = _events_ms(torch, lambda: core.Hierarchy(dA), 3)
-    res = {"mode": "mixed", "config": {"workload": f"SA-AMG-PCG, 27-point diffusion {n}^3 "
-                                                  "(lognormal sigma 1.5, z x100), omega 2/3",
+    res = {"mode": "mixed", "config": {"workload": wl,
                                        "rows": int(A[0].size - 1), "nnz": int(A[2].size),
                                        "levels": H.levels},
            "setup_ms": t_setup, "runs": []}
@@ -549,7 +559,7 @@ def run_mixed(args, d):
         ctl = core.iter_control(rel_tol=rtol, abs_tol=0.0, max_iter=1000)
         x64 = None
         for prec in (L.PREC_FP64, L.PREC_FP32, L.PREC_FP32_BF16):
-            M = core.Preconditioner.amg(H, core.amg_options(omega=2.0 / 3.0, precision=prec))
+            M = core.Preconditioner.amg(H, core.amg_options(omega=omega, precision=prec))
             x = torch.zeros_like(bd)
             core.pcg(dA, bd, x=x, M=M, control=ctl)  # warm-up: value copies, graph capture
             info = []
