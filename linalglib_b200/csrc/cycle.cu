@@ -178,6 +178,25 @@ namespace lab
             y[i] = (float)x[i];
     }
 
+    // k_d2f that also writes x0 = omega D^-1 b (FP32): the level-0 pre-smoothing
+    // pass then gathers x0 once per entry instead of recomputing it from b and
+    // D^-1 at every gather (the same FP32 products op_pre0 forms, so the cycle's
+    // result is unchanged; the reduced-precision passes are issue-bound).
+    __global__ void k_d2f_x0(const double* __restrict__ r, float* __restrict__ b,
+                             const float* __restrict__ invd, float omega, float* __restrict__ x0,
+                             int64_t n, const int* skip)
+    {
+        if(skip && *skip)
+            return;
+        for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+            i += (int64_t)gridDim.x * blockDim.x)
+        {
+            const float bi = (float)r[i];
+            b[i]           = bi;
+            x0[i]          = omega * (invd[i] * bi);
+        }
+    }
+
     // z = (double) x with (z, r) accumulated for the PCG beta.
     __global__ void __launch_bounds__(256)
         k_f2d_dot(const float* __restrict__ x, const double* __restrict__ r, double* __restrict__ z,
@@ -1038,10 +1057,22 @@ namespace lab
             return cycle<double>(h, 0, c.o->cycle, z, r, true, c);
         }
         // Reduced precision: r -> fp32, FP32 cycle, z = fp64(x) with (z, r) fused.
-        level_ws&     w = h->ws[0];
-        const int64_t m = h->A[0]->m;
-        LAB_LAUNCH(k_d2f, grid_for(m), 256, 0, c.s, r, w.bf, m, c.skip);
-        LAB_TRY(cycle<float>(h, 0, c.o->cycle, w.xf, (const float*)w.bf, true, c));
+        level_ws&              w = h->ws[0];
+        const int64_t          m = h->A[0]->m;
+        const lab_amg_options* o = c.o;
+        if(h->levels > 0 && o->smoother == LAB_SMOOTH_JACOBI && o->n1 >= 1)
+        {
+            float* x0 = cycle_start<float>(h, 0, o->cycle, w.xf, o);
+            LAB_LAUNCH(k_d2f_x0, grid_for(m), 256, 0, c.s, r, w.bf, lv<float>::invd(h->A[0]),
+                       (float)o->omega, x0, m, c.skip);
+            LAB_TRY(cycle<float>(h, 0, o->cycle, w.xf, (const float*)w.bf, true, c, red_buf(),
+                                 nullptr, true));
+        }
+        else
+        {
+            LAB_LAUNCH(k_d2f, grid_for(m), 256, 0, c.s, r, w.bf, m, c.skip);
+            LAB_TRY(cycle<float>(h, 0, o->cycle, w.xf, (const float*)w.bf, true, c));
+        }
         LAB_LAUNCH(k_f2d_dot, red_grid(m), 256, 0, c.s, (const float*)w.xf, r, z, m, dot.partial,
                    dot.counter, dot.out, c.skip);
         return LAB_OK;
