@@ -55,7 +55,12 @@ namespace lab
     __device__ __forceinline__ int col_of(IT c, int row)
     {
         if constexpr(sizeof(IT) == 2)
-            return row + (int)c;
+        {
+            // sign extension by integer arithmetic on the zero-extended bits (keeps
+            // it off the conversion pipe)
+            const int u = (int)(unsigned short)c;
+            return row + ((u ^ 0x8000) - 0x8000);
+        }
         else
             return (int)c;
     }
