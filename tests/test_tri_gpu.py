@@ -148,3 +148,36 @@ def test_trsv_in_place_and_ssor_arg_check(gpu, oracle):
     for bad in (0.0, 2.0, -1.0):
         with pytest.raises(L.LabError):
             gpu.Preconditioner.ssor(dA, bad)
+
+
+def _random_nonsym(n, per_row, seed):
+    """Random nonsymmetric pattern (sorted rows, stored diagonal, a few empty
+    off-diagonal rows) with diagonally dominant values."""
+    rng = np.random.default_rng(seed)
+    rp, ci, v = [0], [], []
+    for i in range(n):
+        k = 0 if i % 17 == 5 else rng.integers(1, per_row + 1)
+        cols = set(rng.choice(n, size=min(k, n), replace=False).tolist()) - {i}
+        cols = sorted(cols | {i})
+        vals = rng.uniform(-1, 1, len(cols))
+        vals[cols.index(i)] = len(cols) + 1.0
+        ci += cols
+        v += vals.tolist()
+        rp.append(len(ci))
+    return (np.array(rp, np.int32), np.array(ci, np.int32), np.array(v, np.float64))
+
+
+@pytest.mark.parametrize("n,per_row,seed", [(1, 1, 0), (2, 2, 1), (300, 6, 2), (2000, 12, 3)])
+def test_nonsymmetric_patterns_bit_exact(gpu, oracle, n, per_row, seed):
+    # the level analysis reads the dependents of a row through the pattern's
+    # transpose: nonsymmetric patterns exercise it
+    A = _random_nonsym(n, per_row, seed)
+    b = np.random.default_rng(seed + 10).uniform(-1, 1, n)
+    dA = gpu.CsrMatrix.from_arrays(*A)
+    for lower in (True, False):
+        for unit in (True, False):
+            x = dA.trsv(gpu.vec(b), lower=lower, unit_diag=unit)
+            assert np.array_equal(_bits(x.cpu().numpy()), _bits(oracle.trsv(A, b, lower, unit)))
+    for kind in (0, 1, 2, 3, 4):
+        z = _precond(gpu, kind, dA).apply(gpu.vec(b)).cpu().numpy()
+        assert np.array_equal(_bits(z), _bits(oracle.precond_apply(kind, A, b, omega=1.3))), kind

@@ -79,3 +79,25 @@ def test_precond_cg_oracle_vs_reference(oracle, reference, kind):
     assert io == ir
     tol = 1e-9 if kind in (0, 4) else 1e-6
     assert np.max(np.abs(xo - xr)) <= tol * np.max(np.abs(xr))
+
+
+@pytest.mark.parametrize("n,per_row,seed", [(2, 2, 1), (300, 6, 2)])
+def test_nonsymmetric_patterns_oracle_vs_reference(oracle, reference, n, per_row, seed):
+    rng = np.random.default_rng(seed)
+    rp, ci, v = [0], [], []
+    for i in range(n):
+        cols = sorted(set(rng.choice(n, size=min(per_row, n), replace=False).tolist()) | {i})
+        vals = rng.uniform(-1, 1, len(cols))
+        vals[cols.index(i)] = len(cols) + 1.0
+        ci += cols
+        v += vals.tolist()
+        rp.append(len(ci))
+    A = (np.array(rp, np.int32), np.array(ci, np.int32), np.array(v))
+    b = rng.uniform(-1, 1, n)
+    for kind in range(5):
+        assert np.array_equal(oracle.precond_apply(kind, A, b, omega=1.3).view(np.int64),
+                              reference.precond_apply(kind, A, b, omega=1.3).view(np.int64))
+    for fn in ("csrilu0", "csric0"):
+        vo, so, no = getattr(oracle, fn)(A)
+        vr, sr, nr = getattr(reference, fn)(A)
+        assert np.array_equal(vo.view(np.int64), vr.view(np.int64)) and (so, no) == (sr, nr)
