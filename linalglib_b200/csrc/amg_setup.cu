@@ -798,10 +798,15 @@ namespace lab
     lab_status amg_sa_prolongation(const lab_csr_impl* A, const int32_t* conn, const int64_t* agg,
                                    double relax, lab_csr_impl** P, cudaStream_t s)
     {
-        int64_t mx = -1;
+        // n_c = max aggregate + 1 (saamg.cpp:68-76): the maximum travels to pinned
+        // memory asynchronously and is read at esc_build's first synchronisation
+        int64_t* hp = pinned_small();
+        if(!hp)
+            return LAB_OOM;
+        hp[0] = -1;
         if(A->m > 0)
-            LAB_TRY(max_i64(agg, A->m, &mx, s));
-        int64_t nc = (mx > -1 ? mx : -1) + 1; // saamg.cpp:68-76
+            LAB_TRY(max_i64_async(agg, A->m, hp, s));
+        const std::function<int64_t()> nc_late = [hp] { return (hp[0] > -1 ? hp[0] : -1) + 1; };
         if(A->m > 0 && A->nnz > 12 * A->m)
         {
             dbuf<int32_t> cnt, sci;
@@ -814,13 +819,13 @@ namespace lab
                        A->row_ptr, A->col_ind, (const double*)A->val, conn, A->m, sci.get(),
                        sv.get(), cnt.get(), dgs.get());
             exp_sap_c e{A->row_ptr, cnt.get(), sci.get(), sv.get(), dgs.get(), agg, relax};
-            return esc_build(e, cnt.get(), A->m, nc, P, s);
+            return esc_build(e, cnt.get(), A->m, 0, P, s, nc_late);
         }
         dbuf<int32_t> upper;
         LAB_TRY(upper.alloc((size_t)A->m + 1, s));
         LAB_TRY(row_lengths(A->row_ptr, A->m, upper.get(), s));
         exp_sap e{A->row_ptr, A->col_ind, A->val, conn, agg, relax};
-        return esc_build(e, upper.get(), A->m, nc, P, s);
+        return esc_build(e, upper.get(), A->m, 0, P, s, nc_late);
     }
 
     // ------------------------------------------------------------ UA prolongation

@@ -656,6 +656,33 @@ namespace lab
         return copy_d2h_sync(result, r.out, sizeof(int64_t), s);
     }
 
+    int64_t* pinned_small()
+    {
+        static thread_local int64_t* p = nullptr;
+        if(!p && cudaMallocHost(&p, 64 * sizeof(int64_t)) != cudaSuccess)
+        {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return p;
+    }
+
+    lab_status max_i64_async(const int64_t* x, int64_t n, int64_t* host_out, cudaStream_t s)
+    {
+        if(n <= 0)
+        {
+            *host_out = INT64_MIN;
+            return LAB_OK;
+        }
+        red_scratch r;
+        LAB_TRY(get_red_scratch(r, s));
+        int grid = (int)std::min<int64_t>(kRedBlocks, ceil_div<int64_t>(n, kRedThreads));
+        LAB_LAUNCH(k_max_i64, grid, kRedThreads, 0, s, x, n, (int64_t*)r.partial, r.counter,
+                   (int64_t*)r.out);
+        LAB_CUDA(cudaMemcpyAsync(host_out, r.out, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        return LAB_OK;
+    }
+
     // ------------------------------------------------------------ BLAS-1 kernels
     // Arithmetic follows host_axpy.cpp:35-82 operation by operation (no FMA
     // contraction: __dmul_rn / __dadd_rn), so results are bit-identical.

@@ -17,6 +17,8 @@
 
 #include "internal.cuh"
 
+#include <functional>
+
 namespace lab
 {
     constexpr int kEscLaneCap = 32;
@@ -391,12 +393,18 @@ namespace lab
 
     // Full two-pass construction of a CSR matrix (m x n) from an expansion:
     // item counts -> tiers -> symbolic counts -> row_ptr -> numeric fill.
+    // n_late: when given, the column count is n_late() evaluated after the first
+    // synchronisation here (for a value the caller copies to pinned memory
+    // asynchronously, so it needs no round trip of its own).
     template <class Exp>
     lab_status esc_build(const Exp& e, const int32_t* upper, int64_t m, int64_t n,
-                         lab_csr_impl** out, cudaStream_t s)
+                         lab_csr_impl** out, cudaStream_t s,
+                         const std::function<int64_t()>& n_late = {})
     {
         esc_tiers t;
         LAB_TRY(esc_classify(upper, m, t, s));
+        if(n_late)
+            n = n_late();
         lab_csr_impl* C = nullptr;
         dbuf<int32_t> counts;
         LAB_TRY(counts.alloc((size_t)m + 1, s));

@@ -214,6 +214,11 @@ namespace lab
     lab_status counts_to_rowptr(const int32_t* counts, int32_t* row_ptr, int64_t n,
                                 int64_t* total, cudaStream_t s);
     lab_status max_i64(const int64_t* x, int64_t n, int64_t* result_host, cudaStream_t s);
+    // max_i64 whose result lands in pinned host memory (pinned_small()) when the
+    // stream next synchronises: read it only after a later synchronisation.
+    lab_status max_i64_async(const int64_t* x, int64_t n, int64_t* host_out, cudaStream_t s);
+    // A small pinned host buffer of the calling thread (64 int64 slots), or null.
+    int64_t* pinned_small();
     lab_status copy_d2h_sync(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
     // Fixed-shape reduction grid shared by every deterministic reduction.

@@ -90,9 +90,10 @@ namespace lab
         LAB_CUDA(cudaMemcpyAsync(cnt.get(), cur, sizeof(cur), cudaMemcpyHostToDevice, s));
         LAB_TRY(t.rows.alloc((size_t)m, s));
         LAB_TRY(t.g_offsets.alloc((size_t)std::max(t.ng, 1) + 1, s));
+        // (cur[] may leave scope at once: a copy from pageable host memory is staged
+        // before cudaMemcpyAsync returns)
         LAB_LAUNCH(k_tier_fill, grid, 256, 0, s, upper, m, cnt.get(), t.rows.get(),
                    t.g_offsets.get());
-        LAB_CUDA(cudaStreamSynchronize(s)); // cur[] lives on the host stack
         if(t.ng > 0)
         {
             // scratch offsets: exclusive scan of padded sizes
@@ -487,8 +488,10 @@ namespace lab
     __global__ void __launch_bounds__(32 * WARPS)
         k_hash_gemm(csr_ref A, csr_ref B, const int32_t* __restrict__ rows, int nrows,
                     int32_t* counts, const int32_t* __restrict__ out_rp, int32_t* out_ci,
-                    double* out_v, int32_t* ovf_rows, int* n_ovf)
+                    double* out_v, int32_t* ovf_rows, int* n_ovf, const int* nrows_dev)
     {
+        if(nrows_dev) // the list's length is known on the device only (nrows: its capacity)
+            nrows = min(nrows, *nrows_dev);
         using S = hash_smem<MODE, HS>;
         extern __shared__ __align__(16) unsigned char hsm[];
         const int      wid  = threadIdx.x >> 5;
@@ -810,7 +813,8 @@ namespace lab
     template <int MODE, int HS, int WARPS>
     static lab_status launch_hash_cls(csr_ref Ar, csr_ref Br, const int32_t* rows, int n,
                                       int32_t* counts, const int32_t* out_rp, int32_t* out_ci,
-                                      double* out_v, int32_t* ovf_rows, int* n_ovf, cudaStream_t s)
+                                      double* out_v, int32_t* ovf_rows, int* n_ovf, cudaStream_t s,
+                                      const int* n_dev = nullptr)
     {
         if(n == 0)
             return LAB_OK;
@@ -830,7 +834,7 @@ namespace lab
         const unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(n, WARPS),
                                                           (int64_t)num_sms() * occ);
         LAB_LAUNCH((k_hash_gemm<MODE, HS, WARPS>), grid, 32 * WARPS, smem, s, Ar, Br, rows, n,
-                   counts, out_rp, out_ci, out_v, ovf_rows, n_ovf);
+                   counts, out_rp, out_ci, out_v, ovf_rows, n_ovf, n_dev);
         return LAB_OK;
     }
 
@@ -967,35 +971,42 @@ namespace lab
             LAB_TRY(launch_hash_classes<0>(gs, Ar, Br, counts.get(), nullptr, nullptr, nullptr,
                                            ovf_rows.get(), novf_d.get(), f));
         }
-        int novf = 0;
         if(gs.count(4))
-            LAB_TRY(copy_d2h_sync(&novf, novf_d.get(), sizeof(int), s));
-        if(novf)
         {
-            // rows that filled 3/4 of the 1024-slot table: 4096 slots, then global sort
-            LAB_TRY(ovf2_rows.alloc((size_t)novf, s));
-            LAB_TRY((launch_hash_cls<0, 4096, 4>(Ar, Br, ovf_rows.get(), novf, counts.get(), nullptr,
-                                                 nullptr, nullptr, ovf2_rows.get(),
-                                                 novf_d.get() + 1, s)));
-            int novf2 = 0;
-            LAB_TRY(copy_d2h_sync(&novf2, novf_d.get() + 1, sizeof(int), s));
-            if(novf2)
-            {
-                esc_tiers tg;
-                LAB_TRY(tiers_for_rows(ovf2_rows.get(), novf2, upper.get(), tg, s));
-                LAB_TRY((esc_run<exp_gemm, 0>(e, m, tg, counts.get(), nullptr, nullptr, s)));
-            }
+            // rows that filled 3/4 of the 1024-slot table get 4096 slots; their number
+            // is read on the device (a launch over the list's capacity), so no host
+            // round trip.  Rows that fill that one too (rare) are found at the sync
+            // below and go to the global sort tier.
+            LAB_TRY(ovf2_rows.alloc((size_t)gs.count(4), s));
+            LAB_TRY((launch_hash_cls<0, 4096, 4>(Ar, Br, ovf_rows.get(), gs.count(4), counts.get(),
+                                                 nullptr, nullptr, nullptr, ovf2_rows.get(),
+                                                 novf_d.get() + 1, s, novf_d.get())));
+            LAB_CUDA(cudaMemcpyAsync(hp + 32, novf_d.get() + 1, sizeof(int), cudaMemcpyDeviceToHost,
+                                     s));
         }
+        else
+            hp[32] = 0;
 
         // ---- row pointer and allocation
         LAB_TRY(rp.alloc((size_t)m + 1, s));
-        LAB_TRY(counts_to_rowptr(counts.get(), rp.get(), m, nullptr, s));
-        // the numeric classes (by exact count) are counted before the one sync that
-        // reads the nonzero total
-        LAB_TRY(gemm_class_count(1, upper.get(), rp.get(), m, dh.get() + 2 * kHashClasses,
-                                 hp + 16, s));
         int32_t nnz32 = 0;
-        LAB_TRY(copy_d2h_sync(&nnz32, rp.get() + m, sizeof(int32_t), s));
+        for(int pass = 0; pass < 2; pass++)
+        {
+            LAB_TRY(counts_to_rowptr(counts.get(), rp.get(), m, nullptr, s));
+            // the numeric classes (by exact count) are counted before the one sync
+            // that reads the nonzero total (and the 4096-slot overflow count)
+            LAB_TRY(gemm_class_count(1, upper.get(), rp.get(), m, dh.get() + 2 * kHashClasses,
+                                     hp + 16, s));
+            LAB_TRY(copy_d2h_sync(&nnz32, rp.get() + m, sizeof(int32_t), s));
+            const int novf2 = hp[32];
+            if(pass == 1 || novf2 == 0)
+                break;
+            // the global sort tier fills in the counts of the rows that overflowed,
+            // then the scan runs again
+            esc_tiers tg;
+            LAB_TRY(tiers_for_rows(ovf2_rows.get(), novf2, upper.get(), tg, s));
+            LAB_TRY((esc_run<exp_gemm, 0>(e, m, tg, counts.get(), nullptr, nullptr, s)));
+        }
         if(nnz32 < 0)
         {
             set_error("nonzero count exceeds int32 range");
