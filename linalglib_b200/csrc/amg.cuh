@@ -45,6 +45,8 @@ namespace lab
     };
 
     lab_status hierarchy_release(hierarchy_impl* h);
+    // SpMV schedules of the coarse levels (after a setup or a load).
+    lab_status hierarchy_plans(hierarchy_impl* h, cudaStream_t s);
 
     // pieces (amg_setup.cu)
     lab_status amg_strength(const lab_csr_impl* A, double eps, int32_t* conn, cudaStream_t s);

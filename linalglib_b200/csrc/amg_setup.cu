@@ -1245,6 +1245,32 @@ namespace lab
 
     // saamg_setup (saamg.cpp:210-282), uaamg_setup (uaamg.cpp:131-224),
     // rsamg_setup (rsamg.cpp:869-947)
+    // Row schedules of the coarse levels.  Few rows leave little to spread over the
+    // GPU, so small levels take more lanes per long row (the autotuner's choice on
+    // the SA hierarchies measured), and the smallest ones the plain VECTOR kernel
+    // instead of the staged one (whose tile set-up dominates there).  Level 0 keeps
+    // the CSR-order schedule of the caller's matrix.  Built and loaded hierarchies
+    // both get these plans, so they run identical cycles.
+    lab_status hierarchy_plans(hierarchy_impl* h, cudaStream_t s)
+    {
+        for(int l = 1; l <= h->levels; l++)
+        {
+            lab_csr_impl* Al = h->A[l];
+            LAB_TRY(spmv_analyse(Al, s));
+            spmv_plan& p = Al->plan;
+            if(p.forced || Al->m == 0)
+                continue;
+            if(Al->m <= 16)
+            {
+                p.alg   = LAB_SPMV_VECTOR;
+                p.lanes = p.max_row > 4 ? 32 : 4;
+            }
+            else if(Al->m < 1024 && p.alg == LAB_SPMV_VECTOR)
+                p.lanes = std::min(32, 2 * p.vlanes);
+        }
+        return LAB_OK;
+    }
+
     static lab_status amg_setup(int kind, const lab_csr_impl* A0, int max_level,
                                 hierarchy_impl* h, cudaStream_t s)
     {
@@ -1311,7 +1337,7 @@ namespace lab
             eps *= 0.5;
         }
         h->levels = level;
-        return LAB_OK;
+        return hierarchy_plans(h, s);
     }
 }
 

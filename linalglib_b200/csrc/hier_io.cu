@@ -214,6 +214,8 @@ LAB_API lab_status lab_hierarchy_load(const char* path, lab_hierarchy* out, lab_
             st = LAB_BAD_ARG;
         }
     }
+    if(st == LAB_OK)
+        st = hierarchy_plans(h, s);
     if(st != LAB_OK)
     {
         hierarchy_release(h);
