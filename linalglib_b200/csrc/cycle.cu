@@ -36,6 +36,20 @@ namespace lab
             r[i] = b[i] - s;
             return 0.0;
         }
+        struct pre_t
+        {
+            T b, invd;
+        };
+        __device__ __forceinline__ pre_t pre(int i) const
+        {
+            return {__ldg(b + i), __ldg(invd + i)};
+        }
+        __device__ __forceinline__ double finish(int i, T s, const pre_t& p) const
+        {
+            x[i] = omega * (p.invd * p.b);
+            r[i] = p.b - s;
+            return 0.0;
+        }
     };
 
     // Weighted Jacobi sweep y = x + omega D^-1 (b - A x); with DOT returns y_i dv_i.
@@ -62,6 +76,20 @@ namespace lab
             y[i] = yi;
             return DOT ? (double)yi * (double)dv[i] : 0.0;
         }
+        struct pre_t
+        {
+            T x, b, invd, dv;
+        };
+        __device__ __forceinline__ pre_t pre(int i) const
+        {
+            return {__ldg(x + i), __ldg(b + i), __ldg(invd + i), DOT ? __ldg(dv + i) : T(0)};
+        }
+        __device__ __forceinline__ double finish(int i, T s, const pre_t& p) const
+        {
+            T yi = p.x + omega * (p.invd * (p.b - s));
+            y[i] = yi;
+            return DOT ? (double)yi * (double)p.dv : 0.0;
+        }
     };
 
     template <class VT, class T>
@@ -81,6 +109,16 @@ namespace lab
         __device__ __forceinline__ double finish(int i, T s) const
         {
             r[i] = b[i] - s;
+            return 0.0;
+        }
+        using pre_t = T; // b_i
+        __device__ __forceinline__ T pre(int i) const
+        {
+            return __ldg(b + i);
+        }
+        __device__ __forceinline__ double finish(int i, T s, T bi) const
+        {
+            r[i] = bi - s;
             return 0.0;
         }
     };
@@ -106,6 +144,21 @@ namespace lab
             T yi = x[i] + s;
             y[i] = yi;
             return DOT ? (double)yi * (double)dv[i] : 0.0;
+        }
+        // (x may alias y, but only row i itself writes y_i, after this load)
+        struct pre_t
+        {
+            T x, dv;
+        };
+        __device__ __forceinline__ pre_t pre(int i) const
+        {
+            return {x[i], DOT ? __ldg(dv + i) : T(0)};
+        }
+        __device__ __forceinline__ double finish(int i, T s, const pre_t& p) const
+        {
+            T yi = p.x + s;
+            y[i] = yi;
+            return DOT ? (double)yi * (double)p.dv : 0.0;
         }
     };
 
@@ -133,6 +186,18 @@ namespace lab
             y[i] = s;
             if(x0)
                 x0[i] = omega * (__ldg(invd_c + i) * s);
+            return 0.0;
+        }
+        using pre_t = T; // D_c^-1 of row i (when x0 is written)
+        __device__ __forceinline__ T pre(int i) const
+        {
+            return x0 ? __ldg(invd_c + i) : T(0);
+        }
+        __device__ __forceinline__ double finish(int i, T s, T di) const
+        {
+            y[i] = s;
+            if(x0)
+                x0[i] = omega * (di * s);
             return 0.0;
         }
     };

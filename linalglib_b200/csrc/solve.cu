@@ -277,6 +277,16 @@ namespace lab
             q[i] = s;
             return p[i] * s;
         }
+        using pre_t = double; // p_i
+        __device__ __forceinline__ double pre(int i) const
+        {
+            return __ldg(p + i);
+        }
+        __device__ __forceinline__ double finish(int i, double s, double pi) const
+        {
+            q[i] = s;
+            return pi * s;
+        }
     };
 
     // Initial state: gamma = gnew, flags, r0 == 0 short cut.

@@ -9,6 +9,11 @@
 //                             deterministically over the grid into red.out
 //   acc_t gather(int col)     the x value for a column (may be computed on the fly)
 //   double finish(int row, acc_t s)   epilogue with s = sum_j a_ij x_j in CSR order
+//   Op::pre_t, pre_t pre(int row), double finish(int row, acc_t s, const pre_t&)
+//                             (optional) the row's own epilogue operands (b_i,
+//                             D^-1_i, x_i, ...) loaded before its entries, so their
+//                             round trip overlaps the gathers instead of following
+//                             the reduction; same arithmetic as finish(row, s)
 //
 // Two schedules, picked per matrix by lab_spmv_analysis:
 //   ROWSEQ  one thread per row, CSR order (k_pipe): a persistent CTA streams
@@ -80,6 +85,40 @@ namespace lab
     __device__ __forceinline__ double to_acc(float v, double)
     {
         return (double)v;
+    }
+
+    struct no_pre
+    {
+    };
+    template <class Op, class = void>
+    struct op_pre
+    {
+        using type = no_pre;
+    };
+    template <class Op>
+    struct op_pre<Op, std::void_t<typename Op::pre_t>>
+    {
+        using type = typename Op::pre_t;
+    };
+    template <class Op>
+    using pre_of = typename op_pre<Op>::type;
+
+    template <class Op>
+    __device__ __forceinline__ pre_of<Op> pre_load(const Op& op, int row)
+    {
+        if constexpr(std::is_same<pre_of<Op>, no_pre>::value)
+            return no_pre{};
+        else
+            return op.pre(row);
+    }
+    template <class Op>
+    __device__ __forceinline__ double finish_with(const Op& op, int row, typename Op::acc_t s,
+                                                  const pre_of<Op>& p)
+    {
+        if constexpr(std::is_same<pre_of<Op>, no_pre>::value)
+            return op.finish(row, s);
+        else
+            return op.finish(row, s, p);
     }
 
     template <bool FMA>
@@ -197,8 +236,9 @@ namespace lab
             const int            row    = r0 + threadIdx.x;
             if(row < r1)
             {
-                const int a = sr[row - r0], b = sr[row - r0 + 1];
-                AT        s = AT(0);
+                const pre_of<Op> pr = pre_load(op, row);
+                const int        a = sr[row - r0], b = sr[row - r0 + 1];
+                AT               s = AT(0);
                 if(MAXR > 0 && staged)
                 {
                     // gathers issued 16 at a time before their part of the chain,
@@ -231,7 +271,7 @@ namespace lab
                         s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)),
                                                op.gather(col_of<IT>(A.ci[j], row)), s);
                 }
-                contrib += op.finish(row, s);
+                contrib += finish_with(op, row, s, pr);
             }
             __syncthreads(); // this stage is refilled by the prefetch two tiles on
         }
@@ -304,8 +344,9 @@ namespace lab
             const int row = r0 + lane;
             if(row < r1)
             {
-                const int a = sr[lane], b = sr[lane + 1];
-                AT        s = AT(0);
+                const pre_of<Op> pr = pre_load(op, row);
+                const int        a = sr[lane], b = sr[lane + 1];
+                AT               s = AT(0);
                 if(staged)
                 {
                     constexpr int CH = 16;
@@ -330,7 +371,7 @@ namespace lab
                         s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)),
                                                op.gather(col_of<IT>(A.ci[j], row)), s);
                 }
-                contrib += op.finish(row, s);
+                contrib += finish_with(op, row, s, pr);
             }
             __syncwarp(); // the region is refilled by the warp's next tile
         }
@@ -357,8 +398,9 @@ namespace lab
         const int row     = blockIdx.x * NT + threadIdx.x;
         if(row < A.m)
         {
-            const int a = A.rp[row], b = A.rp[row + 1];
-            AT        s = AT(0);
+            const pre_of<Op> pr = pre_load(op, row);
+            const int        a = A.rp[row], b = A.rp[row + 1];
+            AT               s = AT(0);
             for(int c0 = a; c0 < b; c0 += kSegLen)
             {
                 AT vv[kSegLen], xv[kSegLen];
@@ -374,7 +416,7 @@ namespace lab
                     if(c0 + q < b)
                         s = acc_step<Op::kFma>(vv[q], xv[q], s);
             }
-            contrib = op.finish(row, s);
+            contrib = finish_with(op, row, s, pr);
         }
         if(Op::kReduce)
             reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
@@ -425,9 +467,12 @@ namespace lab
         using AT = typename Op::acc_t;
         if(red.skip && *red.skip)
             return;
-        const int lane = threadIdx.x & (W - 1);
-        const int row  = (int)(((int64_t)blockIdx.x * NT + threadIdx.x) / W);
-        AT        s    = AT(0);
+        const int  lane = threadIdx.x & (W - 1);
+        const int  row  = (int)(((int64_t)blockIdx.x * NT + threadIdx.x) / W);
+        AT         s    = AT(0);
+        pre_of<Op> pr{};
+        if(row < A.m && lane == 0)
+            pr = pre_load(op, row);
         if(row < A.m && sizeof(VT) == 8)
         {
             // FP64 values: one entry per lane step (a quad would need two loads anyway)
@@ -463,7 +508,7 @@ namespace lab
             s += __shfl_xor_sync(0xffffffffu, s, o, W);
         double contrib = 0.0;
         if(row < A.m && lane == 0)
-            contrib = op.finish(row, s);
+            contrib = finish_with(op, row, s, pr);
         if(Op::kReduce)
             reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
     }
@@ -655,6 +700,16 @@ namespace lab
             y[r] = beta == 0.0 ? __dmul_rn(alpha, s) : fma(alpha, s, __dmul_rn(beta, y[r]));
             return 0.0;
         }
+        using pre_t = double; // y_r (read only when beta != 0)
+        __device__ __forceinline__ double pre(int r) const
+        {
+            return beta == 0.0 ? 0.0 : y[r];
+        }
+        __device__ __forceinline__ double finish(int r, double s, double yr) const
+        {
+            y[r] = beta == 0.0 ? __dmul_rn(alpha, s) : fma(alpha, s, __dmul_rn(beta, yr));
+            return 0.0;
+        }
     };
 
     struct op_residual
@@ -673,6 +728,16 @@ namespace lab
         __device__ __forceinline__ double finish(int i, double s) const
         {
             r[i] = __dsub_rn(b[i], s);
+            return 0.0;
+        }
+        using pre_t = double; // b_i
+        __device__ __forceinline__ double pre(int i) const
+        {
+            return __ldg(b + i);
+        }
+        __device__ __forceinline__ double finish(int i, double s, double bi) const
+        {
+            r[i] = __dsub_rn(bi, s);
             return 0.0;
         }
     };
