@@ -280,6 +280,26 @@ namespace lab
             reduce_finish_sum<256>(acc, partial, counter, out);
     }
 
+    // (z, r) and (z, q) with z = (double) x, each summed as k_f2d_dot and
+    // k_red_dev<0> sum theirs (the flexible-PCG step of the reduced-precision
+    // preconditioner; z itself is never written).
+    __global__ void __launch_bounds__(256)
+        k_f2d_dot2(const float* __restrict__ x, const double* __restrict__ r,
+                   const double* __restrict__ q, int64_t n, red_buf zr, red_buf zq)
+    {
+        if(zr.skip && *zr.skip)
+            return;
+        double a1 = 0.0, a2 = 0.0;
+        for(int64_t i = blockIdx.x * 256ll + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256)
+        {
+            double zi = (double)x[i];
+            a1 += zi * r[i];
+            a2 = a2 + zi * q[i];
+        }
+        reduce_finish_sum<256>(a1, zr.partial, zr.counter, zr.out);
+        reduce_finish_sum<256>(a2, zq.partial, zq.counter, zq.out);
+    }
+
     // x += (double) e
     __global__ void k_add_f2d(const float* __restrict__ e, double* __restrict__ x, int64_t n)
     {
@@ -1112,6 +1132,24 @@ namespace lab
     }
 
     // ================================================================ entry points
+    // The reduced-precision cycle on r: x (FP32, the level-0 workspace) = cycle(0; fp32(r)).
+    static lab_status cycle_lowp(hierarchy_impl* h, const cyc_ctx& c, const double* r)
+    {
+        level_ws&              w = h->ws[0];
+        const int64_t          m = h->A[0]->m;
+        const lab_amg_options* o = c.o;
+        if(h->levels > 0 && o->smoother == LAB_SMOOTH_JACOBI && o->n1 >= 1)
+        {
+            float* x0 = cycle_start<float>(h, 0, o->cycle, w.xf, o);
+            LAB_LAUNCH(k_d2f_x0, grid_for(m), 256, 0, c.s, r, w.bf, lv<float>::invd(h->A[0]),
+                       (float)o->omega, x0, m, c.skip);
+            return cycle<float>(h, 0, o->cycle, w.xf, (const float*)w.bf, true, c, red_buf(),
+                                nullptr, true);
+        }
+        LAB_LAUNCH(k_d2f, grid_for(m), 256, 0, c.s, r, w.bf, m, c.skip);
+        return cycle<float>(h, 0, o->cycle, w.xf, (const float*)w.bf, true, c);
+    }
+
     lab_status cycle_precond(hierarchy_impl* h, const cyc_ctx& c, const double* r, double* z,
                              red_buf dot)
     {
@@ -1122,24 +1160,22 @@ namespace lab
             return cycle<double>(h, 0, c.o->cycle, z, r, true, c);
         }
         // Reduced precision: r -> fp32, FP32 cycle, z = fp64(x) with (z, r) fused.
-        level_ws&              w = h->ws[0];
-        const int64_t          m = h->A[0]->m;
-        const lab_amg_options* o = c.o;
-        if(h->levels > 0 && o->smoother == LAB_SMOOTH_JACOBI && o->n1 >= 1)
-        {
-            float* x0 = cycle_start<float>(h, 0, o->cycle, w.xf, o);
-            LAB_LAUNCH(k_d2f_x0, grid_for(m), 256, 0, c.s, r, w.bf, lv<float>::invd(h->A[0]),
-                       (float)o->omega, x0, m, c.skip);
-            LAB_TRY(cycle<float>(h, 0, o->cycle, w.xf, (const float*)w.bf, true, c, red_buf(),
-                                 nullptr, true));
-        }
-        else
-        {
-            LAB_LAUNCH(k_d2f, grid_for(m), 256, 0, c.s, r, w.bf, m, c.skip);
-            LAB_TRY(cycle<float>(h, 0, o->cycle, w.xf, (const float*)w.bf, true, c));
-        }
-        LAB_LAUNCH(k_f2d_dot, red_grid(m), 256, 0, c.s, (const float*)w.xf, r, z, m, dot.partial,
-                   dot.counter, dot.out, c.skip);
+        LAB_TRY(cycle_lowp(h, c, r));
+        const int64_t m = h->A[0]->m;
+        LAB_LAUNCH(k_f2d_dot, red_grid(m), 256, 0, c.s, (const float*)h->ws[0].xf, r, z, m,
+                   dot.partial, dot.counter, dot.out, c.skip);
+        return LAB_OK;
+    }
+
+    lab_status cycle_precond_flex(hierarchy_impl* h, const cyc_ctx& c, const double* r,
+                                  const double* q, red_buf zr, red_buf zq, const float** z32)
+    {
+        LAB_TRY(cycle_lowp(h, c, r));
+        const int64_t m = h->A[0]->m;
+        zr.skip         = c.skip;
+        LAB_LAUNCH(k_f2d_dot2, red_grid(m), 256, 0, c.s, (const float*)h->ws[0].xf, r, q, m, zr,
+                   zq);
+        *z32 = h->ws[0].xf;
         return LAB_OK;
     }
 

@@ -22,6 +22,11 @@ namespace lab
     // With dot.out set, also (z, r) -> dot.out.  Enqueue only (capturable).
     lab_status cycle_precond(hierarchy_impl* h, const cyc_ctx& c, const double* r, double* z,
                              red_buf dot);
+    // Reduced-precision preconditioner step of flexible PCG: the FP32 cycle on r,
+    // (z, r) into zr.out and (z, q) into zq.out with z = fp64 of the cycle's result,
+    // which stays in FP32 in the level-0 workspace (*z32; valid until the next cycle).
+    lab_status cycle_precond_flex(hierarchy_impl* h, const cyc_ctx& c, const double* r,
+                                  const double* q, red_buf zr, red_buf zq, const float** z32);
 
     // x <- cycle(x; b) on level 0 (stationary iteration step).  FP64 cycles run in
     // place; reduced-precision cycles run in correction form x += cycle(0; b - A x).

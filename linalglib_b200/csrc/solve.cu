@@ -232,16 +232,20 @@ namespace lab
     // is not exactly the same symmetric operator at every application (a V-cycle
     // rounded to FP32 / BF16).  With a fixed SPD preconditioner both choices agree
     // in exact arithmetic.
-    template <bool FLEX>
+    // ZT = float: z is the reduced-precision cycle's FP32 result, widened exactly.
+    template <bool FLEX, class ZT = double>
     __global__ void __launch_bounds__(256)
-        k_pcg_pupdate(int64_t n, double* __restrict__ p, const double* __restrict__ z, double* sc,
+        k_pcg_pupdate(int64_t n, double* __restrict__ p, const ZT* __restrict__ z, double* sc,
                       int* flags, unsigned int* counter)
     {
         if(flags[F_DONE])
             return;
         const double beta = FLEX ? -(sc[S_ZQ] / sc[S_PQ]) : sc[S_GNEW] / sc[S_GAMMA];
         for(int64_t i = blockIdx.x * 256ll + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256)
-            p[i] = beta == 0.0 ? z[i] : __dadd_rn(z[i], __dmul_rn(beta, p[i]));
+        {
+            const double zi = (double)z[i];
+            p[i]            = beta == 0.0 ? zi : __dadd_rn(zi, __dmul_rn(beta, p[i]));
+        }
         if(grid_ticket(counter))
         {
             if(threadIdx.x == 0)
@@ -381,16 +385,21 @@ namespace lab
         LAB_LAUNCH(k_pcg_update, red_grid(A->m), 256, 0, s, A->m, x, w->r, (const double*)w->p,
                    (const double*)w->q, w->sc, w->flags, w->partial + w->partial_n,
                    w->counters + 1);
-        LAB_TRY(precond_apply(M, w->r, w->z, s, skip, rbuf(w, 2, w->sc + S_GNEW, skip)));
         if(pcg_flexible(M))
         {
-            LAB_TRY(dot_device(A->m, w->z, w->q, rbuf(w, 5, w->sc + S_ZQ, skip), s));
-            LAB_LAUNCH(k_pcg_pupdate<true>, red_grid(A->m), 256, 0, s, A->m, w->p,
-                       (const double*)w->z, w->sc, w->flags, w->counters + 3);
+            // FP32 cycle, then (z, r) and (z, q) in one pass over its FP32 result,
+            // which p = z + beta p reads directly (no FP64 copy of z)
+            cyc_ctx      c{&M->o, s, skip};
+            const float* z32 = nullptr;
+            LAB_TRY(cycle_precond_flex(M->h, c, w->r, w->q, rbuf(w, 2, w->sc + S_GNEW, skip),
+                                       rbuf(w, 5, w->sc + S_ZQ, skip), &z32));
+            LAB_LAUNCH((k_pcg_pupdate<true, float>), red_grid(A->m), 256, 0, s, A->m, w->p, z32,
+                       w->sc, w->flags, w->counters + 3);
+            return LAB_OK;
         }
-        else
-            LAB_LAUNCH(k_pcg_pupdate<false>, red_grid(A->m), 256, 0, s, A->m, w->p,
-                       (const double*)w->z, w->sc, w->flags, w->counters + 3);
+        LAB_TRY(precond_apply(M, w->r, w->z, s, skip, rbuf(w, 2, w->sc + S_GNEW, skip)));
+        LAB_LAUNCH(k_pcg_pupdate<false>, red_grid(A->m), 256, 0, s, A->m, w->p,
+                   (const double*)w->z, w->sc, w->flags, w->counters + 3);
         return LAB_OK;
     }
 
