@@ -958,6 +958,318 @@ namespace lab
         return LAB_OK;
     }
 
+    // ================================================================ fused tail
+    // The last levels of a V-cycle with Jacobi smoothing from a zero guess hold a
+    // few hundred rows each, so their passes (restriction, residual, smoothing,
+    // prolongation, the coarsest solve) cost launch and round-trip latency, not
+    // bandwidth.  One CTA runs them all, from the restriction out of the entry
+    // level p to the prolongation back into it, passes separated by block
+    // barriers.  Each row is summed in its operator's schedule order (CSR order
+    // for the one-thread-per-row plan, k_vector's lane order and xor tree for W
+    // lanes), with the ops' own epilogue arithmetic, so the result equals the
+    // per-pass launches bit for bit.  Vectors written inside the kernel are read
+    // with plain (coherent) loads.
+    constexpr int kTailMax = 8;
+    constexpr int kTailNT  = 1024;
+
+    struct tail_mat
+    {
+        const int32_t* rp;
+        const int32_t* ci;
+        const int16_t* dc; // col - row (reduced precision), or null
+        const void*    v;
+        int            m;
+        int            W; // 1: CSR order; else lanes per row
+    };
+    struct tail_lvl
+    {
+        tail_mat    A, R, P; // R, P: to / from the next level
+        const void* invd;
+        void *      x, *t, *b, *r;
+    };
+    struct tail_args
+    {
+        tail_mat      Rp, Pp;
+        const void*   wr;  // level-p residual
+        const void*   cur; // level-p iterate
+        void*         dst; // level-p corrected iterate
+        tail_lvl      lv[kTailMax];
+        int           nl; // levels p+1 .. L; lv[nl - 1] is the coarsest
+        int           n1, n2;
+        double        omega;
+        const double* a11;  // coarsest 1x1: its value
+        const double* ainv; // coarsest n x n: dense inverse
+        int           nc;
+        const int*    skip;
+    };
+
+    template <class T>
+    __device__ __forceinline__ T tail_row(const tail_mat& M, int row, int lane, const T* x,
+                                          bool valid)
+    {
+        T s = T(0);
+        if(valid)
+        {
+            const int a = __ldg(M.rp + row), b = __ldg(M.rp + row + 1);
+            const T*  v = static_cast<const T*>(M.v);
+            if(M.W == 1)
+            {
+                for(int j = a; j < b; j++)
+                {
+                    const int c = M.dc ? col_of<int16_t>(__ldg(M.dc + j), row) : __ldg(M.ci + j);
+                    s           = acc_step<true>(__ldg(v + j), x[c], s);
+                }
+            }
+            else if constexpr(sizeof(T) == 8)
+            {
+                for(int j = a + lane; j < b; j += M.W)
+                    s = acc_step<true>(__ldg(v + j), x[__ldg(M.ci + j)], s);
+            }
+            else
+            {
+                for(int q = (a & ~3) + 4 * lane; q < b; q += 4 * M.W)
+                {
+                    T   v4[4];
+                    int c4[4];
+                    ld4(v + q, v4);
+                    if(M.dc)
+                    {
+                        int16_t d4[4];
+                        ld4(M.dc + q, d4);
+#pragma unroll
+                        for(int t = 0; t < 4; t++)
+                            c4[t] = col_of<int16_t>(d4[t], row);
+                    }
+                    else
+                        ld4(M.ci + q, c4);
+                    T xg[4];
+#pragma unroll
+                    for(int t = 0; t < 4; t++)
+                        if(q + t >= a && q + t < b)
+                            xg[t] = x[c4[t]];
+#pragma unroll
+                    for(int t = 0; t < 4; t++)
+                        if(q + t >= a && q + t < b)
+                            s = acc_step<true>(v4[t], xg[t], s);
+                }
+            }
+        }
+        if(M.W > 1)
+            for(int o = M.W / 2; o > 0; o >>= 1)
+                s += __shfl_xor_sync(0xffffffffu, s, o, M.W);
+        return s;
+    }
+
+    // One pass of M over x: fin(row, s) for every row, then a block barrier.
+    template <class T, class F>
+    __device__ __forceinline__ void tail_pass(const tail_mat& M, const T* x, F&& fin)
+    {
+        const int W = M.W, per = kTailNT / W;
+        for(int base = 0; base < M.m; base += per) // same trip count in every thread
+        {
+            const int  row   = base + (int)threadIdx.x / W;
+            const int  lane  = (int)threadIdx.x & (W - 1);
+            const bool valid = row < M.m;
+            const T    sum   = tail_row<T>(M, row, lane, x, valid);
+            if(valid && lane == 0)
+                fin(row, sum);
+        }
+        __syncthreads();
+    }
+
+    template <class T>
+    __global__ void __launch_bounds__(kTailNT) k_tail(tail_args a)
+    {
+        if(a.skip && *a.skip)
+            return;
+        const T om = (T)a.omega;
+        T*      cur[kTailMax];
+        T*      oth[kTailMax];
+        // weighted Jacobi sweep y = x + omega D^-1 (b - A x) (op_jacobi)
+        auto jacobi = [&](const tail_lvl& L, const T* x, T* y) {
+            const T* invd = static_cast<const T*>(L.invd);
+            const T* b    = static_cast<const T*>(L.b);
+            tail_pass<T>(L.A, x, [&](int i, T s) {
+                T yi = x[i] + om * (__ldg(invd + i) * (b[i] - s));
+                y[i] = yi;
+            });
+        };
+        // b_{k} = R r; x_{k} = omega D_k^-1 b_{k} when level k is not the coarsest
+        // (op_restrict with the fused first sweep)
+        auto restrict_into = [&](const tail_mat& R, const T* r, int k) {
+            const tail_lvl& C    = a.lv[k];
+            T*              b    = static_cast<T*>(C.b);
+            T*              x0   = k < a.nl - 1 ? static_cast<T*>(C.x) : nullptr;
+            const T*        invd = static_cast<const T*>(C.invd);
+            tail_pass<T>(R, r, [&](int i, T s) {
+                b[i] = s;
+                if(x0)
+                    x0[i] = om * (__ldg(invd + i) * s);
+            });
+        };
+
+        restrict_into(a.Rp, static_cast<const T*>(a.wr), 0);
+        for(int k = 0; k < a.nl - 1; k++)
+        {
+            const tail_lvl& L = a.lv[k];
+            cur[k]            = static_cast<T*>(L.x);
+            oth[k]            = static_cast<T*>(L.t);
+            for(int it = 1; it < a.n1; it++)
+            {
+                jacobi(L, cur[k], oth[k]);
+                T* tmp = cur[k];
+                cur[k] = oth[k];
+                oth[k] = tmp;
+            }
+            {
+                const T* b = static_cast<const T*>(L.b);
+                T*       r = static_cast<T*>(L.r);
+                tail_pass<T>(L.A, cur[k], [&](int i, T s) { r[i] = b[i] - s; });
+            }
+            restrict_into(L.R, static_cast<const T*>(L.r), k + 1);
+        }
+        {
+            // coarsest level: x = b / a (1x1) or x = Ainv b (k_coarse1, k_coarse_dense)
+            const tail_lvl& C = a.lv[a.nl - 1];
+            const T*        b = static_cast<const T*>(C.b);
+            T*              x = static_cast<T*>(C.x);
+            if(a.nc == 1)
+            {
+                if(threadIdx.x == 0)
+                    x[0] = (T)__ddiv_rn((double)b[0], a.a11[0]);
+            }
+            else
+            {
+                const int lane = threadIdx.x & 31;
+                for(int row = threadIdx.x >> 5; row < a.nc; row += kTailNT / 32)
+                {
+                    double s = 0.0;
+                    for(int k = lane; k < a.nc; k += 32)
+                        s = fma(__ldg(a.ainv + (size_t)row * a.nc + k), (double)b[k], s);
+                    s = warp_sum(s);
+                    if(lane == 0)
+                        x[row] = (T)s;
+                }
+            }
+            __syncthreads();
+            cur[a.nl - 1] = x;
+        }
+        for(int k = a.nl - 2; k >= 0; k--)
+        {
+            const tail_lvl& L = a.lv[k];
+            {
+                // x <- x + P e (op_prolong), into the other buffer
+                const T* x = cur[k];
+                T*       y = oth[k];
+                tail_pass<T>(L.P, cur[k + 1], [&](int i, T s) {
+                    T yi = x[i] + s;
+                    y[i] = yi;
+                });
+                oth[k] = cur[k];
+                cur[k] = y;
+            }
+            for(int it = 0; it < a.n2; it++)
+            {
+                jacobi(L, cur[k], oth[k]);
+                T* tmp = cur[k];
+                cur[k] = oth[k];
+                oth[k] = tmp;
+            }
+        }
+        {
+            const T* x = static_cast<const T*>(a.cur);
+            T*       y = static_cast<T*>(a.dst);
+            tail_pass<T>(a.Pp, cur[0], [&](int i, T s) {
+                T yi = x[i] + s;
+                y[i] = yi;
+            });
+        }
+    }
+
+    template <class T>
+    static tail_mat tail_mat_of(const lab_csr_impl* M)
+    {
+        tail_mat t;
+        t.rp = M->row_ptr;
+        t.ci = M->col_ind;
+        t.m  = (int)M->m;
+        // the W of launch_rowop's VECTOR dispatch (2, 4, 8, 16, else 32)
+        const int ln = M->plan.lanes;
+        t.W = M->plan.alg != LAB_SPMV_VECTOR ? 1 : (ln == 2 || ln == 4 || ln == 8 || ln == 16) ? ln : 32;
+        if constexpr(std::is_same<T, double>::value)
+        {
+            t.dc = nullptr;
+            t.v  = M->val;
+        }
+        else
+        {
+            t.dc = M->lp.dcol;
+            t.v  = M->lp.f32;
+        }
+        return t;
+    }
+
+    // Levels l+1 .. L form a fused tail when the cycle is a V-cycle with Jacobi
+    // smoothing (n1 >= 1) from a zero guess, level l's operators are not BF16,
+    // every operator below l is small (A: <= 1024 rows; A, R, P: <= 16384 entries,
+    // <= 4096 rows) and the coarsest level is solved by a 1x1 division or the
+    // dense inverse.
+    static bool tail_ok(const hierarchy_impl* h, const lab_amg_options* o, int l)
+    {
+        const int L = h->levels;
+        if(o->cycle != LAB_CYCLE_V || o->smoother != LAB_SMOOTH_JACOBI || o->n1 < 1 || l < 1 ||
+           l >= L || L - l > kTailMax || level_bf16(o, l))
+            return false;
+        auto small = [](const lab_csr_impl* M, int64_t rows) {
+            return M && M->m <= rows && M->nnz <= 16384 && M->plan.analysed;
+        };
+        for(int k = l; k < L; k++)
+            if(!small(h->R[k], 4096) || !small(h->P[k], 4096) || !small(h->A[k + 1], 1024))
+                return false;
+        const int64_t nc = h->A[L]->m;
+        return nc == 1 || (nc > 1 && o->coarse == LAB_COARSE_DIRECT && h->coarse_inv);
+    }
+
+    template <class T>
+    static lab_status tail_launch(hierarchy_impl* h, int l, const T* wr, const T* cur, T* dst,
+                                  const cyc_ctx& c)
+    {
+        const lab_amg_options* o = c.o;
+        tail_args              a{};
+        a.Rp  = tail_mat_of<T>(h->R[l]);
+        a.Pp  = tail_mat_of<T>(h->P[l]);
+        a.wr  = wr;
+        a.cur = cur;
+        a.dst = dst;
+        a.nl  = h->levels - l;
+        for(int k = 0; k < a.nl; k++)
+        {
+            const int  lk = l + 1 + k;
+            tail_lvl&  t  = a.lv[k];
+            level_ws&  w  = h->ws[lk];
+            t.A           = tail_mat_of<T>(h->A[lk]);
+            if(lk < h->levels)
+            {
+                t.R = tail_mat_of<T>(h->R[lk]);
+                t.P = tail_mat_of<T>(h->P[lk]);
+            }
+            t.invd = lv<T>::invd(h->A[lk]);
+            t.x    = lv<T>::x(w);
+            t.t    = lv<T>::t(w);
+            t.b    = lv<T>::b(w);
+            t.r    = lv<T>::r(w);
+        }
+        a.n1    = o->n1;
+        a.n2    = o->n2;
+        a.omega = o->omega;
+        a.nc    = (int)h->A[h->levels]->m;
+        a.a11   = (const double*)h->A[h->levels]->val;
+        a.ainv  = (const double*)h->coarse_inv;
+        a.skip  = c.skip;
+        LAB_LAUNCH(k_tail<T>, 1, kTailNT, 0, c.s, a);
+        return LAB_OK;
+    }
+
     // ================================================================ the recursion
     // cycle(l): x <- cycle(x; b) on level l.  kind 0 = V (amg.cpp:144-267),
     // 1 = W (269-390), 2 = F (392-513).  zero_guess: x enters as 0 (not read).
@@ -1072,6 +1384,14 @@ namespace lab
 
         // ---- restrict, recurse, correct
         auto coarse_correct = [&](bool cz, int ckind, bool last) -> lab_status {
+            if(cz && kind == 0 && ckind == 0 && !(last && dv) && tail_ok(h, o, l))
+            {
+                // restriction, levels l+1 .. L and the prolongation in one launch
+                T* dst = jac ? oth : cur;
+                LAB_TRY(tail_launch<T>(h, l, (const T*)wr, (const T*)cur, dst, c));
+                flip(dst);
+                return LAB_OK;
+            }
             // fuse the coarse level's first sweep from zero into the restriction
             const bool fuse_x0 = cz && jac && n1 >= 1 && l + 1 < h->levels;
             T*         x0      = fuse_x0 ? cycle_start<T>(h, l + 1, ckind, cx, o) : nullptr;
