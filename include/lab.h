@@ -98,9 +98,19 @@ LAB_API lab_status lab_csr_copy_to(lab_csr A, int32_t* row_ptr, int32_t* col_ind
                                    lab_memory where, lab_stream s);
 /* Deep copy (csr_matrix::copy_from, csr_matrix.cpp:153-168). */
 LAB_API lab_status lab_csr_clone(lab_csr A, lab_csr* B, lab_stream s);
-/* Values changed in place through lab_csr_device_arrays: drop cached diagonal /
- * reduced-precision copies. */
-LAB_API lab_status lab_csr_values_changed(lab_csr A);
+/* Values changed in place through lab_csr_device_arrays: the cached diagonal and
+ * reduced-precision copies are released on stream s (pass the stream the matrix
+ * was last used on) and the matrix takes a new identity, so solver graphs
+ * captured on the old values are captured again.  Preconditioners built earlier
+ * keep what they copied at build time, as the reference's build() does.  A
+ * hierarchy's own level matrices are not to be changed in place (set up again).
+ * The reference mutates through csr_matrix::get_row_ptr / get_col_ind / get_val
+ * (csr_matrix.h:175-185) and
+ * caches nothing. */
+LAB_API lab_status lab_csr_values_changed(lab_csr A, lab_stream s);
+/* Row pointers or column indices changed in place: lab_csr_values_changed plus
+ * the SpMV plan and the triangular-solve levels (rebuilt on next use). */
+LAB_API lab_status lab_csr_structure_changed(lab_csr A, lab_stream s);
 
 /* ------------------------------------------------------------------ SpMV */
 typedef enum lab_spmv_alg
@@ -165,10 +175,13 @@ LAB_API lab_status lab_jacobi_solve(int64_t n, const double* rhs, const double* 
 /* In-place exclusive prefix sums.  linalg_primitives.h:98 (host_primitives.cpp:76-91). */
 LAB_API lab_status lab_exclusive_scan_i64(int64_t n, int64_t* x, lab_stream s);
 LAB_API lab_status lab_exclusive_scan_i32(int64_t n, int32_t* x, lab_stream s);
-/* The int64 exclusive scan for callers that must not allocate device memory
- * during the call: its scratch is a fixed 512 KiB array in the library's device
- * image, so it calls no cudaMalloc / cudaFree and no allocating routine.  No
- * counterpart in the reference (it has no allocation-free variants).
+/* The int64 exclusive scan for callers that cannot allocate device memory
+ * during the call (a process whose other allocator holds nearly all of the
+ * device, a host thread that cannot wait on the driver's allocator, a fixed
+ * memory budget after start-up): its scratch is a fixed 512 KiB array in the
+ * library's device image, so it calls no cudaMalloc / cudaFree and no
+ * allocating routine.  No counterpart in the reference (it has no
+ * allocation-free variants).
  * Limit: n <= 134,217,728 elements; larger n returns LAB_BAD_ARG untouched.
  * The first call on each device looks up the array's device address (make
  * that first call before any stream capture).  All calls share the one array:
@@ -181,6 +194,16 @@ LAB_API lab_status lab_exclusive_scan_i64_noalloc(int64_t n, int64_t* x, lab_str
  * are computed on first use and kept with A; b and x may be the same array. */
 LAB_API lab_status lab_csrtrsv(lab_csr A, int lower, int unit_diag, const double* b, double* x,
                                lab_stream s);
+/* The bounded wait of the triangular solves on A (the lab_csrtrsv solves and the
+ * ILU / IC / Gauss-Seidel / SOR / SSOR preconditioner applications).  A row waits
+ * for its dependencies by polling; after idle_rounds rounds without progress
+ * (0: the default, 2^26) its warp gives up, the launch returns and the call
+ * reports LAB_TIMEOUT instead of hanging.  held_row >= 0 names a row whose value
+ * the solves never write, so the rows that depend on it run out of their wait:
+ * a test of that path (-1: none, the normal setting).  No reference counterpart
+ * (the reference's host solves are sequential loops, host_csrtrsv.cpp:36-90). */
+LAB_API lab_status lab_csrtrsv_wait_control(lab_csr A, int64_t idle_rounds, int64_t held_row,
+                                            lab_stream s);
 /* In-place incomplete factorizations of A's values: ILU(0) (csrilu0,
  * linalg_math.h:109; host_csrilu0.cpp) and IC(0) (csric0, linalg_math.h:95;
  * host_csric0.cpp, the upper part left unchanged).  The smallest column with a

@@ -65,7 +65,8 @@ _SIGS = {
     "lab_csr_device_arrays": [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p)],
     "lab_csr_copy_to": [_p, _p, _p, _p, _i, _p],
     "lab_csr_clone": [_p, C.POINTER(_p), _p],
-    "lab_csr_values_changed": [_p],
+    "lab_csr_values_changed": [_p, _p],
+    "lab_csr_structure_changed": [_p, _p],
     "lab_spmv_analysis": [_p, _p],
     "lab_spmv_set_algorithm": [_p, _i, _i],
     "lab_spmv_get_algorithm": [_p, C.POINTER(_i), C.POINTER(_i)],
@@ -100,6 +101,7 @@ _SIGS = {
     "lab_hierarchy_level": [_p, _i, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p)],
     "lab_hierarchy_setup_ms": [_p, C.POINTER(_d)],
     "lab_csrtrsv": [_p, _i, _i, _p, _p, _p],
+    "lab_csrtrsv_wait_control": [_p, _i64, _i64, _p],
     "lab_csrilu0": [_p, C.POINTER(_i), C.POINTER(_i), _p],
     "lab_csric0": [_p, C.POINTER(_i), C.POINTER(_i), _p],
     "lab_precond_create_ilu0": [_p, C.POINTER(_p), _p],

@@ -117,6 +117,16 @@ class CsrMatrix:
     def analyse(self):
         call("lab_spmv_analysis", self.h, stream_handle())
 
+    def set_values(self, v):
+        """Overwrite the stored values in place (same pattern) through the device
+        arrays, then tell the library so its cached copies are rebuilt."""
+        v = vec(v)
+        assert v.numel() == self.nnz
+        val = C.c_void_p()
+        call("lab_csr_device_arrays", self.h, None, None, C.byref(val))
+        call("lab_memcpy", val, ptr(v), 8 * v.numel(), stream_handle())
+        call("lab_csr_values_changed", self.h, stream_handle())
+
     def set_algorithm(self, alg, lanes=0):
         call("lab_spmv_set_algorithm", self.h, alg, lanes)
         self.analyse()

@@ -937,17 +937,40 @@ LAB_API lab_status lab_csr_clone(lab_csr A, lab_csr* B, lab_stream s)
                           s);
 }
 
-LAB_API lab_status lab_csr_values_changed(lab_csr A)
+LAB_API lab_status lab_csr_values_changed(lab_csr A, lab_stream ls)
 {
     LAB_ARG(A, "null matrix");
-    cudaDeviceSynchronize();
-    if(A->diag)
-        cudaFree(A->diag);
-    if(A->invdiag)
-        cudaFree(A->invdiag);
+    cudaStream_t s = to_stream(ls);
+    // stream-ordered: the cached arrays are released once the work already queued
+    // on s (the matrix's last users) has run
+    dfree(A->diag, s);
+    dfree(A->invdiag, s);
     A->diag    = nullptr;
     A->invdiag = nullptr;
-    lp_release(A);
+    dfree(A->lp.f32, s);
+    dfree(A->lp.bf16, s);
+    dfree(A->lp.invd32, s);
+    dfree(A->lp.dcol, s);
+    A->lp = csr_values_lp();
+    // a new identity: solver graphs captured on the old values (and on the cached
+    // arrays just released) no longer match and are captured again
+    A->uid = next_uid();
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_csr_structure_changed(lab_csr A, lab_stream ls)
+{
+    LAB_ARG(A, "null matrix");
+    LAB_TRY(lab_csr_values_changed(A, ls));
+    cudaStream_t s = to_stream(ls);
+    dfree(A->plan.block_row, s);
+    dfree(A->plan.merge_coords, s);
+    A->plan = spmv_plan();
+    if(A->tri)
+    {
+        LAB_CUDA(cudaStreamSynchronize(s));
+        tri_release(A);
+    }
     return LAB_OK;
 }
 

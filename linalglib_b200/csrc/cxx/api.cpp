@@ -453,7 +453,7 @@ namespace linalg
         {
             int32_t* p = nullptr;
             lab_csr_device_arrays(device(), &p, nullptr, nullptr);
-            lab_csr_values_changed(dev.get());
+            lab_csr_structure_changed(dev.get(), nullptr);
             return p;
         }
         sync_host();
@@ -467,7 +467,7 @@ namespace linalg
         {
             int32_t* p = nullptr;
             lab_csr_device_arrays(device(), nullptr, &p, nullptr);
-            lab_csr_values_changed(dev.get());
+            lab_csr_structure_changed(dev.get(), nullptr);
             return p;
         }
         sync_host();
@@ -481,7 +481,7 @@ namespace linalg
         {
             double* p = nullptr;
             lab_csr_device_arrays(device(), nullptr, nullptr, &p);
-            lab_csr_values_changed(dev.get());
+            lab_csr_values_changed(dev.get(), nullptr);
             return reinterpret_cast<T*>(p);
         }
         sync_host();

@@ -1,13 +1,12 @@
 // An entry point that allocates no memory: the exclusive scan with its
 // block-sum scratch in a fixed file-scope device array.
 //
-// Who needs it: callers that may not allocate device memory at the point of
-// the call -- code recording a CUDA graph that must not contain allocation
-// nodes, latency-critical host threads that cannot wait on the driver's
-// allocator, processes whose framework allocator has already reserved the
-// whole device so a cudaMalloc would fail, and deployments that forbid dynamic
-// device allocation after start-up.  Every other scan entry point takes its
-// scratch from the stream-ordered pool.
+// Who needs it: callers that cannot allocate device memory at the point of the
+// call.  A process whose framework allocator has already reserved nearly all of
+// the device has nothing left for a cudaMalloc; a latency-critical host thread
+// cannot wait on the driver's allocator, which may synchronise; a deployment
+// with a fixed memory budget forbids device allocation after start-up.  Every
+// other scan entry point takes its scratch from the stream-ordered pool.
 #include "internal.cuh"
 
 #include <mutex>

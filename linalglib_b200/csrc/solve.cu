@@ -19,7 +19,8 @@ namespace lab
         hierarchy_impl*  h    = nullptr;
         lab_amg_options  o;
         lab_csr_impl*    A    = nullptr; // the operator
-        double*          diag = nullptr; // Jacobi: the reference divides by the diagonal
+        double*          diag = nullptr; // Jacobi: own copy of the diagonal taken at build
+                                         // (jacobi_precond::build keeps its own, preconditioner.cpp:41-78)
         lab_csr_impl*    F    = nullptr; // kinds 2-5: factored / copied operator; SSOR: L
         lab_csr_impl*    G    = nullptr; // SSOR: U
         double*          y    = nullptr; // intermediate of the two solves (kinds 2, 3, 6)
@@ -32,6 +33,8 @@ namespace lab
                 csr_release(G);
             if(y)
                 cudaFree(y);
+            if(diag)
+                cudaFree(diag);
         }
     };
 
@@ -1548,8 +1551,22 @@ LAB_API lab_status lab_precond_create_jacobi(lab_csr A, lab_precond* out, lab_st
         delete M;
         return st;
     }
-    M->diag = A->diag;
-    *out    = M;
+    // a private copy: later value changes of A (lab_csr_values_changed frees and
+    // rebuilds A's cached diagonal) leave the built preconditioner as it was
+    st = dalloc(&M->diag, (size_t)A->m + 1, to_stream(s));
+    if(st == LAB_OK && A->m > 0)
+    {
+        cudaError_t e = cudaMemcpyAsync(M->diag, A->diag, sizeof(double) * A->m,
+                                        cudaMemcpyDeviceToDevice, to_stream(s));
+        if(e != cudaSuccess)
+            st = cuda_status(e, "jacobi diagonal copy", __FILE__, __LINE__);
+    }
+    if(st != LAB_OK)
+    {
+        delete M;
+        return st;
+    }
+    *out = M;
     return LAB_OK;
 }
 

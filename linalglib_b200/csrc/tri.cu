@@ -36,6 +36,10 @@ namespace lab
         int32_t*  ctl      = nullptr; // device: claim counter, error flag of the solves
         double*   scratch  = nullptr; // device: copy of b for in-place solves
         bool      all_diag = true;
+        // bounded wait: idle polling rounds before a warp gives up, and a row whose
+        // value the solves never write (-1: none; set only to test that path)
+        unsigned  idle_limit = 0;     // 0: kTriIdle
+        int       held_row   = -1;
     };
 
     void tri_release(lab_csr_impl* A)
@@ -396,7 +400,7 @@ namespace lab
     constexpr uint64_t kTriPending = 0x7ff4d1b0c0de0001ull; // signalling NaN
     constexpr int      kTriBlock   = 256;
     constexpr int      kTriPf      = 8;        // entries of a row held in registers
-    constexpr unsigned kTriIdle    = 1u << 26; // idle rounds before a warp gives up
+    constexpr unsigned kTriIdle    = 1u << 26; // default idle rounds before a warp gives up
 
     __device__ __forceinline__ uint64_t ld_relaxed(const double* p)
     {
@@ -461,13 +465,16 @@ namespace lab
     // Warps claim 32-row chunks of `order` (rows by level) from ctl[0]; each lane
     // polls the dependencies of its row's next entries at once, consumes the solved
     // prefix in order, and writes x_i when the row is done.  ctl[1] is the error
-    // flag, set when a warp waited kTriIdle rounds without progress.
+    // flag, set when a warp waited idle_limit rounds without progress; the other
+    // warps see it when they claim their next chunk or every 1024 idle rounds and
+    // return.  held (>= 0) is a row whose value is never written: the rows that
+    // depend on it can only run out of their wait (the test of this path).
     template <bool LOWER>
     __global__ void __launch_bounds__(kTriBlock)
         k_trsv(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                const double* __restrict__ v, const int32_t* __restrict__ order, int m, int unit,
                double dscale, const double* __restrict__ b, double* x, int32_t* ctl,
-               const int* skip)
+               const int* skip, unsigned idle_limit, int held)
     {
         if(skip && *skip)
             return;
@@ -532,7 +539,12 @@ namespace lab
                         blocked = !tri_entry<LOWER>(c, v[j], xc, i, unit, dscale, len, k, acc, d);
                     }
                     progress = k != k0;
-                    if(!blocked)
+                    if(!blocked && i == held)
+                    {
+                        done     = true; // x_i stays pending
+                        progress = true;
+                    }
+                    else if(!blocked)
                     {
                         st_relaxed(x + i,
                                    LOWER ? __ddiv_rn(__dsub_rn(bi, acc), d) : __ddiv_rn(acc, d));
@@ -546,7 +558,7 @@ namespace lab
                     idle = 0;
                 else
                 {
-                    if(++idle >= kTriIdle)
+                    if(++idle >= idle_limit)
                     {
                         if(lane == 0)
                             atomicExch(ctl + 1, 1);
@@ -585,14 +597,15 @@ namespace lab
         }
         LAB_LAUNCH(k_trsv_prep, (unsigned)std::min<int64_t>(ceil_div(m, 256), 4 * num_sms()), 256,
                    0, s, x, m, p.ctl, skip);
+        const unsigned idle = p.idle_limit ? p.idle_limit : kTriIdle;
         if(lower)
             LAB_LAUNCH(k_trsv<true>, trsv_grid(m), kTriBlock, 0, s, A->row_ptr, A->col_ind,
                        (const double*)A->val, (const int32_t*)p.lower.rows, m, (int)unit, dscale,
-                       b, x, p.ctl, skip);
+                       b, x, p.ctl, skip, idle, p.held_row);
         else
             LAB_LAUNCH(k_trsv<false>, trsv_grid(m), kTriBlock, 0, s, A->row_ptr,
                        A->col_ind, (const double*)A->val, (const int32_t*)p.upper.rows, m,
-                       (int)unit, 0.0, b, x, p.ctl, skip);
+                       (int)unit, 0.0, b, x, p.ctl, skip, idle, p.held_row);
         return LAB_OK;
     }
 
@@ -605,8 +618,9 @@ namespace lab
         if(e)
         {
             LAB_CUDA(cudaMemsetAsync(A->tri->ctl + 1, 0, sizeof(int32_t), s));
-            set_error("triangular solve: a row waited too long for its dependencies");
-            return LAB_CUDA_ERROR;
+            set_error("triangular solve: a row waited longer than the wait limit for its "
+                      "dependencies");
+            return LAB_TIMEOUT;
         }
         return LAB_OK;
     }
@@ -911,13 +925,28 @@ LAB_API lab_status lab_csrtrsv(lab_csr A, int lower, int unit_diag, const double
     return tri_check(A, to_stream(s));
 }
 
+LAB_API lab_status lab_csrtrsv_wait_control(lab_csr A, int64_t idle_rounds, int64_t held_row,
+                                            lab_stream s)
+{
+    LAB_ARG(A, "null matrix");
+    LAB_ARG(idle_rounds >= 0 && idle_rounds <= 0xffffffffll, "idle_rounds out of range");
+    LAB_ARG(held_row >= -1 && held_row < A->m, "held_row out of range");
+    LAB_TRY(ensure_init());
+    if(A->m == 0)
+        return LAB_OK;
+    LAB_TRY(tri_analyse(A, to_stream(s)));
+    A->tri->idle_limit = (unsigned)idle_rounds;
+    A->tri->held_row   = (int)held_row;
+    return LAB_OK;
+}
+
 LAB_API lab_status lab_csrilu0(lab_csr A, int* structural_zero, int* numeric_zero, lab_stream s)
 {
     LAB_ARG(A, "null matrix");
     LAB_ARG(A->m == A->n, "ILU(0) needs a square matrix");
     LAB_TRY(ensure_init());
     LAB_TRY(tri_factor(A, false, structural_zero, numeric_zero, to_stream(s)));
-    return lab_csr_values_changed(A);
+    return lab_csr_values_changed(A, s);
 }
 
 LAB_API lab_status lab_csric0(lab_csr A, int* structural_zero, int* numeric_zero, lab_stream s)
@@ -926,7 +955,7 @@ LAB_API lab_status lab_csric0(lab_csr A, int* structural_zero, int* numeric_zero
     LAB_ARG(A->m == A->n, "IC(0) needs a square matrix");
     LAB_TRY(ensure_init());
     LAB_TRY(tri_factor(A, true, structural_zero, numeric_zero, to_stream(s)));
-    return lab_csr_values_changed(A);
+    return lab_csr_values_changed(A, s);
 }
 
 } // extern "C"

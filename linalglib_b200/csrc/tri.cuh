@@ -21,7 +21,7 @@ namespace lab
     lab_status ssor_split(lab_csr_impl* A, double omega, lab_csr_impl** L, lab_csr_impl** U,
                           cudaStream_t s);
 
-    // Reads (and clears) the error flag of A's solves: LAB_CUDA_ERROR if a solve
+    // Reads (and clears) the error flag of A's solves: LAB_TIMEOUT if a solve
     // gave up waiting (synchronises the stream).
     lab_status tri_check(lab_csr_impl* A, cudaStream_t s);
 

@@ -25,11 +25,18 @@ _d = C.c_double
 _p = C.c_void_p
 
 
+def reference_root() -> str:
+    """Where the reference LinAlgLib sources are: $LINALGLIB_REF, else the
+    default location the Makefile uses (its REF variable)."""
+    return os.environ.get("LINALGLIB_REF", "/root/reference")
+
+
 def build(reference: bool = True) -> None:
     """Compile the oracle (and, where the reference sources exist, oracle/_ref)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if reference:
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={reference_root()}"],
+                       check=True)
 
 
 def _ptr(a):

@@ -127,6 +127,34 @@ def test_jacobi_pcg_matches_oracle(gpu, oracle, name):
     assert np.max(np.abs(x.cpu().numpy() - xo)) <= 1e-6 * np.max(np.abs(xo))
 
 
+def test_jacobi_precond_keeps_its_diagonal_after_values_change(gpu, oracle):
+    """jacobi_precond::build takes its own copy of the diagonal
+    (preconditioner.cpp:41-78): values changed in A afterwards leave it as built,
+    and the next solve on A sees the new values (the cached iteration graph of the
+    old values is not replayed).  With A <- 2A the old diagonal is twice the new
+    one; a constant scale of the preconditioner leaves CG's iterates unchanged, so
+    the solve must match the oracle's Jacobi-PCG on 2A."""
+    A = P.poisson2d(64)
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    M_old = gpu.Preconditioner.jacobi(dA)
+    ctl = gpu.iter_control(rel_tol=1e-8, abs_tol=0.0, max_iter=3000)
+    x0, info0 = gpu.pcg(dA, gpu.vec(b), M=M_old, control=ctl)
+    A2 = (A[0], A[1], 2.0 * A[2])
+    dA.set_values(A2[2])
+    x1, info1 = gpu.pcg(dA, gpu.vec(b), M=M_old, control=ctl)
+    xo, ito = oracle.cg(A2, b, jacobi=True, rel_tol=1e-8, abs_tol=0.0, max_iter=3000)
+    assert info0.converged == 1 and info1.converged == 1
+    assert abs(info1.iterations - ito) <= 2, (info1.iterations, ito)
+    x0, x1 = x0.cpu().numpy(), x1.cpu().numpy()
+    assert np.max(np.abs(x1 - xo)) <= 1e-6 * np.max(np.abs(xo))
+    assert np.max(np.abs(2.0 * x1 - x0)) <= 1e-6 * np.max(np.abs(x0))
+    # a preconditioner built after the change takes the new diagonal
+    x2, info2 = gpu.pcg(dA, gpu.vec(b), M=gpu.Preconditioner.jacobi(dA), control=ctl)
+    assert abs(info2.iterations - ito) <= 2
+    assert np.max(np.abs(x2.cpu().numpy() - xo)) <= 1e-6 * np.max(np.abs(xo))
+
+
 def test_plain_cg_restart_quirk(gpu, oracle):
     """No preconditioner: the reference restarts every iteration (cg.cpp:89)."""
     A = P.poisson2d(24)

@@ -181,3 +181,26 @@ def test_nonsymmetric_patterns_bit_exact(gpu, oracle, n, per_row, seed):
     for kind in (0, 1, 2, 3, 4):
         z = _precond(gpu, kind, dA).apply(gpu.vec(b)).cpu().numpy()
         assert np.array_equal(_bits(z), _bits(oracle.precond_apply(kind, A, b, omega=1.3))), kind
+
+
+@pytest.mark.parametrize("lower", [True, False])
+def test_trsv_bounded_wait_reports_timeout(gpu, oracle, lower):
+    """The solves poll for their dependencies with a bounded wait.  A held row
+    (its value never written) makes every row that depends on it run out of its
+    wait: the launch must return and the call report LAB_TIMEOUT, and the same
+    matrix must solve bit-exactly again once the hold is lifted."""
+    import ctypes as C
+    from linalglib_b200 import _lib as L
+    A = P.poisson3d(24)
+    m = A[0].size - 1
+    b = np.random.default_rng(4).uniform(-1, 1, m)
+    dA = gpu.CsrMatrix.from_arrays(*A[:3])
+    held = 0 if lower else m - 1  # the first row solved; every other row depends on it
+    L.call("lab_csrtrsv_wait_control", dA.h, 1 << 12, held, gpu.stream_handle())
+    bx, x = gpu.vec(b), gpu.vec(np.zeros(m))
+    st = L.lib().lab_csrtrsv(dA.h, int(lower), 0, gpu.ptr(bx), gpu.ptr(x), gpu.stream_handle())
+    assert st == L.LAB_TIMEOUT, L.lib().lab_last_error().decode()
+    assert "wait" in L.lib().lab_last_error().decode()
+    L.call("lab_csrtrsv_wait_control", dA.h, 0, -1, gpu.stream_handle())
+    x = dA.trsv(gpu.vec(b), lower=lower)
+    assert np.array_equal(_bits(x.cpu().numpy()), _bits(oracle.trsv(A, b, lower, False)))
