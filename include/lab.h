@@ -112,6 +112,26 @@ LAB_API lab_status lab_csr_values_changed(lab_csr A, lab_stream s);
  * the SpMV plan and the triangular-solve levels (rebuilt on next use). */
 LAB_API lab_status lab_csr_structure_changed(lab_csr A, lab_stream s);
 
+/* ------------------------------------------------------------------ Matrix Market
+ * Host-only file I/O (no device needed), behind csr_matrix::read_mtx / write_mtx.
+ *
+ * lab_mtx_read replaces csr_matrix::read_mtx (library/src/csr_matrix.cpp:523-729):
+ * coordinate files with real or integer values, general or symmetric (array,
+ * complex, pattern, hermitian and skew-symmetric files are refused with
+ * LAB_BAD_ARG, as the reference refuses them); symmetric files are mirrored;
+ * repeated entries are summed in the reference's order, so the CSR arrays are
+ * bit-identical to the reference's.  Files the reference would crash on (an
+ * unparsable entry, an index outside the stated size) are refused.  The three
+ * arrays are allocated with malloc; release each with lab_mtx_free. */
+LAB_API lab_status lab_mtx_read(const char* path, int64_t* m, int64_t* n, int64_t* nnz,
+                                int32_t** row_ptr, int32_t** col_ind, double** val);
+LAB_API void       lab_mtx_free(void* p);
+/* Replaces csr_matrix::write_mtx (csr_matrix.cpp:731-795): the same bytes (banner,
+ * comment line, sizes, one "row col value" line per entry, values "%.10f"). */
+LAB_API lab_status lab_mtx_write(const char* path, int64_t m, int64_t n, int64_t nnz,
+                                 const int32_t* row_ptr, const int32_t* col_ind,
+                                 const double* val);
+
 /* ------------------------------------------------------------------ SpMV */
 typedef enum lab_spmv_alg
 {

@@ -101,6 +101,9 @@ _SIGS = {
     "lab_hierarchy_level": [_p, _i, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p)],
     "lab_hierarchy_setup_ms": [_p, C.POINTER(_d)],
     "lab_csrtrsv": [_p, _i, _i, _p, _p, _p],
+    "lab_mtx_read": [_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_p),
+                     C.POINTER(_p), C.POINTER(_p)],
+    "lab_mtx_write": [_p, _i64, _i64, _i64, _p, _p, _p],
     "lab_csrtrsv_wait_control": [_p, _i64, _i64, _p],
     "lab_csrilu0": [_p, C.POINTER(_i), C.POINTER(_i), _p],
     "lab_csric0": [_p, C.POINTER(_i), C.POINTER(_i), _p],
@@ -161,6 +164,8 @@ def lib():
     L.lab_amg_options_default.argtypes = [C.POINTER(AmgOptions)]
     L.lab_iter_control_default.restype = None
     L.lab_iter_control_default.argtypes = [C.POINTER(IterControl)]
+    L.lab_mtx_free.restype = None
+    L.lab_mtx_free.argtypes = [_p]
     _lib = L
     return L
 
@@ -185,6 +190,35 @@ def call_solve(name, *args):
     if st in (LAB_NAN, LAB_BREAKDOWN):
         return st
     return check(st, name)
+
+
+def mtx_read(path):
+    """lab_mtx_read on the host: (row_ptr, col_ind, val, n) numpy arrays."""
+    L = lib()
+    m, n, z = C.c_int64(), C.c_int64(), C.c_int64()
+    rp, ci, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    call("lab_mtx_read", str(path).encode(), C.byref(m), C.byref(n), C.byref(z), C.byref(rp),
+         C.byref(ci), C.byref(v))
+    try:
+        import numpy as np
+        a = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int32)), shape=(m.value + 1,)).copy()
+        b = np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_int32)), shape=(max(z.value, 1),))
+        c = np.ctypeslib.as_array(C.cast(v, C.POINTER(C.c_double)), shape=(max(z.value, 1),))
+        return a, b[:z.value].copy(), c[:z.value].copy(), n.value
+    finally:
+        for p in (rp, ci, v):
+            L.lab_mtx_free(p)
+
+
+def mtx_write(path, rp, ci, v, n=None):
+    """lab_mtx_write of host CSR arrays."""
+    import numpy as np
+    rp = np.ascontiguousarray(rp, dtype=np.int32)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    m = rp.size - 1
+    call("lab_mtx_write", str(path).encode(), m, m if n is None else n, int(rp[-1]),
+         rp.ctypes.data, ci.ctypes.data, v.ctypes.data)
 
 
 def declared_symbols(header_path=None):

@@ -583,64 +583,26 @@ namespace linalg
             Trans.adopt(out, true);
     }
 
-    // Matrix Market coordinate real (general or symmetric), 1-based; rows are
-    // sorted by column and duplicate entries summed.
+    // Matrix Market I/O through the host routines of the C ABI (lab_mtx_read /
+    // lab_mtx_write, the reference's csr_matrix.cpp:523-795 behaviour).
     template <typename T>
     bool csr_matrix<T>::read_mtx(const std::string& filename)
     {
-        std::ifstream f(filename);
-        if(!f)
+        int64_t  M = 0, N = 0, Z = 0;
+        int32_t *rp = nullptr, *ci = nullptr;
+        double*  v  = nullptr;
+        if(lab_mtx_read(filename.c_str(), &M, &N, &Z, &rp, &ci, &v) != LAB_OK)
+        {
+            std::cerr << "Error: " << lab_last_error() << std::endl;
             return false;
-        std::string line;
-        std::getline(f, line);
-        bool symmetric = line.find("symmetric") != std::string::npos;
-        bool pattern   = line.find("pattern") != std::string::npos;
-        while(std::getline(f, line) && (line.empty() || line[0] == '%'))
-        {
         }
-        std::istringstream hdr(line);
-        long               M = 0, N = 0, Z = 0;
-        hdr >> M >> N >> Z;
-        std::vector<std::tuple<int, int, double>> e;
-        e.reserve(symmetric ? 2 * Z : Z);
-        for(long k = 0; k < Z; k++)
-        {
-            long   i, j;
-            double v = 1.0;
-            if(pattern)
-                f >> i >> j;
-            else
-                f >> i >> j >> v;
-            if(!f)
-                return false;
-            e.emplace_back((int)i - 1, (int)j - 1, v);
-            if(symmetric && i != j)
-                e.emplace_back((int)j - 1, (int)i - 1, v);
-        }
-        std::sort(e.begin(), e.end(), [](const auto& a, const auto& b) {
-            return std::get<0>(a) != std::get<0>(b) ? std::get<0>(a) < std::get<0>(b)
-                                                    : std::get<1>(a) < std::get<1>(b);
-        });
-        std::vector<int>    rp(M + 1, 0), ci;
-        std::vector<double> vv;
-        for(size_t k = 0; k < e.size(); k++)
-        {
-            if(!ci.empty() && k > 0 && std::get<0>(e[k]) == std::get<0>(e[k - 1]) &&
-               std::get<1>(e[k]) == std::get<1>(e[k - 1]))
-            {
-                vv.back() += std::get<2>(e[k]);
-                continue;
-            }
-            rp[std::get<0>(e[k]) + 1]++;
-            ci.push_back(std::get<1>(e[k]));
-            vv.push_back(std::get<2>(e[k]));
-        }
-        for(long i = 0; i < M; i++)
-            rp[i + 1] += rp[i];
-        resize((int)M, (int)N, (int)ci.size());
-        std::copy(rp.begin(), rp.end(), csr_row_ptr.get_vec());
-        std::copy(ci.begin(), ci.end(), csr_col_ind.get_vec());
-        std::copy(vv.begin(), vv.end(), csr_val.get_vec());
+        resize((int)M, (int)N, (int)Z);
+        std::copy(rp, rp + M + 1, csr_row_ptr.get_vec());
+        std::copy(ci, ci + Z, csr_col_ind.get_vec());
+        std::copy(v, v + Z, csr_val.get_vec());
+        lab_mtx_free(rp);
+        lab_mtx_free(ci);
+        lab_mtx_free(v);
         host_valid = true;
         dev.reset();
         return true;
@@ -650,18 +612,12 @@ namespace linalg
     bool csr_matrix<T>::write_mtx(const std::string& filename)
     {
         sync_host();
-        std::ofstream f(filename);
-        if(!f)
+        if(lab_mtx_write(filename.c_str(), m, n, nnz, csr_row_ptr.get_vec(), csr_col_ind.get_vec(),
+                         csr_val.get_vec()) != LAB_OK)
+        {
+            std::cerr << "Error: " << lab_last_error() << std::endl;
             return false;
-        f << "%%MatrixMarket matrix coordinate real general\n";
-        f << m << " " << n << " " << nnz << "\n";
-        f.precision(17);
-        const int* rp = csr_row_ptr.get_vec();
-        const int* ci = csr_col_ind.get_vec();
-        const T*   v  = csr_val.get_vec();
-        for(int i = 0; i < m; i++)
-            for(int j = rp[i]; j < rp[i + 1]; j++)
-                f << i + 1 << " " << ci[j] + 1 << " " << v[j] << "\n";
+        }
         return true;
     }
 

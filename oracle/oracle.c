@@ -865,6 +865,11 @@ void orc_hier_free(orc_hier* h)
         orc_csr_free(&h->R[l]);
     }
     free(h->coarse_inv);
+    for(int l = 0; l < 21; l++)
+    {
+        free(h->mc_order[l]);
+        free(h->mc_ptr[l]);
+    }
     free(h);
 }
 
@@ -904,6 +909,128 @@ static void gs_sweep(const orc_csr* A, double* x, const double* b)
         }
         x[j] = (b[j] - sigma) / ajj;
     }
+}
+
+/* ------------------------------------------------------------------ multicolour GS
+ * No reference counterpart (the reference's Gauss-Seidel visits rows in order,
+ * gauss_seidel.cpp:50-87).  This restates the device smoother, so its GS / SGS /
+ * SOR / SSOR V-cycles are checked against something: a Jones-Plassmann-Luby
+ * colouring of the pattern of A + A^T in which a row takes colour c when its
+ * priority (hash(i), i) beats every neighbour still uncoloured at the start of
+ * round c; a sweep visits the colours in order (SSOR: forward, then backward)
+ * and sets x_i <- x_i + omega * ((1 / a_ii) * (b_i - sum_j a_ij x_j)), the sum in
+ * CSR order over the whole row (a_ii included) with the current x. */
+static unsigned mc_hash(unsigned x)
+{
+    x ^= 0x9e3779b9u;
+    x = ((x >> 16) ^ x) * 0x45d9f3bu;
+    x = ((x >> 16) ^ x) * 0x45d9f3bu;
+    return (x >> 16) ^ x;
+}
+
+int orc_mc_colouring(const orc_csr* A, int* colour)
+{
+    const int m = A->m;
+    orc_csr   T = {0}, G = {0};
+    orc_transpose(A, &T);
+    orc_spgeam(1.0, A, 1.0, &T, &G);
+    orc_csr_free(&T);
+    for(int i = 0; i < m; i++)
+        colour[i] = -1;
+    int left = m, c = 0;
+    /* a row coloured earlier in this round still counts as uncoloured: the round
+     * reads the state at its start, so colour c is a neighbour that competed */
+    for(; left > 0; c++)
+        for(int i = 0; i < m; i++)
+        {
+            if(colour[i] >= 0)
+                continue;
+            const unsigned hi = mc_hash((unsigned)i);
+            int            win = 1;
+            for(int j = G.rp[i]; j < G.rp[i + 1] && win; j++)
+            {
+                const int k = G.ci[j];
+                if(k == i || (colour[k] >= 0 && colour[k] != c))
+                    continue;
+                const unsigned hk = mc_hash((unsigned)k);
+                if(hk > hi || (hk == hi && k > i))
+                    win = 0;
+            }
+            if(win)
+            {
+                colour[i] = c;
+                left--;
+            }
+        }
+    orc_csr_free(&G);
+    return c;
+}
+
+static void mc_prepare(orc_hier* h, int level)
+{
+    if(h->mc_order[level])
+        return;
+    const orc_csr* A   = &h->A[level];
+    int*           col = (int*)malloc(sizeof(int) * ((size_t)A->m + 1));
+    int            nc  = orc_mc_colouring(A, col);
+    int*           ptr = (int*)calloc((size_t)nc + 2, sizeof(int));
+    int*           ord = (int*)malloc(sizeof(int) * ((size_t)A->m + 1));
+    for(int i = 0; i < A->m; i++)
+        ptr[col[i] + 1]++;
+    for(int c = 0; c < nc; c++)
+        ptr[c + 1] += ptr[c];
+    int* cur = (int*)malloc(sizeof(int) * ((size_t)nc + 1));
+    memcpy(cur, ptr, sizeof(int) * (size_t)nc);
+    for(int i = 0; i < A->m; i++)
+        ord[cur[col[i]]++] = i;
+    free(cur);
+    free(col);
+    h->mc_order[level] = ord;
+    h->mc_ptr[level]   = ptr;
+    h->mc_ncol[level]  = nc;
+}
+
+static void mc_colour_pass(const orc_csr* A, const int* rows, int nr, const double* invd,
+                           double* x, const double* b, double omega)
+{
+    for(int q = 0; q < nr; q++)
+    {
+        const int i = rows[q];
+        double    s = 0.0;
+        for(int j = A->rp[i]; j < A->rp[i + 1]; j++)
+            s = fma(A->v[j], x[A->ci[j]], s);
+        x[i] = x[i] + omega * (invd[i] * (b[i] - s));
+    }
+}
+
+static void mc_sweep(orc_hier* h, int level, double* x, const double* b, double omega, int sym)
+{
+    mc_prepare(h, level);
+    const orc_csr* A    = &h->A[level];
+    double*        invd = (double*)malloc(sizeof(double) * ((size_t)A->m + 1));
+    orc_diag(A, invd);
+    for(int i = 0; i < A->m; i++)
+        invd[i] = 1.0 / invd[i];
+    const int* ptr = h->mc_ptr[level];
+    for(int c = 0; c < h->mc_ncol[level]; c++)
+        mc_colour_pass(A, h->mc_order[level] + ptr[c], ptr[c + 1] - ptr[c], invd, x, b, omega);
+    if(sym)
+        for(int c = h->mc_ncol[level] - 1; c >= 0; c--)
+            mc_colour_pass(A, h->mc_order[level] + ptr[c], ptr[c + 1] - ptr[c], invd, x, b,
+                           omega);
+    free(invd);
+}
+
+static void smooth_sweep(orc_hier* h, int level, double* x, const double* b, int smoother,
+                         double omega, double* tmp)
+{
+    const orc_csr* A = &h->A[level];
+    if(smoother == ORC_SMOOTH_GS)
+        gs_sweep(A, x, b);
+    else if(smoother == ORC_SMOOTH_MC_GS || smoother == ORC_SMOOTH_MC_SSOR)
+        mc_sweep(h, level, x, b, omega, smoother == ORC_SMOOTH_MC_SSOR);
+    else
+        jacobi_sweep(A, x, b, omega, tmp);
 }
 
 /* dense inverse of the coarsest operator by Gauss-Jordan with partial pivoting */
@@ -972,12 +1099,7 @@ void orc_vcycle(orc_hier* h, int level, double* x, const double* b, int n1, int 
         int            Nc = h->A[level + 1].m;
         double*        tmp = (double*)malloc(sizeof(double) * ((size_t)N + 1));
         for(int i = 0; i < n1; i++)
-        {
-            if(smoother == ORC_SMOOTH_GS)
-                gs_sweep(A, x, b);
-            else
-                jacobi_sweep(A, x, b, omega, tmp);
-        }
+            smooth_sweep(h, level, x, b, smoother, omega, tmp);
         double* r  = (double*)malloc(sizeof(double) * ((size_t)N + 1));
         double* wr = (double*)calloc((size_t)Nc + 1, sizeof(double));
         double* ec = (double*)calloc((size_t)Nc + 1, sizeof(double));
@@ -986,12 +1108,7 @@ void orc_vcycle(orc_hier* h, int level, double* x, const double* b, int n1, int 
         orc_vcycle(h, level + 1, ec, wr, n1, n2, smoother, omega, coarse);
         orc_spmv(P, 1.0, ec, 1.0, x);
         for(int i = 0; i < n2; i++)
-        {
-            if(smoother == ORC_SMOOTH_GS)
-                gs_sweep(A, x, b);
-            else
-                jacobi_sweep(A, x, b, omega, tmp);
-        }
+            smooth_sweep(h, level, x, b, smoother, omega, tmp);
         free(tmp);
         free(r);
         free(wr);

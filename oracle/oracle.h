@@ -40,6 +40,11 @@ typedef struct
     orc_csr R[20];
     /* dense inverse of the coarsest operator (built on demand for ORC_COARSE_DIRECT) */
     double* coarse_inv;
+    /* multicolour orderings of the levels (built on demand for ORC_SMOOTH_MC_*):
+     * rows of colour c are mc_order[l][mc_ptr[l][c] .. mc_ptr[l][c+1]) */
+    int* mc_order[21];
+    int* mc_ptr[21];
+    int  mc_ncol[21];
 } orc_hier;
 
 enum
@@ -50,8 +55,10 @@ enum
 };
 enum
 {
-    ORC_SMOOTH_JACOBI = 0,
-    ORC_SMOOTH_GS     = 1
+    ORC_SMOOTH_JACOBI  = 0,
+    ORC_SMOOTH_GS      = 1, /* the reference's lexicographic sweep */
+    ORC_SMOOTH_MC_GS   = 2, /* the device's multicolour sweep, weight omega (GS, SGS: 1) */
+    ORC_SMOOTH_MC_SSOR = 3  /* multicolour sweep forward then backward, weight omega */
 };
 enum
 {
@@ -85,6 +92,9 @@ int  orc_direct_interpolation(const orc_csr* A, const orc_csr* S, const uint32_t
                               orc_csr* P);
 
 orc_hier* orc_amg_setup(int kind, const orc_csr* A, int max_level);
+/* Jones-Plassmann-Luby colouring of the pattern of A + A^T as the device smoother
+ * builds it: colour[i] for every row; returns the number of colours. */
+int orc_mc_colouring(const orc_csr* A, int* colour);
 void      orc_hier_free(orc_hier* h);
 
 /* solve phase.  omega: Jacobi weight (1.0 reproduces the reference's unweighted

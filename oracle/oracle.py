@@ -77,6 +77,8 @@ class Oracle:
     """The C restatement (oracle.c)."""
 
     SA, UA, RS = 0, 1, 2
+    # smoother codes of vcycle / pcg / amg_solve
+    JACOBI, GS, MC_GS, MC_SSOR = 0, 1, 2, 3
 
     def __init__(self, path: str = ORACLE_SO):
         if not os.path.exists(path):
@@ -106,6 +108,8 @@ class Oracle:
         L.orc_amg_solve.argtypes = [C.POINTER(_Hier), _p, _p, _i, _i, _i, _d, _i, _d, _d, _i]
         L.orc_cg.argtypes = [P, _p, _p, _i, _d, _d, _i]
         L.orc_exclusive_scan_i64.argtypes = [_p, _i]
+        L.orc_mc_colouring.argtypes = [P, _p]
+        L.orc_mc_colouring.restype = _i
         L.orc_csrilu0.argtypes = [P, _p, _p]
         L.orc_csric0.argtypes = [P, _p, _p]
         L.orc_trsv.argtypes = [P, _i, _i, _p, _p]
@@ -200,6 +204,13 @@ class Oracle:
         x = np.array(x, dtype=np.int64)
         self.L.orc_exclusive_scan_i64(_ptr(x), x.size)
         return x
+
+    def mc_colouring(self, A):
+        """(colour of every row, number of colours) of the multicolour smoother."""
+        s = _csr_in(*A[:3])
+        col = np.zeros(s.m + 1, dtype=np.int32)
+        nc = self.L.orc_mc_colouring(C.byref(s), _ptr(col))
+        return col[:s.m], nc
 
     # -- hierarchy / solvers
     def amg_setup(self, A, kind=0, max_level=20):
@@ -345,6 +356,9 @@ class Reference:
         L.ref_trsv.argtypes = [_i, _i, _p, _p, _p, _i, _i, _p, _p]
         L.ref_precond_apply.argtypes = [_i, _d, _i, _i, _p, _p, _p, _p, _p]
         L.ref_precond_cg.argtypes = [_i, _d, _i, _i, _p, _p, _p, _p, _p, _d, _d, _i]
+        L.ref_read_mtx.restype = _p
+        L.ref_read_mtx.argtypes = [C.c_char_p]
+        L.ref_write_mtx.argtypes = [C.c_char_p, _i, _i, _i, _p, _p, _p]
 
     @staticmethod
     def _arr(A):
@@ -475,6 +489,16 @@ class Reference:
         it = self.L.ref_precond_cg(kind, omega, m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(b),
                                    _ptr(x), rel_tol, abs_tol, max_iter)
         return x, it
+
+    def read_mtx(self, path):
+        """csr_matrix::read_mtx: (rp, ci, v, n), or None where it returns false."""
+        M = self.L.ref_read_mtx(str(path).encode())
+        return None if not M else self._mat(M)
+
+    def write_mtx(self, path, A):
+        rp, ci, v, m, n, z = self._arr(A)
+        return bool(self.L.ref_write_mtx(str(path).encode(), m, n, z, _ptr(rp), _ptr(ci),
+                                         _ptr(v)))
 
     # No gmres(): the reference's gmres_solver::build leaves its residual vectors
     # unsized (gmres.cpp:211-220) and its solve writes out of bounds (it crashed

@@ -552,4 +552,30 @@ int ref_precond_cg(int kind, double omega, int m, int nnz, const int* rp, const 
     delete P;
     return it;
 }
+
+// ---------------------------------------------------------------- Matrix Market
+// csr_matrix::read_mtx (csr_matrix.cpp:523-729).  Returns a matrix to read with
+// ref_mat_dims / ref_mat_copy, or null when read_mtx returned false.
+void* ref_read_mtx(const char* path)
+{
+    quiet_scope         q;
+    csr_matrix<double>* A = new csr_matrix<double>();
+    if(!A->read_mtx(path))
+    {
+        delete A;
+        return nullptr;
+    }
+    return A;
 }
+
+// csr_matrix::write_mtx (csr_matrix.cpp:731-795); returns its bool.
+int ref_write_mtx(const char* path, int m, int n, int nnz, const int* rp, const int* ci,
+                  const double* v)
+{
+    quiet_scope        q;
+    csr_matrix<double> A;
+    to_csr(A, m, n, nnz, rp, ci, v);
+    return A.write_mtx(path) ? 1 : 0;
+}
+
+} // extern "C"

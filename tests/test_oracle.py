@@ -136,3 +136,45 @@ def test_oracle_matches_golden(oracle, fname):
         x, it, _ = h.pcg(g["b"], rel_tol=float(g["rtol"]), abs_tol=0.0)
         assert it == int(g["pcg_iters"])
         assert np.max(np.abs(x - g["pcg_x"])) <= 1e-9 * np.max(np.abs(g["pcg_x"]))
+
+
+@pytest.mark.parametrize("name", ["poisson2d_33", "diffusion27_7", "nonsym"])
+def test_multicolour_colouring_is_proper(oracle, name):
+    """The colouring behind the multicolour smoothers: rows of one colour are never
+    coupled (in A or A^T), and every colour class is non-empty."""
+    from linalglib_b200 import problems as P
+    if name == "poisson2d_33":
+        A = P.poisson2d(33)
+    elif name == "diffusion27_7":
+        A = P.diffusion27(7, seed=1)
+    else:
+        rp, ci, v = P.poisson2d(17)
+        rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+        keep = ~(ci == rows - 17)  # drop one lower neighbour: a non-symmetric pattern
+        rows = rows[keep]
+        rp = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=rp.size - 1))]).astype(np.int32)
+        A = (rp, ci[keep], v[keep])
+    col, nc = oracle.mc_colouring(A)
+    rp, ci = A[0], A[1]
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+    off = ci != rows
+    assert np.all(col >= 0) and np.all(col < nc)
+    assert not np.any(col[rows[off]] == col[ci[off]])
+    assert np.array_equal(np.unique(col), np.arange(nc))
+
+
+@pytest.mark.parametrize("name", ["poisson2d_33", "poisson3d_12"])
+@pytest.mark.parametrize("ref_smoother,code,omega", [(1, 2, 1.0), (3, 2, 0.5), (4, 3, 0.5)])
+def test_multicolour_stationary_amg_close_to_reference(oracle, reference, name, ref_smoother,
+                                                       code, omega):
+    """The multicolour GS / SOR / SSOR restatement against the reference's
+    lexicographic sweeps in stationary AMG (amg.cpp:516-571): the orderings differ,
+    the cycle counts to 1e-8 agree within one."""
+    A = SMALL[name]()
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    xo, ito = oracle.amg_setup(A).amg_solve(b, smoother=code, omega=omega, coarse=0,
+                                            rel_tol=1e-8, abs_tol=0.0, max_cycle=300)
+    xr, itr = reference.amg_setup(A, kind=0).amg_solve(b, smoother=ref_smoother, rel_tol=1e-8,
+                                                       abs_tol=1e-300, max_cycle=300)
+    assert itr <= 300 and abs(ito - itr) <= 1, (ito, itr)
+    assert np.max(np.abs(xo - xr)) <= 2e-6 * np.max(np.abs(xr))
