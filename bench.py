@@ -192,8 +192,8 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ CPU baseline
-def cpu_reference_solve(A, b, rtol):
-    """One full solve on the compiled reference: (setup_s, solve_s, iters)."""
+def cpu_reference_solve(A, b, rtol, want_x=False):
+    """One full solve on the compiled reference: (setup_s, solve_s, iters[, x])."""
     from oracle.oracle import load_reference
     ref = load_reference()
     if ref is None:
@@ -204,7 +204,7 @@ def cpu_reference_solve(A, b, rtol):
     x, it = h.pcg(b, rel_tol=rtol, abs_tol=1e-300, max_iter=1000)
     t2 = time.perf_counter()
     del h
-    return t1 - t0, t2 - t1, it
+    return (t1 - t0, t2 - t1, it, x) if want_x else (t1 - t0, t2 - t1, it)
 
 
 def cpu_port_solve(A, b, rtol):
@@ -215,20 +215,33 @@ def cpu_port_solve(A, b, rtol):
     t1 = time.perf_counter()
     x, it, _ = h.pcg(b, rel_tol=rtol, abs_tol=0.0, coarse=0)
     t2 = time.perf_counter()
-    return t1 - t0, t2 - t1, it
+    return t1 - t0, t2 - t1, it, x
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def cpu_baseline(A, b, rtol, n):
+    """The reference on this machine's cores; returns (line entry, its FP64 x)."""
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    r = cpu_reference_solve(A, b, rtol)
+    r = cpu_reference_solve(A, b, rtol, want_x=True)
     kind = "reference"
     if r is None:
         r = cpu_port_solve(A, b, rtol)
         kind, cores = "port", 1
-    ts, tv, it = r
+    ts, tv, it, x = r
     return {"value": 1.0 / (ts + tv), "unit": UNIT, "cores": cores, "kind": kind,
+            "cpu_model": cpu_model(),
             "sample": f"one full solve of the {n}^3 system: setup {ts:.2f} s + PCG {tv:.2f} s "
-                      f"({it} iterations, AMG adapter adds 2 residual SpMVs per V-cycle)"}
+                      f"({it} iterations, AMG adapter adds 2 residual SpMVs per V-cycle)"}, x
 
 
 # ------------------------------------------------------------------ reference arm
@@ -259,6 +272,7 @@ def run_reference(args, d):
                    "rows": int(A[0].size - 1), "nnz": int(A[2].size),
                    "parallelism": "host OpenMP, rank 0 only"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "cpu_model": cpu_model(),
                          "sample": f"{steps} full solves (setup + PCG) of the {args.n}^3 system"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "setup_s": [p[0] for p in parts], "solve_s": [p[1] for p in parts],
@@ -466,14 +480,24 @@ def run_ours(args, d):
     e2e_t = d.max(f0.elapsed_time(f1) * 1e-3)
     h2d = 4 * (m + 1) + 4 * nnz + 8 * nnz + 8 * m + 8 * m  # A, b, x0
     d2h = 8 * m
+    e2e_parts = e2e_breakdown(lib, L, C, torch, pin, xh, m, nnz, opts, ctl, sh,
+                              max(3, min(args.steps, 5)))
 
     roof = dominant_kernel_roofline(core, dA, m, nnz, torch, profiled=args.n == 128)
     pcg_roof = pcg_iteration_roofline(core, dA, solves, iters, roof["peak"])
+    mixed, mixed_x = mixed_half(core, L, torch, dA, bd, ctl, setups, max(3, args.steps))
+    setup_roof = setup_roofline(core, torch, dA, roof["peak"], setups)
 
     if d.rank == 0:
-        cpu = None
+        cpu, x_ref = None, None
         if args.gpus == 1 and d.world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline(A, b, args.rtol, args.n)
+            cpu, x_ref = cpu_baseline(A, b, args.rtol, args.n)
+        scale = np.max(np.abs(x_ref)) if x_ref is not None else None
+        for name, xv in mixed_x.items():
+            if x_ref is not None:
+                mixed[name]["err_vs_fp64_reference_solve"] = float(np.max(np.abs(xv - x_ref)) / scale)
+            else:
+                mixed[name]["err_vs_fp64_reference_solve"] = None
         value = d.world * args.steps / t_max
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world,
@@ -487,8 +511,11 @@ def run_ours(args, d):
                        "smoother": "1+1 Jacobi, omega 1 (reference)", "coarse": "dense direct"},
             "e2e": {"value": d.world * args.steps / e2e_t, "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "e2e_parts": e2e_parts,
             "roofline": roof,
             "pcg_iteration_roofline": pcg_roof,
+            "setup_roofline": setup_roof,
+            "mixed_precision": mixed,
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": int(launches),
@@ -498,6 +525,128 @@ def run_ours(args, d):
         print(json.dumps(line), flush=True)
     d.close()
     return 0
+
+
+def setup_roofline(core, torch, dA, peak, setups):
+    """The setup's Galerkin products against HBM: for every level l, AP = A_l P_l and
+    A_l+1 = R_l (AP) rerun on the built hierarchy's operators, each timed with CUDA
+    events (median of 3 after one warm-up), with the reference's SpGEMM bytes
+    |A| + |B| + |C|, |X| = 8 nnz + 4 (nnz + m + 1)
+    (test_functions_multiply_by_matrix.cpp:198-205)."""
+    H = core.Hierarchy(dA)
+
+    def size(X):
+        mm, nn, zz = X.info()
+        return 8 * zz + 4 * (zz + mm + 1)
+
+    levels, tot_b, tot_t = [], 0, 0.0
+    for l in range(H.levels):
+        A, P, R = H.A(l), H.P(l), H.R(l)
+        AP = A.spgemm(P)
+        RAP = R.spgemm(AP)
+        t_ap, _ = _events_ms(torch, lambda: A.spgemm(P), 3)
+        t_rap, _ = _events_ms(torch, lambda: R.spgemm(AP), 3)
+        b_ap = size(A) + size(P) + size(AP)
+        b_rap = size(R) + size(AP) + size(RAP)
+        levels.append({"level": l, "rows": A.m, "AP_bytes": b_ap, "AP_us": 1e3 * t_ap,
+                       "AP_gbs": b_ap / (t_ap * 1e-3) / 1e9, "RAP_bytes": b_rap,
+                       "RAP_us": 1e3 * t_rap, "RAP_gbs": b_rap / (t_rap * 1e-3) / 1e9})
+        tot_b += b_ap + b_rap
+        tot_t += (t_ap + t_rap) * 1e-3
+    achieved = tot_b / tot_t / 1e9
+    del H
+    return {"bound": "hbm", "kernel": "Galerkin SpGEMM (k_hash_gemm / k_esc_* classes), all levels",
+            "algorithmic_bytes": int(tot_b), "ms": 1e3 * tot_t, "achieved": achieved,
+            "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "share_of_setup": 1e3 * tot_t / statistics.median(setups), "levels": levels}
+
+
+def mixed_half(core, L, torch, dA, bd, ctl, setups, reps):
+    """The metric's mixed-precision half on the same system: one FP64 hierarchy,
+    PCG with the FP64, FP32 and FP32 + BF16 (two finest levels) V-cycles to the
+    same FP64 relative residual; solve-only and setup + solve speed-ups against
+    FP64 (the setup is FP64 in every form; the reduced-precision forms add the
+    one-off value conversion, timed as prepare_ms).  The error against the FP64
+    reference solve is filled in by the caller."""
+    H = core.Hierarchy(dA)
+    setup_ms = statistics.median(setups)
+    out, xs = {}, {}
+    for name, prec in (("fp64", L.PREC_FP64), ("fp32", L.PREC_FP32),
+                       ("fp32+bf16", L.PREC_FP32_BF16)):
+        opts = core.amg_options(n1=1, n2=1, omega=1.0, precision=prec)
+        prep, _ = _events_ms(torch, lambda: core.Preconditioner.amg(core.Hierarchy(dA), opts), 1) \
+            if prec != L.PREC_FP64 else (0.0, None)
+        M = core.Preconditioner.amg(H, opts)
+        x = torch.zeros_like(bd)
+        info = []
+
+        def solve():
+            x.zero_()
+            info.append(core.pcg(dA, bd, x=x, M=M, control=ctl)[1])
+        solve()
+        t, ts = _events_ms(torch, solve, reps)
+        out[name] = {"solve_ms": t, "iterations": info[-1].iterations,
+                     "converged": bool(info[-1].converged),
+                     "true_rel_residual": _rel_res(torch, dA, x, bd)}
+        if prec != L.PREC_FP64:
+            # conversion of the values of a fresh hierarchy (setup excluded)
+            out[name]["prepare_ms"] = max(0.0, prep - setup_ms)
+        xs[name] = x.cpu().numpy()
+        del M
+    base = out["fp64"]["solve_ms"]
+    for name in ("fp32", "fp32+bf16"):
+        r = out[name]
+        r["speedup_solve_vs_fp64"] = base / r["solve_ms"]
+        r["speedup_setup_plus_solve_vs_fp64"] = ((setup_ms + base) /
+                                                 (setup_ms + r["prepare_ms"] + r["solve_ms"]))
+    out["setup_ms_fp64"] = setup_ms
+    out["target"] = ">= 1.6x FP64 at the same 1e-8 accuracy"
+    return out, xs
+
+
+def e2e_breakdown(lib, L, C, torch, pin, xh, m, nnz, opts, ctl, sh, reps):
+    """Where an end-to-end step's time goes: the same C-ABI calls as the e2e step,
+    in a separate pass with a device synchronisation after each phase, host wall
+    time per phase (median over reps, ms).  solve_host includes the b upload, the
+    SpMV plan of the new matrix, the capture of the iteration graph for the new
+    preconditioner, the solve and the x download."""
+    parts = {k: [] for k in ("upload_and_create", "setup", "precond_build", "spmv_plan",
+                             "solve_host", "release")}
+
+    def timed(key, fn):
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        parts[key].append(1e3 * (time.perf_counter() - t0))
+        return r
+
+    for _ in range(reps):
+        hA, hH, hM = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        torch.cuda.synchronize()
+        timed("upload_and_create", lambda: L.check(lib.lab_csr_create(
+            C.byref(hA), m, m, nnz, C.c_void_p(pin["rp"].data_ptr()),
+            C.c_void_p(pin["ci"].data_ptr()), C.c_void_p(pin["v"].data_ptr()), L.MEM_HOST, sh)))
+        timed("setup", lambda: L.check(lib.lab_amg_setup(L.AMG_SA, hA, 20, C.byref(hH), sh)))
+        timed("precond_build", lambda: L.check(lib.lab_precond_create_amg(hH, C.byref(opts),
+                                                                          C.byref(hM), sh)))
+        timed("spmv_plan", lambda: L.check(lib.lab_spmv_analysis(hA, sh)))
+        xh.zero_()
+        info = L.SolveInfo()
+        timed("solve_host", lambda: L.check(lib.lab_pcg_solve_host(
+            hA, hM, C.c_void_p(pin["b"].data_ptr()), C.c_void_p(xh.data_ptr()), C.byref(ctl),
+            C.byref(info), sh)))
+        parts.setdefault("solve_device", []).append(info.solve_ms)
+
+        def release():
+            lib.lab_precond_destroy(hM)
+            lib.lab_hierarchy_destroy(hH)
+            lib.lab_csr_destroy(hA)
+        timed("release", release)
+    out = {k: statistics.median(v) for k, v in parts.items()}
+    out["total"] = sum(v for k, v in out.items() if k != "solve_device")
+    out["note"] = ("host wall ms per phase, a device synchronisation after each; "
+                   "solve_device = CUDA-event time of the PCG iterations inside solve_host")
+    return out
 
 
 # ------------------------------------------------------------------ extra workloads

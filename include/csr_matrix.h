@@ -60,12 +60,26 @@ namespace linalg
 
         void resize(int m, int n, int nnz);
         void copy_from(const csr_matrix<T>& A);
+        // csr_matrix.h:215-227: the triangle with columns <= i (>= i), diagonal
+        // included; unit_diag is accepted and, as in the reference, not used
+        void copy_lower_triangular_from(const csr_matrix<T>& A, bool unit_diag);
+        void copy_upper_triangular_from(const csr_matrix<T>& A, bool unit_diag);
         void move_to_device();
         void move_to_host();
         void extract_diagonal(vector<T>& diag) const;
+        // csr_matrix.h:254-262: a_ii *= scalar; a_ij *= 1 / a_jj (by column, as the
+        // reference's host_scale.cpp computes it)
+        void scale_diagonal_by(T scalar);
+        void scale_by_inverse_diagonal();
         void multiply_by_vector(vector<T>& y, const vector<T>& x) const;
         void multiply_by_vector_and_add(vector<T>& y, const vector<T>& x) const;
         void multiply_by_matrix(csr_matrix<T>& C, const csr_matrix<T>& B) const;
+        // csr_matrix.h:298-357: triangular solves on the lower / upper part and the
+        // in-place IC(0) / ILU(0), bit-identical to the reference's host loops
+        void triangular_solve_lower(vector<T>& x, const vector<T>& y, bool unit_diag) const;
+        void triangular_solve_upper(vector<T>& x, const vector<T>& y, bool unit_diag) const;
+        void compute_incomplete_cholesky_factorization();
+        void compute_incomplete_LU_factorization();
         void transpose(csr_matrix<T>& Trans) const;
         bool read_mtx(const std::string& filename);
         bool write_mtx(const std::string& filename);

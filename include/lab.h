@@ -214,6 +214,22 @@ LAB_API lab_status lab_exclusive_scan_i64_noalloc(int64_t n, int64_t* x, lab_str
  * are computed on first use and kept with A; b and x may be the same array. */
 LAB_API lab_status lab_csrtrsv(lab_csr A, int lower, int unit_diag, const double* b, double* x,
                                lab_stream s);
+/* Build (once) the dependency levels of A's pattern that the triangular solves and
+ * the IC(0) / ILU(0) factorizations use; otherwise their first call builds them.
+ * Replaces csrtrsv_analysis / csric0_analysis / csrilu0_analysis
+ * (linalg_math.h:229-237, 469, 510). */
+LAB_API lab_status lab_csrtrsv_analysis(lab_csr A, lab_stream s);
+/* T = the lower (columns <= i) or upper (columns >= i) triangle of A, diagonal
+ * included, a new matrix.  Replaces csr_matrix::copy_lower_triangular_from /
+ * copy_upper_triangular_from (csr_matrix.h:215, 227; host_extract.cpp:54-181). */
+LAB_API lab_status lab_csr_triangle(lab_csr A, int upper, lab_csr* T, lab_stream s);
+/* a_ii *= scalar on the first stored diagonal entry of every row.  Replaces
+ * csr_matrix::scale_diagonal_by (csr_matrix.h:254; host_scale.cpp:34-52). */
+LAB_API lab_status lab_csr_scale_diagonal(lab_csr A, double scalar, lab_stream s);
+/* a_ij *= 1 / a_jj (the diagonal of lab_diagonal, indexed by column, as the
+ * reference computes it).  Replaces csr_matrix::scale_by_inverse_diagonal
+ * (csr_matrix.h:262; csr_matrix.cpp:277-299; host_scale.cpp:54-69). */
+LAB_API lab_status lab_csr_scale_by_inverse_diagonal(lab_csr A, lab_stream s);
 /* The bounded wait of the triangular solves on A (the lab_csrtrsv solves and the
  * ILU / IC / Gauss-Seidel / SOR / SSOR preconditioner applications).  A row waits
  * for its dependencies by polling; after idle_rounds rounds without progress

@@ -31,6 +31,20 @@ namespace linalg
     void csric0(csr_matrix<double>& LL, int* structural_zero, int* numeric_zero);
     void csrilu0(csr_matrix<double>& LU, int* structural_zero, int* numeric_zero);
 
+    // Descriptor form of the same factorizations (linalg_math.h:447-520): the
+    // analysis builds the dependency levels of A's pattern (kept with the matrix),
+    // the compute step factors A in place.
+    struct csric0_descr;
+    struct csrilu0_descr;
+    void create_csric0_descr(csric0_descr** descr);
+    void destroy_csric0_descr(csric0_descr* descr);
+    void csric0_analysis(const csr_matrix<double>& A, csric0_descr* descr);
+    void csric0_compute(csr_matrix<double>& A, const csric0_descr* descr);
+    void create_csrilu0_descr(csrilu0_descr** descr);
+    void destroy_csrilu0_descr(csrilu0_descr* descr);
+    void csrilu0_analysis(const csr_matrix<double>& A, csrilu0_descr* descr);
+    void csrilu0_compute(csr_matrix<double>& A, const csrilu0_descr* descr);
+
     // Sparse triangular solve on the lower or upper part of A (linalg_math.h:
     // 198-254, linalg_enums.h:37-48).  The analysis builds the level schedule of
     // A's pattern (cached on the matrix); x = T^-1 (alpha b).

@@ -101,10 +101,14 @@ _SIGS = {
     "lab_hierarchy_level": [_p, _i, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p)],
     "lab_hierarchy_setup_ms": [_p, C.POINTER(_d)],
     "lab_csrtrsv": [_p, _i, _i, _p, _p, _p],
+    "lab_csrtrsv_analysis": [_p, _p],
     "lab_mtx_read": [_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_p),
                      C.POINTER(_p), C.POINTER(_p)],
     "lab_mtx_write": [_p, _i64, _i64, _i64, _p, _p, _p],
     "lab_csrtrsv_wait_control": [_p, _i64, _i64, _p],
+    "lab_csr_triangle": [_p, _i, C.POINTER(_p), _p],
+    "lab_csr_scale_diagonal": [_p, _d, _p],
+    "lab_csr_scale_by_inverse_diagonal": [_p, _p],
     "lab_csrilu0": [_p, C.POINTER(_i), C.POINTER(_i), _p],
     "lab_csric0": [_p, C.POINTER(_i), C.POINTER(_i), _p],
     "lab_precond_create_ilu0": [_p, C.POINTER(_p), _p],

@@ -193,6 +193,16 @@ class CsrMatrix:
              stream_handle())
         return sz.value, nz.value
 
+    def triangle(self, upper=False):
+        """The lower (columns <= i) or upper triangle, diagonal included."""
+        return self._new("lab_csr_triangle", self.h, int(bool(upper)))
+
+    def scale_diagonal(self, scalar):
+        call("lab_csr_scale_diagonal", self.h, C.c_double(scalar), stream_handle())
+
+    def scale_by_inverse_diagonal(self):
+        call("lab_csr_scale_by_inverse_diagonal", self.h, stream_handle())
+
     def spgemm(self, B):
         return self._new("lab_spgemm", self.h, B.h)
 

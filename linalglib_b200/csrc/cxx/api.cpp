@@ -527,6 +527,76 @@ namespace linalg
     }
 
     template <typename T>
+    void csr_matrix<T>::copy_lower_triangular_from(const csr_matrix<T>& A, bool)
+    {
+        lab_csr out = nullptr;
+        if(ok(lab_csr_triangle(A.device(), 0, &out, nullptr), "copy_lower_triangular_from"))
+            adopt(out, true);
+    }
+
+    template <typename T>
+    void csr_matrix<T>::copy_upper_triangular_from(const csr_matrix<T>& A, bool)
+    {
+        lab_csr out = nullptr;
+        if(ok(lab_csr_triangle(A.device(), 1, &out, nullptr), "copy_upper_triangular_from"))
+            adopt(out, true);
+    }
+
+    template <typename T>
+    void csr_matrix<T>::scale_diagonal_by(T scalar)
+    {
+        if(ok(lab_csr_scale_diagonal(device(), (double)scalar, nullptr), "scale_diagonal_by"))
+            device_changed();
+    }
+
+    template <typename T>
+    void csr_matrix<T>::scale_by_inverse_diagonal()
+    {
+        if(ok(lab_csr_scale_by_inverse_diagonal(device(), nullptr), "scale_by_inverse_diagonal"))
+            device_changed();
+    }
+
+    template <typename T>
+    void csr_matrix<T>::triangular_solve_lower(vector<T>& x, const vector<T>& y,
+                                               bool unit_diag) const
+    {
+        if(x.get_size() < (size_t)m)
+            x.resize(m);
+        ok(lab_csrtrsv(device(), 1, unit_diag ? 1 : 0,
+                       reinterpret_cast<const double*>(y.device_read()),
+                       reinterpret_cast<double*>(x.device_write()), nullptr),
+           "triangular_solve_lower");
+    }
+
+    template <typename T>
+    void csr_matrix<T>::triangular_solve_upper(vector<T>& x, const vector<T>& y,
+                                               bool unit_diag) const
+    {
+        if(x.get_size() < (size_t)m)
+            x.resize(m);
+        ok(lab_csrtrsv(device(), 0, unit_diag ? 1 : 0,
+                       reinterpret_cast<const double*>(y.device_read()),
+                       reinterpret_cast<double*>(x.device_write()), nullptr),
+           "triangular_solve_upper");
+    }
+
+    template <typename T>
+    void csr_matrix<T>::compute_incomplete_cholesky_factorization()
+    {
+        int sz = -1, nz = -1;
+        if(ok(lab_csric0(device(), &sz, &nz, nullptr), "compute_incomplete_cholesky_factorization"))
+            device_changed();
+    }
+
+    template <typename T>
+    void csr_matrix<T>::compute_incomplete_LU_factorization()
+    {
+        int sz = -1, nz = -1;
+        if(ok(lab_csrilu0(device(), &sz, &nz, nullptr), "compute_incomplete_LU_factorization"))
+            device_changed();
+    }
+
+    template <typename T>
     void csr_matrix<T>::move_to_device()
     {
         on_host = false;
@@ -766,6 +836,52 @@ namespace linalg
         }
     }
 
+    // The descriptors hold nothing of their own: the dependency levels the
+    // analysis builds stay with the matrix (its first triangular operation builds
+    // them), so analysis is optional and compute is the in-place factorization.
+    struct csric0_descr
+    {
+        int analysed = 0;
+    };
+    struct csrilu0_descr
+    {
+        int analysed = 0;
+    };
+    void create_csric0_descr(csric0_descr** d)
+    {
+        *d = new csric0_descr();
+    }
+    void destroy_csric0_descr(csric0_descr* d)
+    {
+        delete d;
+    }
+    void csric0_analysis(const csr_matrix<double>& A, csric0_descr* d)
+    {
+        if(ok(lab_csrtrsv_analysis(A.device(), nullptr), "csric0_analysis") && d)
+            d->analysed = 1;
+    }
+    void csric0_compute(csr_matrix<double>& A, const csric0_descr*)
+    {
+        csric0(A, nullptr, nullptr);
+    }
+    void create_csrilu0_descr(csrilu0_descr** d)
+    {
+        *d = new csrilu0_descr();
+    }
+    void destroy_csrilu0_descr(csrilu0_descr* d)
+    {
+        delete d;
+    }
+    void csrilu0_analysis(const csr_matrix<double>& A, csrilu0_descr* d)
+    {
+        if(ok(lab_csrtrsv_analysis(A.device(), nullptr), "csrilu0_analysis") && d)
+            d->analysed = 1;
+    }
+    void csrilu0_compute(csr_matrix<double>& A, const csrilu0_descr*)
+    {
+        csrilu0(A, nullptr, nullptr);
+    }
+
     struct csrtrsv_descr
     {
         int analysed = 0;
@@ -781,17 +897,8 @@ namespace linalg
     void csrtrsv_analysis(const csr_matrix<double>& A, triangular_type, diagonal_type,
                           csrtrsv_descr* d)
     {
-        // the schedule is built and cached on the matrix by its first solve: a
-        // zero-length solve is not enough, so solve once into scratch
-        const int m = A.get_m();
-        if(m > 0)
-        {
-            vector<double> b(m), x(m);
-            b.zeros();
-            ok(lab_csrtrsv(A.device(), 1, 1, b.device_read(), x.device_write(), nullptr),
-               "csrtrsv_analysis");
-        }
-        if(d)
+        // the level schedule of A's pattern is built once and kept with the matrix
+        if(ok(lab_csrtrsv_analysis(A.device(), nullptr), "csrtrsv_analysis") && d)
             d->analysed = 1;
     }
     void csrtrsv_solve(const csr_matrix<double>& A, const vector<double>& b, vector<double>& x,

@@ -858,6 +858,100 @@ namespace lab
         }
     }
 
+    // ------------------------------------------------------------ csr_matrix members
+    // The triangle of A with columns <= i (lower) or >= i (upper), diagonal
+    // included, rows kept in CSR order (host_extract.cpp:54-181; the reference
+    // passes its unit_diag flag nowhere, so neither does this).
+    __global__ void k_tri_count(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                int m, int upper, int32_t* __restrict__ cnt)
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int c = 0;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+            c += upper ? ci[j] >= i : ci[j] <= i;
+        cnt[i] = c;
+    }
+
+    __global__ void k_tri_fill(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                               const double* __restrict__ v, int m, int upper,
+                               const int32_t* __restrict__ trp, int32_t* __restrict__ tci,
+                               double* __restrict__ tv)
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        int o = trp[i];
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+            if(upper ? ci[j] >= i : ci[j] <= i)
+            {
+                tci[o] = ci[j];
+                tv[o]  = v[j];
+                o++;
+            }
+    }
+
+    // host_scale.cpp:34-52: the first stored a_ii of each row times the scalar
+    __global__ void k_scale_diag(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                 double* __restrict__ v, int m, double scalar)
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= m)
+            return;
+        for(int j = rp[i]; j < rp[i + 1]; j++)
+            if(ci[j] == i)
+            {
+                v[j] = __dmul_rn(v[j], scalar);
+                break;
+            }
+    }
+
+    // host_scale.cpp:54-69: every entry a_ij times (1 / d_j), d the diagonal of
+    // extract_diagonal (first stored a_jj, 0 if none: the factor is then inf)
+    __global__ void k_scale_inv_diag(const int32_t* __restrict__ ci, double* __restrict__ v,
+                                     int64_t nnz, const double* __restrict__ d)
+    {
+        for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nnz;
+            j += (int64_t)gridDim.x * blockDim.x)
+            v[j] = __dmul_rn(v[j], __ddiv_rn(1.0, d[ci[j]]));
+    }
+
+    static lab_status triangle(lab_csr_impl* A, bool upper, lab_csr_impl** T, cudaStream_t s)
+    {
+        const int     m = (int)A->m;
+        dbuf<int32_t> cnt;
+        LAB_TRY(cnt.alloc((size_t)m + 1, s));
+        if(m > 0)
+            LAB_LAUNCH(k_tri_count, (unsigned)ceil_div(m, 256), 256, 0, s, A->row_ptr, A->col_ind,
+                       m, (int)upper, cnt.get());
+        int64_t nt = 0;
+        LAB_TRY(counts_to_rowptr(cnt.get(), cnt.get(), m, &nt, s));
+        lab_csr_impl* t = nullptr;
+        LAB_TRY(csr_alloc(&t, A->m, A->n, nt, s));
+        lab_status st = LAB_OK;
+        if(cudaMemcpyAsync(t->row_ptr, cnt.get(), sizeof(int32_t) * ((size_t)m + 1),
+                           cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            st = LAB_CUDA_ERROR;
+        if(st == LAB_OK && m > 0)
+        {
+            k_tri_fill<<<(unsigned)ceil_div(m, 256), 256, 0, s>>>(
+                A->row_ptr, A->col_ind, (const double*)A->val, m, (int)upper, t->row_ptr,
+                t->col_ind, (double*)t->val);
+            g_launches.fetch_add(1);
+            if(cudaGetLastError() != cudaSuccess)
+                st = LAB_CUDA_ERROR;
+        }
+        if(st != LAB_OK)
+        {
+            set_error("triangle extraction failed");
+            csr_release(t);
+            return st;
+        }
+        *T = t;
+        return LAB_OK;
+    }
+
     lab_status ssor_split(lab_csr_impl* A, double omega, lab_csr_impl** L, lab_csr_impl** U,
                           cudaStream_t s)
     {
@@ -938,6 +1032,52 @@ LAB_API lab_status lab_csrtrsv_wait_control(lab_csr A, int64_t idle_rounds, int6
     A->tri->idle_limit = (unsigned)idle_rounds;
     A->tri->held_row   = (int)held_row;
     return LAB_OK;
+}
+
+LAB_API lab_status lab_csr_triangle(lab_csr A, int upper, lab_csr* T, lab_stream s)
+{
+    LAB_ARG(A && T, "null argument");
+    LAB_TRY(ensure_init());
+    lab_csr_impl* t = nullptr;
+    LAB_TRY(triangle(A, upper != 0, &t, to_stream(s)));
+    *T = static_cast<lab_csr_s*>(t);
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_csrtrsv_analysis(lab_csr A, lab_stream s)
+{
+    LAB_ARG(A, "null matrix");
+    LAB_ARG(A->m == A->n, "triangular analysis needs a square matrix");
+    LAB_TRY(ensure_init());
+    return A->m == 0 ? LAB_OK : tri_analyse(A, to_stream(s));
+}
+
+LAB_API lab_status lab_csr_scale_diagonal(lab_csr A, double scalar, lab_stream s)
+{
+    LAB_ARG(A, "null matrix");
+    LAB_TRY(ensure_init());
+    if(A->m > 0)
+        LAB_LAUNCH(k_scale_diag, (unsigned)ceil_div<int64_t>(A->m, 256), 256, 0, to_stream(s),
+                   A->row_ptr, A->col_ind, A->val, (int)A->m, scalar);
+    return lab_csr_values_changed(A, s);
+}
+
+LAB_API lab_status lab_csr_scale_by_inverse_diagonal(lab_csr A, lab_stream ls)
+{
+    LAB_ARG(A, "null matrix");
+    LAB_ARG(A->m == A->n, "square matrix required (columns index the diagonal)");
+    LAB_TRY(ensure_init());
+    cudaStream_t s = to_stream(ls);
+    if(A->nnz > 0)
+    {
+        dbuf<double> d;
+        LAB_TRY(d.alloc((size_t)A->m, s));
+        LAB_TRY(diag_into(A, d.get(), nullptr, s));
+        LAB_LAUNCH(k_scale_inv_diag,
+                   (unsigned)std::min<int64_t>(ceil_div<int64_t>(A->nnz, 256), 8 * num_sms()), 256,
+                   0, s, A->col_ind, A->val, A->nnz, (const double*)d.get());
+    }
+    return lab_csr_values_changed(A, ls);
 }
 
 LAB_API lab_status lab_csrilu0(lab_csr A, int* structural_zero, int* numeric_zero, lab_stream s)

@@ -356,6 +356,9 @@ class Reference:
         L.ref_trsv.argtypes = [_i, _i, _p, _p, _p, _i, _i, _p, _p]
         L.ref_precond_apply.argtypes = [_i, _d, _i, _i, _p, _p, _p, _p, _p]
         L.ref_precond_cg.argtypes = [_i, _d, _i, _i, _p, _p, _p, _p, _p, _d, _d, _i]
+        L.ref_triangle.restype = _p
+        L.ref_triangle.argtypes = [_i, _i, _i, _p, _p, _p, _i]
+        L.ref_scale.argtypes = [_i, _i, _i, _p, _p, _p, _i, _d, _p]
         L.ref_read_mtx.restype = _p
         L.ref_read_mtx.argtypes = [C.c_char_p]
         L.ref_write_mtx.argtypes = [C.c_char_p, _i, _i, _i, _p, _p, _p]
@@ -489,6 +492,23 @@ class Reference:
         it = self.L.ref_precond_cg(kind, omega, m, z, _ptr(rp), _ptr(ci), _ptr(v), _ptr(b),
                                    _ptr(x), rel_tol, abs_tol, max_iter)
         return x, it
+
+    def triangle(self, A, upper=False):
+        """copy_lower_triangular_from / copy_upper_triangular_from."""
+        rp, ci, v, m, n, z = self._arr(A)
+        return self._mat(self.L.ref_triangle(m, n, z, _ptr(rp), _ptr(ci), _ptr(v), int(upper)))
+
+    def scale_diagonal(self, A, scalar):
+        rp, ci, v, m, n, z = self._arr(A)
+        out = np.zeros(max(z, 1))
+        self.L.ref_scale(m, n, z, _ptr(rp), _ptr(ci), _ptr(v), 0, scalar, _ptr(out))
+        return out[:z]
+
+    def scale_by_inverse_diagonal(self, A):
+        rp, ci, v, m, n, z = self._arr(A)
+        out = np.zeros(max(z, 1))
+        self.L.ref_scale(m, n, z, _ptr(rp), _ptr(ci), _ptr(v), 1, 0.0, _ptr(out))
+        return out[:z]
 
     def read_mtx(self, path):
         """csr_matrix::read_mtx: (rp, ci, v, n), or None where it returns false."""

@@ -578,4 +578,34 @@ int ref_write_mtx(const char* path, int m, int n, int nnz, const int* rp, const 
     return A.write_mtx(path) ? 1 : 0;
 }
 
+// ---------------------------------------------------------------- csr_matrix members
+// copy_lower_triangular_from / copy_upper_triangular_from (csr_matrix.cpp:170-225)
+void* ref_triangle(int m, int n, int nnz, const int* rp, const int* ci, const double* v,
+                   int upper)
+{
+    quiet_scope         q;
+    csr_matrix<double>  A;
+    to_csr(A, m, n, nnz, rp, ci, v);
+    csr_matrix<double>* T = new csr_matrix<double>();
+    if(upper)
+        T->copy_upper_triangular_from(A, false);
+    else
+        T->copy_lower_triangular_from(A, false);
+    return T;
+}
+
+// scale_diagonal_by (kind 0) / scale_by_inverse_diagonal (kind 1), values out
+void ref_scale(int m, int n, int nnz, const int* rp, const int* ci, const double* v, int kind,
+               double scalar, double* out)
+{
+    quiet_scope        q;
+    csr_matrix<double> A;
+    to_csr(A, m, n, nnz, rp, ci, v);
+    if(kind == 0)
+        A.scale_diagonal_by(scalar);
+    else
+        A.scale_by_inverse_diagonal();
+    std::memcpy(out, A.get_val(), sizeof(double) * nnz);
+}
+
 } // extern "C"

@@ -69,3 +69,42 @@ def test_cxx_triangular_preconditioners(gpu, oracle, reference, tmp_path_factory
     # GMRES stops on the preconditioned 2-norm residual (1e-10 relative); the
     # printed figure is the true inf-norm residual
     assert float(rel) <= 1e-8
+
+
+def test_cxx_matrix_members_and_mtx(gpu, reference, tmp_path_factory, tmp_path):
+    """read_mtx, the triangle copies, diagonal scalings, IC(0) / ILU(0) (members
+    and descriptor form), write_mtx and the triangular-solve members, called as a
+    reference client calls them; every file written must be byte-identical to the
+    reference's write_mtx of the reference's own result, and the solves bitwise."""
+    from linalglib_b200 import _lib as L
+    exe = _compile(tmp_path_factory, "matrix_members_example")
+    n = 14
+    rp, ci, v = P.poisson2d(n)
+    v = v.copy()
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+    v[ci == rows + 1] *= 0.625
+    v[ci == rows] += np.linspace(0.0, 1.0, rp.size - 1)
+    src = tmp_path / "in.mtx"
+    L.mtx_write(src, rp, ci, v)
+    out = subprocess.run([exe, str(src), str(tmp_path)], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    A = reference.read_mtx(src)
+    m = A[0].size - 1
+
+    def same(name, R):
+        reference.write_mtx(tmp_path / ("ref_" + name), R)
+        assert (tmp_path / name).read_bytes() == (tmp_path / ("ref_" + name)).read_bytes(), name
+
+    same("lower.mtx", reference.triangle(A, upper=False))
+    same("upper.mtx", reference.triangle(A, upper=True))
+    same("diag.mtx", (A[0], A[1], reference.scale_diagonal(A, 2.5), A[3]))
+    same("invdiag.mtx", (A[0], A[1], reference.scale_by_inverse_diagonal(A), A[3]))
+    for name, fn in (("ic0", reference.csric0), ("ilu0", reference.csrilu0)):
+        R = (A[0], A[1], fn(A)[0], A[3])
+        same(name + ".mtx", R)
+        same(name + "_descr.mtx", R)
+    xs = np.array([float.fromhex(t) for t in out.stdout.split()])
+    xl, xu = xs[:m], xs[m:]
+    assert np.array_equal(xl.view(np.int64), reference.trsv(A, np.ones(m), True, False).view(np.int64))
+    assert np.array_equal(xu.view(np.int64), reference.trsv(A, np.ones(m), False, False).view(np.int64))

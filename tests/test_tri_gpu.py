@@ -204,3 +204,49 @@ def test_trsv_bounded_wait_reports_timeout(gpu, oracle, lower):
     L.call("lab_csrtrsv_wait_control", dA.h, 0, -1, gpu.stream_handle())
     x = dA.trsv(gpu.vec(b), lower=lower)
     assert np.array_equal(_bits(x.cpu().numpy()), _bits(oracle.trsv(A, b, lower, False)))
+
+
+MEMBER_CASES = {
+    "poisson2d_20": lambda: P.poisson2d(20),
+    "diffusion27_6": lambda: P.diffusion27(6, seed=2),
+    "nonsym_18": lambda: _nonsym(18),
+}
+
+
+def _nonsym(n):
+    rp, ci, v = P.poisson2d(n)
+    v = v.copy()
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+    v[ci == rows + 1] *= 0.37
+    v[ci == rows - n] *= 1.9
+    return rp, ci, v
+
+
+@pytest.mark.parametrize("name", list(MEMBER_CASES))
+def test_triangle_copies_match_reference(gpu, reference, name):
+    """copy_lower_triangular_from / copy_upper_triangular_from
+    (csr_matrix.cpp:170-225): same pattern, same values."""
+    from helpers import csr_diff, csr_equal
+    A = MEMBER_CASES[name]()
+    dA = gpu.CsrMatrix.from_arrays(*A)
+    for upper in (False, True):
+        g = dA.triangle(upper=upper).to_numpy()
+        r = reference.triangle(A, upper=upper)
+        assert csr_equal(g, r), csr_diff(g, r)
+
+
+@pytest.mark.parametrize("name", list(MEMBER_CASES))
+def test_diagonal_scalings_match_reference(gpu, reference, name):
+    """scale_diagonal_by and scale_by_inverse_diagonal (host_scale.cpp:34-69)."""
+    A = MEMBER_CASES[name]()
+    dA = gpu.CsrMatrix.from_arrays(*A)
+    dA.scale_diagonal(-2.75)
+    assert np.array_equal(_bits(dA.to_numpy()[2]), _bits(reference.scale_diagonal(A, -2.75)))
+    dB = gpu.CsrMatrix.from_arrays(*A)
+    dB.scale_by_inverse_diagonal()
+    assert np.array_equal(_bits(dB.to_numpy()[2]), _bits(reference.scale_by_inverse_diagonal(A)))
+    # the scaled matrix's cached diagonal is rebuilt (the next Jacobi sees new values)
+    assert np.array_equal(dB.diagonal().cpu().numpy(),
+                          [dB.to_numpy()[2][j] for j in
+                           [next(k for k in range(A[0][i], A[0][i + 1]) if A[1][k] == i)
+                            for i in range(A[0].size - 1)]])
