@@ -950,8 +950,9 @@ LAB_API lab_status lab_csr_values_changed(lab_csr A, lab_stream ls)
     dfree(A->lp.f32, s);
     dfree(A->lp.bf16, s);
     dfree(A->lp.invd32, s);
-    dfree(A->lp.dcol, s);
-    A->lp = csr_values_lp();
+    A->lp.f32    = nullptr;
+    A->lp.bf16   = nullptr;
+    A->lp.invd32 = nullptr; // the 16-bit column offsets depend on the pattern only
     // a new identity: solver graphs captured on the old values (and on the cached
     // arrays just released) no longer match and are captured again
     A->uid = next_uid();
@@ -963,6 +964,9 @@ LAB_API lab_status lab_csr_structure_changed(lab_csr A, lab_stream ls)
     LAB_ARG(A, "null matrix");
     LAB_TRY(lab_csr_values_changed(A, ls));
     cudaStream_t s = to_stream(ls);
+    dfree(A->lp.dcol, s);
+    A->lp.dcol       = nullptr;
+    A->lp.dcol_state = 0;
     dfree(A->plan.block_row, s);
     dfree(A->plan.merge_coords, s);
     A->plan = spmv_plan();

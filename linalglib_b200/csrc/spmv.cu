@@ -17,6 +17,27 @@ namespace lab
             atomicMax(maxlen, local);
     }
 
+    // 16-bit column offsets col - row, W lanes per row (coalesced over the row's
+    // entries); *wide = 1 when some offset leaves the int16 range (the copy is
+    // then discarded).
+    template <int W>
+    __global__ void k_dcol_build(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                 int64_t m, int16_t* __restrict__ dcol, int* wide)
+    {
+        const int lane = threadIdx.x & (W - 1);
+        int       bad  = 0;
+        for(int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / W; i < m;
+            i += (int64_t)gridDim.x * blockDim.x / W)
+            for(int j = rp[i] + lane; j < rp[i + 1]; j += W)
+            {
+                const int64_t d = (int64_t)ci[j] - i;
+                bad |= d < INT16_MIN || d > INT16_MAX;
+                dcol[j] = (int16_t)d;
+            }
+        if(__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0)
+            atomicOr(wide, 1);
+    }
+
     // Largest power of two <= v, clamped to 2..32.
     static int pow2_at_most(double v)
     {
@@ -35,23 +56,61 @@ namespace lab
     // entries, 8 at 41-73, 16 at 143-178, 16-32 beyond); lab_spmv_autotune times
     // every choice on the actual matrix instead.  vlanes is also the lane count of
     // SpMM and multicolour Gauss-Seidel on long rows.
+    //
+    // The same pass checks whether every column offset col - row fits in 16 bits;
+    // then a 16-bit offset copy is built once per pattern and the row kernels read
+    // it in place of the int32 columns in every precision (2 instead of 4 index
+    // bytes per entry; the column, and so the arithmetic, is the same).
     lab_status spmv_analyse(lab_csr_impl* A, cudaStream_t s)
     {
         spmv_plan& p = A->plan;
         if(p.analysed)
             return LAB_OK;
-        int maxlen = 0;
+        int stats[2] = {0, 0}; // longest row, offsets too wide for 16 bits
         if(A->m > 0)
         {
             int* d = nullptr;
-            LAB_TRY(dalloc(&d, 1, s));
-            LAB_CUDA(cudaMemsetAsync(d, 0, sizeof(int), s));
+            LAB_TRY(dalloc(&d, 2, s));
+            LAB_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(int), s));
             unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(A->m, 256), 2048);
             LAB_LAUNCH(k_row_stats, grid, 256, 0, s, A->row_ptr, A->m, d);
-            lab_status st = copy_d2h_sync(&maxlen, d, sizeof(int), s);
+            // square matrices only: a prolongation's or restriction's col - row
+            // spans the ratio of the two grids and does not fit
+            const bool build = A->lp.dcol_state == 0 && A->nnz > 0 && A->m == A->n;
+            if(build)
+            {
+                LAB_TRY(dalloc(&A->lp.dcol, (size_t)A->nnz, s));
+                // lanes per row: the largest power of two <= the mean row length
+                const double avg = (double)A->nnz / (double)A->m;
+                int          w   = 1;
+                while(w < 32 && 2 * w <= avg)
+                    w <<= 1;
+                const unsigned g = (unsigned)std::min<int64_t>(
+                    ceil_div<int64_t>(A->m * (int64_t)w, 256), (int64_t)num_sms() * 8);
+                switch(w)
+                {
+                case 1: LAB_LAUNCH(k_dcol_build<1>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
+                case 2: LAB_LAUNCH(k_dcol_build<2>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
+                case 4: LAB_LAUNCH(k_dcol_build<4>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
+                case 8: LAB_LAUNCH(k_dcol_build<8>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
+                case 16: LAB_LAUNCH(k_dcol_build<16>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
+                default: LAB_LAUNCH(k_dcol_build<32>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
+                }
+            }
+            lab_status st = copy_d2h_sync(stats, d, sizeof(stats), s);
             dfree(d, s);
             LAB_TRY(st);
+            if(build)
+            {
+                A->lp.dcol_state = stats[1] ? -1 : 1;
+                if(stats[1])
+                {
+                    dfree(A->lp.dcol, s);
+                    A->lp.dcol = nullptr;
+                }
+            }
         }
+        const int maxlen = stats[0];
         p.max_row = maxlen;
         p.avg_row = A->m > 0 ? (double)A->nnz / (double)A->m : 0.0;
         p.vlanes  = pow2_at_most(p.avg_row / 5.0);

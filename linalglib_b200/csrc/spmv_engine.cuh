@@ -657,10 +657,10 @@ namespace lab
         }
     }
 
-    // One CSR pass of `op` over A with the given value array.  Reduced-precision
-    // values read the matrix's 16-bit column offsets when it has them (compact
-    // storage of the mixed-precision cycle); FP64 values read the stored int32
-    // columns (the reference layout).
+    // One CSR pass of `op` over A with the given value array.  The matrix's 16-bit
+    // column offsets are read in place of the int32 columns when it has them (every
+    // offset fits: built with the SpMV plan), in every precision; the column each
+    // entry names is the same, so results are unchanged.
     template <class Op>
     lab_status launch_rowop(const lab_csr_impl* A, const typename Op::val_t* vals, const Op& op,
                             cudaStream_t s, red_buf red = red_buf())
@@ -668,13 +668,10 @@ namespace lab
         using VT = typename Op::val_t;
         if(A->m == 0)
             return LAB_OK;
-        if constexpr(!std::is_same<VT, double>::value)
+        if(A->lp.dcol)
         {
-            if(A->lp.dcol)
-            {
-                csr_view<VT, int16_t> V{A->row_ptr, A->lp.dcol, vals, (int32_t)A->m};
-                return launch_rowop_view<Op, int16_t>(A, V, op, s, red);
-            }
+            csr_view<VT, int16_t> V{A->row_ptr, A->lp.dcol, vals, (int32_t)A->m};
+            return launch_rowop_view<Op, int16_t>(A, V, op, s, red);
         }
         csr_view<VT, int32_t> V{A->row_ptr, A->col_ind, vals, (int32_t)A->m};
         return launch_rowop_view<Op, int32_t>(A, V, op, s, red);
