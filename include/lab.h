@@ -71,6 +71,11 @@ LAB_API lab_status lab_init(int device);
 LAB_API lab_status lab_synchronize(lab_stream s);
 /* Number of kernel launches issued by this library since load (all threads). */
 LAB_API int64_t lab_launch_count(void);
+/* How many bounded device-side waits of the streaming row kernels ran out on the
+ * current device since the library was loaded (0 in normal operation: a wait
+ * that runs out ends its kernel early instead of hanging the GPU, and the rows
+ * it had not reached are left unwritten).  No reference counterpart. */
+LAB_API lab_status lab_wait_timeouts(int64_t* count, lab_stream s);
 /* Allocate / free library device memory (stream ordered). */
 LAB_API lab_status lab_malloc(void** p, size_t bytes, lab_stream s);
 LAB_API lab_status lab_free(void* p, lab_stream s);
@@ -138,7 +143,11 @@ typedef enum lab_spmv_alg
     LAB_SPMV_AUTO    = 0, /* chosen by lab_spmv_analysis from row statistics */
     LAB_SPMV_ROWSEQ  = 1, /* thread per row over shared-memory staged rows, fma in CSR order */
     LAB_SPMV_VECTOR  = 2, /* 2..32 lanes per row, vectorised loads, shuffle reduction */
-    LAB_SPMV_MERGE   = 3  /* merge-path nnz split for skewed row lengths */
+    LAB_SPMV_MERGE   = 3, /* merge-path nnz split for skewed row lengths */
+    LAB_SPMV_VECTOR_STREAM = 4 /* LAB_SPMV_VECTOR with the matrix streamed through shared
+                                  memory by bulk copies (one producer warp, mbarrier
+                                  stage ring) on operators of >= 8192 rows; the same
+                                  per-row arithmetic, bit-identical; elsewhere as VECTOR */
 } lab_spmv_alg;
 
 /* Row-length statistics -> algorithm and launch shape, cached on the matrix.

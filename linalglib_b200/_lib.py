@@ -20,7 +20,7 @@ CYCLE_V, CYCLE_W, CYCLE_F = 0, 1, 2
 SMOOTH_JACOBI, SMOOTH_GS, SMOOTH_SGS, SMOOTH_SOR, SMOOTH_SSOR = range(5)
 COARSE_DIRECT, COARSE_GS = 0, 1
 PREC_FP64, PREC_FP32, PREC_FP32_BF16 = 0, 1, 2
-SPMV_AUTO, SPMV_ROWSEQ, SPMV_VECTOR, SPMV_MERGE = 0, 1, 2, 3
+SPMV_AUTO, SPMV_ROWSEQ, SPMV_VECTOR, SPMV_MERGE, SPMV_VECTOR_STREAM = 0, 1, 2, 3, 4
 
 
 class LabError(RuntimeError):
@@ -58,6 +58,7 @@ _SIGS = {
     "lab_malloc": [C.POINTER(_p), C.c_size_t, _p],
     "lab_free": [_p, _p],
     "lab_memcpy": [_p, _p, C.c_size_t, _p],
+    "lab_wait_timeouts": [C.POINTER(_i64), _p],
     "lab_csr_create": [C.POINTER(_p), _i64, _i64, _i64, _p, _p, _p, _i, _p],
     "lab_csr_create_empty": [C.POINTER(_p), _i64, _i64, _i64, _p],
     "lab_csr_destroy": [_p],

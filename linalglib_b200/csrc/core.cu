@@ -103,6 +103,29 @@ namespace lab
             cudaFreeAsync(p, s);
     }
 
+    // One small device word per device for kernels to report bounded waits that
+    // ran out (word 0); allocated once and kept for the life of the process.
+    int* device_status_word()
+    {
+        static std::mutex mu;
+        static int*       words[64] = {};
+        int               dev       = 0;
+        if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+            return nullptr;
+        std::lock_guard<std::mutex> g(mu);
+        if(!words[dev])
+        {
+            int* p = nullptr;
+            if(cudaMalloc(&p, 64) != cudaSuccess || cudaMemset(p, 0, 64) != cudaSuccess)
+            {
+                cudaGetLastError();
+                return nullptr;
+            }
+            words[dev] = p;
+        }
+        return words[dev];
+    }
+
     lab_status pinned_scratch(void** p, size_t bytes)
     {
         static thread_local void*  buf = nullptr;
@@ -935,6 +958,22 @@ LAB_API lab_status lab_csr_clone(lab_csr A, lab_csr* B, lab_stream s)
     LAB_ARG(A && B, "null matrix");
     return lab_csr_create(B, A->m, A->n, A->nnz, A->row_ptr, A->col_ind, A->val, LAB_MEM_DEVICE,
                           s);
+}
+
+LAB_API lab_status lab_wait_timeouts(int64_t* count, lab_stream s)
+{
+    LAB_ARG(count, "null count");
+    LAB_TRY(ensure_init());
+    int* w = device_status_word();
+    if(!w)
+    {
+        set_error("device status word unavailable");
+        return LAB_CUDA_ERROR;
+    }
+    int h = 0;
+    LAB_TRY(copy_d2h_sync(&h, w, sizeof(int), to_stream(s)));
+    *count = h;
+    return LAB_OK;
 }
 
 LAB_API lab_status lab_csr_values_changed(lab_csr A, lab_stream ls)

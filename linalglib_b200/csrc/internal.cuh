@@ -161,6 +161,12 @@ namespace lab
         // LAB_SPMV_MERGE: merge-path split points
         int  merge_items_per_block = 0;
         int* merge_coords          = nullptr; // device int32[2*(nblocks+1)]
+        // streamed VECTOR form (vstream.cuh): rows per tile and stage capacity in
+        // entries (the largest tile plus alignment slack; 0: no stream geometry),
+        // and whether the plan uses it (LAB_SPMV_VECTOR_STREAM)
+        int st_rows = 0;
+        int st_cap  = 0;
+        int stream  = 0;
     };
 
     struct csr_values_lp

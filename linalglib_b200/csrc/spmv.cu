@@ -17,6 +17,25 @@ namespace lab
             atomicMax(maxlen, local);
     }
 
+    // Largest number of entries in a tile of `rows` consecutive rows.
+    __global__ void k_tile_max(const int32_t* __restrict__ rp, int64_t m, int rows, int* out)
+    {
+        int           local  = 0;
+        const int64_t ntiles = (m + rows - 1) / rows;
+        for(int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntiles;
+            t += (int64_t)gridDim.x * blockDim.x)
+        {
+            const int64_t r0 = t * rows;
+            const int64_t r1 = r0 + rows < m ? r0 + rows : m;
+            local            = max(local, rp[r1] - rp[r0]);
+        }
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            local = max(local, __shfl_xor_sync(0xffffffffu, local, o));
+        if((threadIdx.x & 31) == 0)
+            atomicMax(out, local);
+    }
+
     // 16-bit column offsets col - row, W lanes per row (coalesced over the row's
     // entries); *wide = 1 when some offset leaves the int16 range (the copy is
     // then discarded).
@@ -66,14 +85,31 @@ namespace lab
         spmv_plan& p = A->plan;
         if(p.analysed)
             return LAB_OK;
-        int stats[2] = {0, 0}; // longest row, offsets too wide for 16 bits
+        // longest row, offsets too wide for 16 bits, largest stream tile
+        int stats[3] = {0, 0, 0};
+        int st_rows  = 0;
         if(A->m > 0)
         {
             int* d = nullptr;
-            LAB_TRY(dalloc(&d, 2, s));
-            LAB_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(int), s));
+            LAB_TRY(dalloc(&d, 3, s));
+            LAB_CUDA(cudaMemsetAsync(d, 0, 3 * sizeof(int), s));
             unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(A->m, 256), 2048);
             LAB_LAUNCH(k_row_stats, grid, 256, 0, s, A->row_ptr, A->m, d);
+            if(A->m >= kStreamMinRows && A->nnz > 0)
+            {
+                // tiles of at most about kStreamTileEntries entries and a whole number
+                // of consumer passes (8 warps x 32 / W rows, W the lane count the
+                // VECTOR plan takes), so every consumer warp has rows in every tile;
+                // a multiple of 4 rows keeps the row-pointer copy 16-byte aligned
+                const double avg = (double)A->nnz / (double)A->m;
+                const int    w   = p.forced && p.alg == LAB_SPMV_VECTOR ? p.lanes
+                                                                       : pow2_at_most(avg / 5.0);
+                const int    rpp = kStreamConsumers * 32 / w;
+                st_rows = std::min(1024, rpp * std::max(1, (int)(kStreamTileEntries / avg / rpp)));
+                const int64_t nt = ceil_div<int64_t>(A->m, st_rows);
+                LAB_LAUNCH(k_tile_max, (unsigned)std::min<int64_t>(ceil_div<int64_t>(nt, 256), 1024),
+                           256, 0, s, A->row_ptr, A->m, st_rows, d + 2);
+            }
             // square matrices only: a prolongation's or restriction's col - row
             // spans the ratio of the two grids and does not fit
             const bool build = A->lp.dcol_state == 0 && A->nnz > 0 && A->m == A->n;
@@ -100,6 +136,11 @@ namespace lab
             lab_status st = copy_d2h_sync(stats, d, sizeof(stats), s);
             dfree(d, s);
             LAB_TRY(st);
+            // stage capacity: the largest tile plus the alignment slack of its copies
+            // (start rounded down to 16 bytes, quads read past the row end)
+            const int cap = stats[2] + 16;
+            p.st_rows     = st_rows > 0 && cap <= kStreamMaxCap ? st_rows : 0;
+            p.st_cap      = p.st_rows ? cap : 0;
             if(build)
             {
                 A->lp.dcol_state = stats[1] ? -1 : 1;
@@ -215,12 +256,15 @@ LAB_API lab_status lab_spmv_set_algorithm(lab_csr A, lab_spmv_alg alg, int lanes
     {
         A->plan.forced   = 0;
         A->plan.analysed = 0;
+        A->plan.stream   = 0;
         return LAB_OK;
     }
-    LAB_ARG(alg == LAB_SPMV_ROWSEQ || alg == LAB_SPMV_VECTOR || alg == LAB_SPMV_MERGE,
+    LAB_ARG(alg == LAB_SPMV_ROWSEQ || alg == LAB_SPMV_VECTOR || alg == LAB_SPMV_MERGE ||
+                alg == LAB_SPMV_VECTOR_STREAM,
             "unknown algorithm");
     A->plan.forced   = 1;
     A->plan.analysed = 0;
+    A->plan.stream   = alg == LAB_SPMV_VECTOR_STREAM;
     if(alg == LAB_SPMV_ROWSEQ)
     {
         A->plan.alg   = LAB_SPMV_ROWSEQ;
@@ -239,7 +283,9 @@ LAB_API lab_status lab_spmv_get_algorithm(lab_csr A, int* alg, int* lanes)
 {
     LAB_ARG(A, "null matrix");
     if(alg)
-        *alg = A->plan.alg;
+        *alg = A->plan.alg == LAB_SPMV_VECTOR && A->plan.stream && A->plan.st_rows > 0
+                   ? LAB_SPMV_VECTOR_STREAM
+                   : A->plan.alg;
     if(lanes)
         *lanes = A->plan.lanes;
     return LAB_OK;

@@ -625,6 +625,12 @@ namespace lab
         return LAB_OK;
     }
 
+}
+
+#include "vstream.cuh"
+
+namespace lab
+{
     template <class Op, class IT>
     lab_status launch_rowop_view(const lab_csr_impl* A, const csr_view<typename Op::val_t, IT>& V,
                                  const Op& op, cudaStream_t s, const red_buf& red)
@@ -642,17 +648,28 @@ namespace lab
             return launch_row_seg<Op, IT>(V, op, s, red);
         }
         const unsigned grid = (unsigned)rowop_grid(A);
+        lab_status     st   = LAB_OK;
         switch(p.lanes)
         {
         case 2:
+            if(launch_vstream<Op, 2, IT>(A, V, op, s, red, &st))
+                return st;
             return launch_vector<Op, 2, IT>(V, op, grid, s, red);
         case 4:
+            if(launch_vstream<Op, 4, IT>(A, V, op, s, red, &st))
+                return st;
             return launch_vector<Op, 4, IT>(V, op, grid, s, red);
         case 8:
+            if(launch_vstream<Op, 8, IT>(A, V, op, s, red, &st))
+                return st;
             return launch_vector<Op, 8, IT>(V, op, grid, s, red);
         case 16:
+            if(launch_vstream<Op, 16, IT>(A, V, op, s, red, &st))
+                return st;
             return launch_vector<Op, 16, IT>(V, op, grid, s, red);
         default:
+            if(launch_vstream<Op, 32, IT>(A, V, op, s, red, &st))
+                return st;
             return launch_vector<Op, 32, IT>(V, op, grid, s, red);
         }
     }

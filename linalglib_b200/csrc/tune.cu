@@ -3,7 +3,9 @@
 // matrix itself (CUDA events, back-to-back launches of y = A x) and keeps the
 // fastest.  Candidates: the one-thread-per-row pipeline (CSR-order accumulation,
 // bit-identical to the reference host SpMV) and, unless the caller asks for
-// bit-exact results, W = 2, 4, 8, 16, 32 lanes per row (reordered sums).  The
+// bit-exact results, W = 2, 4, 8, 16, 32 lanes per row (reordered sums), each
+// with the matrix read directly and, on operators large enough, streamed
+// through shared memory.  The
 // fused V-cycle passes (smoother, restriction, prolongation) run on the same
 // schedule as the plain SpMV of their matrix, so tuning a hierarchy tunes them.
 #include "amg.cuh"
@@ -21,6 +23,7 @@ namespace lab
         lab_status tune_one(lab_csr_impl* A, int exact, double* best_us, cudaStream_t s)
         {
             A->plan.forced   = 0;
+            A->plan.stream   = 0;
             A->plan.analysed = 0;
             LAB_TRY(spmv_analyse(A, s)); // row statistics (and the default plan)
             if(A->m == 0 || A->nnz == 0)
@@ -31,12 +34,16 @@ namespace lab
             }
             struct cand
             {
-                int alg, lanes;
+                int alg, lanes, stream;
             };
-            std::vector<cand> cands = {{LAB_SPMV_ROWSEQ, 1}};
+            std::vector<cand> cands = {{LAB_SPMV_ROWSEQ, 1, 0}};
             if(!exact)
                 for(int w : {2, 4, 8, 16, 32})
-                    cands.push_back({LAB_SPMV_VECTOR, w});
+                {
+                    cands.push_back({LAB_SPMV_VECTOR, w, 0});
+                    if(A->plan.st_rows > 0) // the streamed form where the matrix has one
+                        cands.push_back({LAB_SPMV_VECTOR, w, 1});
+                }
             dbuf<double> x, y;
             LAB_TRY(x.alloc((size_t)A->n + 1, s));
             LAB_TRY(y.alloc((size_t)A->m + 1, s));
@@ -49,8 +56,9 @@ namespace lab
             cand       win  = cands[0];
             for(const cand& c : cands)
             {
-                A->plan.alg   = c.alg;
-                A->plan.lanes = c.lanes;
+                A->plan.alg    = c.alg;
+                A->plan.lanes  = c.lanes;
+                A->plan.stream = c.stream;
                 op_spmv op{x.get(), y.get(), 1.0, 0.0};
                 for(int k = 0; k < kTuneWarm && st == LAB_OK; k++)
                     st = launch_rowop(A, A->val, op, s);
@@ -78,6 +86,7 @@ namespace lab
             cudaEventDestroy(e1);
             A->plan.alg    = win.alg;
             A->plan.lanes  = win.lanes;
+            A->plan.stream = win.stream;
             A->plan.forced = 1;
             if(st != LAB_OK)
                 return st;

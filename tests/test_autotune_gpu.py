@@ -28,7 +28,8 @@ def test_spmv_autotune_keeps_results(gpu, oracle, name):
     assert np.array_equal(y, y_ref)
     dA.autotune(exact=False)
     alg, lanes = dA.algorithm()
-    assert (alg, lanes) in [(L.SPMV_ROWSEQ, 1)] + [(L.SPMV_VECTOR, w) for w in (2, 4, 8, 16, 32)]
+    assert (alg, lanes) in [(L.SPMV_ROWSEQ, 1)] + [(a, w) for w in (2, 4, 8, 16, 32)
+                                                   for a in (L.SPMV_VECTOR, L.SPMV_VECTOR_STREAM)]
     y = dA.spmv(gpu.vec(x)).cpu().numpy()
     assert np.max(np.abs(y - y_ref)) <= 1e-9
 

@@ -87,3 +87,55 @@ def test_vector_matches_oracle(gpu, oracle, lanes):
     assert np.max(np.abs(y - yo)) <= 1e-9
     # deterministic: a second run is identical
     assert np.array_equal(A.spmv(gpu.vec(x)).cpu().numpy(), y)
+
+
+def _timeouts(gpu):
+    import ctypes as C
+    n = C.c_int64()
+    L.call("lab_wait_timeouts", C.byref(n), gpu.stream_handle())
+    return n.value
+
+
+@pytest.mark.parametrize("case", ["mean41", "spiky"])
+@pytest.mark.parametrize("lanes", [2, 4, 8, 16, 32])
+def test_vector_streamed_equals_direct(gpu, case, lanes):
+    """The streamed VECTOR schedule (the matrix moved through shared memory by bulk
+    copies, one producer warp) sums each row exactly as the direct-load kernel
+    does, so the results are bit-identical."""
+    rng = np.random.default_rng(77 + lanes)
+    lens = CASES[case](rng).astype(np.int64)
+    n = 60000
+    rp, ci, v = _csr_from_lens(np.minimum(lens, 800), n, rng, ints=False)
+    x = gpu.vec(rng.uniform(-1, 1, n))
+    y0 = rng.uniform(-1, 1, rp.size - 1)
+    A = gpu.CsrMatrix.from_arrays(rp, ci, v, n=n)
+    before = _timeouts(gpu)
+    out = {}
+    for alg in (L.SPMV_VECTOR, L.SPMV_VECTOR_STREAM):
+        A.set_algorithm(alg, lanes)
+        out[alg] = A.spmv(x, gpu.vec(y0), alpha=1.5, beta=-0.5).cpu().numpy()
+    assert A.algorithm() == (L.SPMV_VECTOR_STREAM, lanes)  # the matrix has a stream geometry
+    assert np.array_equal(out[L.SPMV_VECTOR].view(np.int64), out[L.SPMV_VECTOR_STREAM].view(np.int64))
+    assert _timeouts(gpu) == before
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP64, L.PREC_FP32, L.PREC_FP32_BF16])
+def test_cycle_streamed_equals_direct(gpu, prec):
+    """A V-cycle (FP64, FP32 and FP32 + BF16 values) whose large coarse operators
+    and restriction run streamed equals the default cycle (every VECTOR pass
+    reading global memory directly), bit for bit."""
+    from linalglib_b200 import problems as P
+    A = P.poisson3d(64)
+    dA = gpu.CsrMatrix.from_arrays(*A)
+    H = gpu.Hierarchy(dA)
+    r = gpu.vec(np.random.default_rng(1).uniform(-1, 1, A[0].size - 1))
+    mats = [H.A(l) for l in range(H.levels + 1)] + [H.R(l) for l in range(H.levels)]
+    vec_mats = [(M, M.algorithm()[1]) for M in mats if M.algorithm()[0] == L.SPMV_VECTOR]
+    assert any(M.m >= 8192 for M, _ in vec_mats)
+    M = gpu.Preconditioner.amg(H, gpu.amg_options(precision=prec))
+    z_direct = M.apply(r).cpu().numpy()
+    for Mx, w in vec_mats:
+        Mx.set_algorithm(L.SPMV_VECTOR_STREAM, w)
+    z_stream = M.apply(r).cpu().numpy()
+    assert np.array_equal(z_stream.view(np.int64), z_direct.view(np.int64))
+    assert _timeouts(gpu) == 0
