@@ -474,6 +474,13 @@ LAB_API lab_status lab_batched_pcg_solve(lab_csr A, lab_precond M, int nsys,
                                          const int64_t* offsets, const double* b, double* x,
                                          const lab_iter_control* c, int* iterations,
                                          int* converged, lab_solve_info* info, lab_stream s);
+/* Split nsys independent systems of the given costs (e.g. nonzeros) over nparts
+ * workers, one per GPU: part[k] in [0, nparts) for each system, size-balanced by
+ * the longest-processing-time greedy rule (largest first, to the least-loaded
+ * worker; deterministic).  Host only, no device needed.  The workers solve their
+ * systems independently (no collective on the data path); the caller gathers the
+ * solutions.  No reference counterpart (the reference has no multi-GPU code). */
+LAB_API lab_status lab_batch_partition(int nsys, const int64_t* cost, int nparts, int* part);
 /* Block PCG for nrhs right-hand sides of one matrix: B and X are n x nrhs
  * column-major (leading dimension n).  Every column has its own scalars and
  * stopping test; the products with A use SpMM (one pass over A per block of 8

@@ -106,6 +106,7 @@ _SIGS = {
     "lab_mtx_read": [_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_p),
                      C.POINTER(_p), C.POINTER(_p)],
     "lab_mtx_write": [_p, _i64, _i64, _i64, _p, _p, _p],
+    "lab_batch_partition": [_i, _p, _i, _p],
     "lab_csrtrsv_wait_control": [_p, _i64, _i64, _p],
     "lab_csr_triangle": [_p, _i, C.POINTER(_p), _p],
     "lab_csr_scale_diagonal": [_p, _d, _p],

@@ -107,6 +107,93 @@ namespace lab
             grad[j] = li * __ldg(x + ci[j]);
     }
 
+    // ================================================================ device-side loops
+    // A solver's iterations as ONE graph launch: a conditional WHILE node runs the
+    // captured iteration body again and again on the device.  A small kernel
+    // before the node and one at the end of each body pass set the node's
+    // condition: continue while *done == 0 and fewer than `limit` passes ran (the
+    // pass counter lives in device memory and is reset by the first kernel).  The
+    // host neither launches nor waits per iteration.
+    __global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* done, int* counter,
+                                int limit, int reset)
+    {
+        if(threadIdx.x == 0)
+        {
+            const int c = reset ? 0 : *counter + 1;
+            *counter    = c;
+            cudaGraphSetConditional(h, (*(volatile const int*)done == 0 && c < limit) ? 1u : 0u);
+        }
+    }
+
+    // Builds and instantiates the loop graph; `body(stream)` enqueues one iteration
+    // on the capturing stream.  *nodes receives the body's node count (kernel
+    // launches per pass, for the launch counter).  Returns LAB_NOT_SUPPORTED,
+    // with nothing built, where the driver has no conditional nodes.
+    template <class Body>
+    static lab_status build_loop_graph(cudaStream_t cap, const int* done, int* counter, int limit,
+                                       Body&& body, cudaGraphExec_t* out, int64_t* nodes)
+    {
+        *out             = nullptr;
+        cudaGraph_t    g = nullptr;
+        LAB_CUDA(cudaGraphCreate(&g, 0));
+        cudaGraphConditionalHandle h;
+        if(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+        {
+            cudaGetLastError();
+            cudaGraphDestroy(g);
+            return LAB_NOT_SUPPORTED;
+        }
+        lab_status  st = LAB_OK;
+        cudaError_t e  = cudaStreamBeginCaptureToGraph(cap, g, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeThreadLocal);
+        if(e == cudaSuccess)
+        {
+            k_loop_cond<<<1, 32, 0, cap>>>(h, done, counter, limit, 1);
+            cudaGraph_t gg = nullptr;
+            e              = cudaStreamEndCapture(cap, &gg);
+        }
+        cudaGraphNode_t pro = nullptr;
+        size_t          np  = 1;
+        if(e == cudaSuccess)
+            e = cudaGraphGetNodes(g, &pro, &np);
+        cudaGraphNodeParams cp = {};
+        cp.type                = cudaGraphNodeTypeConditional;
+        cp.conditional.handle  = h;
+        cp.conditional.type    = cudaGraphCondTypeWhile;
+        cp.conditional.size    = 1;
+        cudaGraphNode_t cn     = nullptr;
+        if(e == cudaSuccess)
+            e = cudaGraphAddNode(&cn, g, &pro, 1, &cp);
+        if(e == cudaSuccess)
+        {
+            cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+            e = cudaStreamBeginCaptureToGraph(cap, bodyg, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal);
+            if(e == cudaSuccess)
+            {
+                st = body(cap);
+                k_loop_cond<<<1, 32, 0, cap>>>(h, done, counter, limit, 0);
+                cudaGraph_t bg = nullptr;
+                e              = cudaStreamEndCapture(cap, &bg);
+                size_t n       = 0;
+                if(e == cudaSuccess && st == LAB_OK)
+                    e = cudaGraphGetNodes(bodyg, nullptr, &n);
+                *nodes = (int64_t)n;
+            }
+        }
+        if(e == cudaSuccess && st == LAB_OK)
+            e = cudaGraphInstantiate(out, g, 0);
+        cudaGraphDestroy(g);
+        if(st != LAB_OK)
+            return st;
+        if(e != cudaSuccess)
+        {
+            *out = nullptr;
+            return cuda_status(e, "loop graph", __FILE__, __LINE__);
+        }
+        return LAB_OK;
+    }
+
     // ================================================================ PCG
     enum
     {
@@ -127,6 +214,7 @@ namespace lab
         F_STATUS = 2,
         F_CONV   = 3,
         F_MAXIT  = 4,
+        F_LOOP   = 5, // passes of the device-side iteration loop
         F_COUNT  = 8
     };
 
@@ -153,6 +241,8 @@ namespace lab
         const double* key_x   = nullptr;
         uint64_t      key_A   = 0;
         cudaStream_t  key_s   = nullptr;
+        int           key_lim = 0; // max_iter + 1 the loop graph was built for
+        int           host_loop = 0; // 1: conditional nodes unavailable, host drives
         // iterative-refinement vectors (mixed precision): kept with the matrix so the
         // inner solve's iteration graph (keyed by its x = ir_e) is captured once
         double*       ir_r   = nullptr;
@@ -435,52 +525,75 @@ namespace lab
         LAB_LAUNCH(k_pcg_init, 1, 1, 0, s, w->sc, w->flags, ctl->rel_tol, ctl->abs_tol,
                    ctl->max_iter);
 
-        // iteration graph (rebuilt when the operands change)
-        if(!w->graph || w->key_M != M->uid || w->key_x != x || w->key_A != A->uid)
+        // iteration graph (rebuilt when the operands change): the whole iteration
+        // loop as one graph launch (conditional WHILE node, bounded by max_iter + 1
+        // passes), or, where conditional nodes are unavailable, one iteration per
+        // launch driven by the host
+        const int max_launch = ctl->max_iter + 1;
+        if(!w->graph || w->key_M != M->uid || w->key_x != x || w->key_A != A->uid ||
+           w->key_lim != max_launch)
         {
             if(w->graph)
                 cudaGraphExecDestroy(w->graph);
-            w->graph = nullptr;
-            cudaGraph_t g = nullptr;
-            LAB_CUDA(cudaStreamBeginCapture(w->cap, cudaStreamCaptureModeThreadLocal));
-            lab_status  st = pcg_iteration(A, M, x, w, w->cap);
-            cudaError_t ce = cudaStreamEndCapture(w->cap, &g);
-            if(st != LAB_OK && g)
+            w->graph         = nullptr;
+            const int64_t l0 = g_launches.load();
+            lab_status    st = w->host_loop
+                                   ? LAB_NOT_SUPPORTED
+                                   : build_loop_graph(
+                                         w->cap, w->flags + F_DONE, w->flags + F_LOOP, max_launch,
+                                         [&](cudaStream_t c) { return pcg_iteration(A, M, x, w, c); },
+                                         &w->graph, &w->graph_nodes);
+            if(st == LAB_NOT_SUPPORTED)
+            {
+                w->host_loop = 1;
+                cudaGraph_t g = nullptr;
+                LAB_CUDA(cudaStreamBeginCapture(w->cap, cudaStreamCaptureModeThreadLocal));
+                st             = pcg_iteration(A, M, x, w, w->cap);
+                cudaError_t ce = cudaStreamEndCapture(w->cap, &g);
+                if(st != LAB_OK && g)
+                    cudaGraphDestroy(g);
+                LAB_TRY(st);
+                LAB_CUDA(ce);
+                size_t nodes = 0;
+                cudaGraphGetNodes(g, nullptr, &nodes);
+                w->graph_nodes = (int64_t)nodes;
+                ce             = cudaGraphInstantiate(&w->graph, g, 0);
                 cudaGraphDestroy(g);
+                LAB_CUDA(ce);
+            }
             LAB_TRY(st);
-            LAB_CUDA(ce);
-            size_t nodes = 0;
-            cudaGraphGetNodes(g, nullptr, &nodes);
-            w->graph_nodes = (int64_t)nodes;
-            // the captured launches were counted once at capture; replays add them again
-            g_launches.fetch_sub(w->graph_nodes);
-            ce = cudaGraphInstantiate(&w->graph, g, 0);
-            cudaGraphDestroy(g);
-            LAB_CUDA(ce);
-            w->key_M = M->uid;
-            w->key_x = x;
-            w->key_A = A->uid;
-            w->key_s = s;
+            // launches counted while capturing are counted again as they run
+            g_launches.fetch_sub(g_launches.load() - l0);
+            w->key_M   = M->uid;
+            w->key_x   = x;
+            w->key_A   = A->uid;
+            w->key_s   = s;
+            w->key_lim = max_launch;
         }
-        // Pipelined host loop: iteration k+1 is queued before the flags of
-        // iteration k are inspected; a queued iteration after convergence is a
-        // no-op because every kernel checks flags[F_DONE] first.
-        const int max_launch = ctl->max_iter + 1;
-        int       launched   = 0;
-        for(; launched < max_launch; launched++)
+        if(!w->host_loop)
         {
             LAB_CUDA(cudaGraphLaunch(w->graph, s));
-            g_launches.fetch_add(w->graph_nodes, std::memory_order_relaxed);
-            int slot = launched & 1;
-            LAB_CUDA(cudaMemcpyAsync(w->hflags + slot * F_COUNT, w->flags, sizeof(int) * F_COUNT,
-                                     cudaMemcpyDeviceToHost, s));
-            LAB_CUDA(cudaEventRecord(w->ev[slot], s));
-            if(launched >= 1)
+        }
+        else
+        {
+            // Pipelined host loop: iteration k+1 is queued before the flags of
+            // iteration k are inspected; a queued iteration after convergence is a
+            // no-op because every kernel checks flags[F_DONE] first.
+            for(int launched = 0; launched < max_launch; launched++)
             {
-                int prev = (launched - 1) & 1;
-                LAB_CUDA(cudaEventSynchronize(w->ev[prev]));
-                if(w->hflags[prev * F_COUNT + F_DONE])
-                    break;
+                LAB_CUDA(cudaGraphLaunch(w->graph, s));
+                g_launches.fetch_add(w->graph_nodes, std::memory_order_relaxed);
+                int slot = launched & 1;
+                LAB_CUDA(cudaMemcpyAsync(w->hflags + slot * F_COUNT, w->flags,
+                                         sizeof(int) * F_COUNT, cudaMemcpyDeviceToHost, s));
+                LAB_CUDA(cudaEventRecord(w->ev[slot], s));
+                if(launched >= 1)
+                {
+                    int prev = (launched - 1) & 1;
+                    LAB_CUDA(cudaEventSynchronize(w->ev[prev]));
+                    if(w->hflags[prev * F_COUNT + F_DONE])
+                        break;
+                }
             }
         }
         cudaEventRecord(t1, s);
@@ -488,6 +601,9 @@ namespace lab
         double hs[S_COUNT];
         LAB_TRY(copy_d2h_sync(hf, w->flags, sizeof(hf), s));
         LAB_TRY(copy_d2h_sync(hs, w->sc, sizeof(hs), s));
+        if(!w->host_loop) // the loop's passes ran on the device: prologue + passes x body
+            g_launches.fetch_add(1 + (int64_t)hf[F_LOOP] * w->graph_nodes,
+                                 std::memory_order_relaxed);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, t0, t1);
         cudaEventDestroy(t0);
@@ -1034,7 +1150,8 @@ namespace lab
         GF_STATUS = 3,
         GF_N      = 4
     };
-    // global flags: [0] = all done, [1] = active segments, [2] = max_iter
+    // global flags: [0] = all done, [1] = active segments, [2] = max_iter,
+    // [3] = passes of the device-side iteration loop
     struct seg_ws
     {
         int           nseg   = 0;
@@ -1333,47 +1450,77 @@ namespace lab
             k_seg_init<<<1, 1, 0, s>>>(w.sc, w.sf, w.gflags, nseg, ctl->max_iter);
             g_launches.fetch_add(4);
 
-            // one iteration as a graph (captured on a private stream)
+            // the iterations as one graph launch (a device-side WHILE loop of at
+            // most max_iter + 1 passes that stops once every system has retired);
+            // where conditional nodes are unavailable, one launch per iteration
             if(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
             {
                 st = LAB_CUDA_ERROR;
                 break;
             }
-            cudaGraph_t g = nullptr;
-            if(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            auto iteration = [&](cudaStream_t c) -> lab_status {
+                lab_status r = seg_apply_A(o, w, w.p, w.q, c, skip);
+                k_seg_reduce<0><<<grid, 256, 0, c>>>(w.off, w.p, w.q, w.sc, G_PQ, w.sf, w.gflags,
+                                                     red(2), tik(2), 1);
+                k_seg_update<<<grid, 256, 0, c>>>(w.off, x, w.r, w.p, w.q, w.sc, w.sf, w.gflags,
+                                                  red(3), tik(3), ctl->rel_tol, ctl->abs_tol);
+                if(r == LAB_OK)
+                    r = seg_apply_M(o, w, w.r, w.z, c, skip);
+                k_seg_reduce<0><<<grid, 256, 0, c>>>(w.off, w.z, w.r, w.sc, G_GNEW, w.sf, w.gflags,
+                                                     red(1), tik(1), 1);
+                k_seg_pupdate<<<grid, 256, 0, c>>>(w.off, w.p, w.z, w.sc, w.sf, w.gflags, tik(0));
+                return r;
+            };
+            const int     limit = ctl->max_iter + 1;
+            const int64_t l0    = g_launches.load();
+            int64_t       nodes = 0;
+            st = build_loop_graph(cap, w.gflags, w.gflags + 3, limit, iteration, &gexec, &nodes);
+            const bool device_loop = st == LAB_OK;
+            if(st == LAB_NOT_SUPPORTED)
             {
-                st = LAB_CUDA_ERROR;
+                cudaGraph_t g = nullptr;
+                if(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+                {
+                    st = LAB_CUDA_ERROR;
+                    break;
+                }
+                st             = iteration(cap);
+                cudaError_t ce = cudaStreamEndCapture(cap, &g);
+                if(st != LAB_OK || ce != cudaSuccess)
+                {
+                    if(g)
+                        cudaGraphDestroy(g);
+                    if(st == LAB_OK)
+                        st = cuda_status(ce, "batched PCG capture", __FILE__, __LINE__);
+                    break;
+                }
+                size_t n = 0;
+                cudaGraphGetNodes(g, nullptr, &n);
+                nodes = (int64_t)n;
+                ce    = cudaGraphInstantiate(&gexec, g, 0);
+                cudaGraphDestroy(g);
+                if(ce != cudaSuccess)
+                {
+                    st = cuda_status(ce, "batched PCG instantiate", __FILE__, __LINE__);
+                    break;
+                }
+            }
+            if(st != LAB_OK)
+                break;
+            // launches counted while capturing are counted again as they run
+            g_launches.fetch_sub(g_launches.load() - l0);
+            if(device_loop)
+            {
+                if(cudaGraphLaunch(gexec, s) != cudaSuccess)
+                {
+                    st = LAB_CUDA_ERROR;
+                    break;
+                }
+                int passes = 0;
+                st         = copy_d2h_sync(&passes, w.gflags + 3, sizeof(int), s);
+                g_launches.fetch_add(1 + (int64_t)passes * nodes);
                 break;
             }
-            st = seg_apply_A(o, w, w.p, w.q, cap, skip);
-            k_seg_reduce<0><<<grid, 256, 0, cap>>>(w.off, w.p, w.q, w.sc, G_PQ, w.sf, w.gflags,
-                                                   red(2), tik(2), 1);
-            k_seg_update<<<grid, 256, 0, cap>>>(w.off, x, w.r, w.p, w.q, w.sc, w.sf, w.gflags,
-                                                red(3), tik(3), ctl->rel_tol, ctl->abs_tol);
-            if(st == LAB_OK)
-                st = seg_apply_M(o, w, w.r, w.z, cap, skip);
-            k_seg_reduce<0><<<grid, 256, 0, cap>>>(w.off, w.z, w.r, w.sc, G_GNEW, w.sf, w.gflags,
-                                                   red(1), tik(1), 1);
-            k_seg_pupdate<<<grid, 256, 0, cap>>>(w.off, w.p, w.z, w.sc, w.sf, w.gflags, tik(0));
-            cudaError_t ce = cudaStreamEndCapture(cap, &g);
-            if(st != LAB_OK || ce != cudaSuccess)
-            {
-                if(g)
-                    cudaGraphDestroy(g);
-                if(st == LAB_OK)
-                    st = cuda_status(ce, "batched PCG capture", __FILE__, __LINE__);
-                break;
-            }
-            size_t nodes = 0;
-            cudaGraphGetNodes(g, nullptr, &nodes);
-            ce = cudaGraphInstantiate(&gexec, g, 0);
-            cudaGraphDestroy(g);
-            if(ce != cudaSuccess)
-            {
-                st = cuda_status(ce, "batched PCG instantiate", __FILE__, __LINE__);
-                break;
-            }
-            g_launches.fetch_sub(4); // capture-time launches of the 4 segmented kernels
             if(cudaMallocHost(&hf, sizeof(int) * 8) != cudaSuccess)
             {
                 st = LAB_OOM;
@@ -1381,14 +1528,14 @@ namespace lab
             }
             cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
             cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
-            for(int it = 0; it <= ctl->max_iter; it++)
+            for(int it = 0; it < limit; it++)
             {
                 if(cudaGraphLaunch(gexec, s) != cudaSuccess)
                 {
                     st = LAB_CUDA_ERROR;
                     break;
                 }
-                g_launches.fetch_add((int64_t)nodes);
+                g_launches.fetch_add(nodes);
                 int slot = it & 1;
                 cudaMemcpyAsync(hf + slot * 4, w.gflags, sizeof(int) * 4, cudaMemcpyDeviceToHost,
                                 s);

@@ -114,7 +114,18 @@ def test_vector_streamed_equals_direct(gpu, case, lanes):
     for alg in (L.SPMV_VECTOR, L.SPMV_VECTOR_STREAM):
         A.set_algorithm(alg, lanes)
         out[alg] = A.spmv(x, gpu.vec(y0), alpha=1.5, beta=-0.5).cpu().numpy()
-    assert A.algorithm() == (L.SPMV_VECTOR_STREAM, lanes)  # the matrix has a stream geometry
+    # the library's tile rule: whole consumer passes (8 warps x 32 / W rows) of about
+    # 2048 entries; the matrix streams if its largest tile (+16) fits 4096 entries
+    m = rp.size - 1
+    avg = rp[-1] / m
+    rpp = 8 * 32 // lanes
+    rows = min(1024, rpp * max(1, int(2048 / avg / rpp)))
+    r0 = np.arange(0, m, rows)
+    biggest = int(np.max(rp[np.minimum(r0 + rows, m)] - rp[r0]))
+    streams = m >= 8192 and biggest + 16 <= 4096
+    assert A.algorithm() == ((L.SPMV_VECTOR_STREAM if streams else L.SPMV_VECTOR), lanes)
+    if case == "mean41" and lanes == 8:
+        assert streams
     assert np.array_equal(out[L.SPMV_VECTOR].view(np.int64), out[L.SPMV_VECTOR_STREAM].view(np.int64))
     assert _timeouts(gpu) == before
 
