@@ -60,6 +60,11 @@ def parse():
                     help="operator of --mode spmv (default 3D 7-point Poisson) and --mode "
                          "mixed (default the 27-point diffusion operator)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--level", type=int, default=0,
+                    help="--mode spmv: time the SpMV of hierarchy level L's operator A_L "
+                         "(0: the input matrix)")
+    ap.add_argument("--spmv-alg", default=None, choices=["rowseq", "vector", "stream"],
+                    help="--mode spmv: force a schedule (default: the analysed plan)")
     ap.add_argument("--mode", default="full",
                     choices=["full", "profile", "spmv", "mixed", "batched", "batched_split",
                              "adjoint", "tri"],
@@ -296,7 +301,8 @@ def run_reference(args, d):
 
 
 # ------------------------------------------------------------------ our arm
-def dominant_kernel_roofline(core, dA, m, nnz, torch, profiled=True):
+def dominant_kernel_roofline(core, dA, m, nnz, torch, profiled=True,
+                             label="A_0 (level-0 CSR pass)"):
     """CUDA-event timing of the dominant kernel class (level-0 CSR pass: SpMV on
     the 128^3 operator, the same row engine as the smoother kernels): 20 launches
     back to back between two events on the launching stream, three times; A_0
@@ -336,9 +342,10 @@ def dominant_kernel_roofline(core, dA, m, nnz, torch, profiled=True):
         if mt:
             traffic = float(mt.group(1))
     alg, lanes = dA.algorithm()
-    kname = ("k_pipe<op_spmv> (one thread per row, staged tiles)" if alg == 1
-             else f"k_vector<op_spmv> ({lanes} lanes per row)")
-    return {"bound": "hbm", "kernel": kname + " on A_0 (level-0 CSR pass)",
+    kname = {1: "k_pipe<op_spmv> (one thread per row, staged tiles)",
+             4: f"k_vstream<op_spmv> ({lanes} lanes per row, bulk-copy stage ring)"}.get(
+        alg, f"k_vector<op_spmv> ({lanes} lanes per row)")
+    return {"bound": "hbm", "kernel": kname + " on " + label,
             "achieved": achieved, "peak": peak, "peak_source": which, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": algo,
             "index_bytes_per_entry": ib,
@@ -397,13 +404,25 @@ def run_ours(args, d):
     dA = core.CsrMatrix.from_arrays(*A)
     dA.analyse()
     if args.mode == "spmv":
-        roof = dominant_kernel_roofline(core, dA, m, nnz, torch,
+        target, H = dA, None
+        if args.level > 0:
+            H = core.Hierarchy(dA)
+            target = H.A(min(args.level, H.levels))
+            m, _, nnz = target.info()
+        if args.spmv_alg:
+            lanes = target.algorithm()[1]
+            alg = {"rowseq": L.SPMV_ROWSEQ, "vector": L.SPMV_VECTOR,
+                   "stream": L.SPMV_VECTOR_STREAM}[args.spmv_alg]
+            target.set_algorithm(alg, lanes if lanes > 1 else 0)
+        roof = dominant_kernel_roofline(core, target, m, nnz, torch,
                                         profiled=(args.matrix or "poisson") == "poisson"
-                                        and args.n == 128)
+                                        and args.n == 128 and args.level == 0
+                                        and not args.spmv_alg,
+                                        label=f"A_{args.level}")
         if d.rank == 0:
             print(json.dumps({"mode": "spmv", "matrix": f"{args.matrix or 'poisson'} {args.n}^3",
-                              "rows": int(m),
-                              "nnz": int(nnz), "roofline": roof}), flush=True)
+                              "level": args.level, "schedule": list(target.algorithm()),
+                              "rows": int(m), "nnz": int(nnz), "roofline": roof}), flush=True)
         d.close()
         return 0
     bd = core.vec(b)

@@ -4,6 +4,7 @@
 #include "tri.cuh"
 
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -125,6 +126,18 @@ namespace lab
         }
     }
 
+    // LAB_SOLVE_HOST_LOOP=1 in the environment makes the host drive the iterations
+    // (one graph launch per iteration, the same kernels): kernel profilers cannot
+    // attribute kernels inside graphs that hold conditional nodes.
+    static bool host_loop_forced()
+    {
+        static const bool forced = [] {
+            const char* e = std::getenv("LAB_SOLVE_HOST_LOOP");
+            return e && e[0] == '1';
+        }();
+        return forced;
+    }
+
     // Builds and instantiates the loop graph; `body(stream)` enqueues one iteration
     // on the capturing stream.  *nodes receives the body's node count (kernel
     // launches per pass, for the launch counter).  Returns LAB_NOT_SUPPORTED,
@@ -134,6 +147,8 @@ namespace lab
                                        Body&& body, cudaGraphExec_t* out, int64_t* nodes)
     {
         *out             = nullptr;
+        if(host_loop_forced())
+            return LAB_NOT_SUPPORTED;
         cudaGraph_t    g = nullptr;
         LAB_CUDA(cudaGraphCreate(&g, 0));
         cudaGraphConditionalHandle h;

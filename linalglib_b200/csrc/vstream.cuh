@@ -35,7 +35,7 @@ namespace lab
 {
     constexpr int      kStreamConsumers = 8;
     constexpr int      kStreamNT        = 32 * (kStreamConsumers + 1);
-    constexpr int      kStreamStages    = 4;
+    constexpr int      kStreamStages    = 2;
     constexpr unsigned kStreamWaitLimit = 1u << 22;
     // operators with fewer rows keep k_vector (a few tiles cannot fill the GPU)
     constexpr int64_t kStreamMinRows = 8192;
@@ -185,10 +185,26 @@ namespace lab
         double        contrib = 0.0;
         if(warp == 0)
         {
-            if(lane == 0)
+            // the whole producer warp walks the tiles; every 32 tiles each lane loads
+            // the entry bounds of one upcoming tile (one warp-wide load instead of a
+            // dependent round trip per tile), and lane 0 issues the copies
+            int it = 0, jb0 = 0, jb1 = 0;
+            for(int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++)
             {
-                int it = 0;
-                for(int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++)
+                const int k = it & 31;
+                if(k == 0)
+                {
+                    const int t = tile + lane * gridDim.x;
+                    if(t < ntiles)
+                    {
+                        jb0 = A.rp[t * rows];
+                        jb1 = A.rp[min(t * rows + rows, A.m)];
+                    }
+                }
+                const int j0 = __shfl_sync(0xffffffffu, jb0, k);
+                const int j1 = __shfl_sync(0xffffffffu, jb1, k);
+                int stop = 0;
+                if(lane == 0)
                 {
                     const int      st = it % kStreamStages;
                     const unsigned ph = (unsigned)(it / kStreamStages) & 1u;
@@ -198,27 +214,34 @@ namespace lab
                         if(!*abort_v)
                             atomicAdd(status, 1);
                         *abort_v = 1;
-                        break;
+                        stop     = 1;
                     }
-                    const int      r0   = tile * rows;
-                    const int      r1   = min(r0 + rows, A.m);
-                    const int      j0   = A.rp[r0];
-                    const int      j1   = A.rp[r1];
-                    const int      j0v  = j0 & ~(VPC - 1);
-                    const int      j0c  = j0 & ~(CPC - 1);
-                    const unsigned bv   = (unsigned)round16((size_t)(j1 - j0v) * sizeof(VT));
-                    const unsigned bc   = (unsigned)round16((size_t)(j1 - j0c) * sizeof(IT));
-                    const unsigned br   = (unsigned)round16((size_t)(r1 - r0 + 1) * sizeof(int32_t));
-                    unsigned char* base = smem_stream + (size_t)st * stage_b;
-                    mbar_arrive_expect_tx(&full[st], bv + bc + br);
-                    bulk_g2s(base + sv_b + sc_b, A.rp + r0, br, &full[st]);
-                    if(bv)
-                        bulk_g2s(base, A.v + j0v, bv, &full[st]);
-                    if(bc)
-                        bulk_g2s(base + sv_b, A.ci + j0c, bc, &full[st]);
+                    else
+                    {
+                        const int      r0   = tile * rows;
+                        const int      r1   = min(r0 + rows, A.m);
+                        const int      j0v  = j0 & ~(VPC - 1);
+                        const int      j0c  = j0 & ~(CPC - 1);
+                        const unsigned bv   = (unsigned)round16((size_t)(j1 - j0v) * sizeof(VT));
+                        const unsigned bc   = (unsigned)round16((size_t)(j1 - j0c) * sizeof(IT));
+                        const unsigned br   = (unsigned)round16((size_t)(r1 - r0 + 1) * sizeof(int32_t));
+                        unsigned char* base = smem_stream + (size_t)st * stage_b;
+                        mbar_arrive_expect_tx(&full[st], bv + bc + br);
+                        bulk_g2s(base + sv_b + sc_b, A.rp + r0, br, &full[st]);
+                        if(bv)
+                            bulk_g2s(base, A.v + j0v, bv, &full[st]);
+                        if(bc)
+                            bulk_g2s(base + sv_b, A.ci + j0c, bc, &full[st]);
+                    }
                 }
+                if(__shfl_sync(0xffffffffu, stop, 0))
+                    break;
+            }
+            if(lane == 0)
+            {
                 // no copy may land after the CTA has left: wait for the copies of
-                // the last stages issued (their phases complete as the bytes arrive)
+                // the last stages issued (their phases complete as the bytes arrive);
+                // `it` counts the tiles whose copies were issued
                 for(int k = max(0, it - kStreamStages); k < it; k++)
                 {
                     const int      st = k % kStreamStages;
