@@ -341,6 +341,26 @@ LAB_API lab_status lab_hierarchy_setup_ms(lab_hierarchy h, double* ms);
  * creating preconditioners on h: iteration graphs captured earlier keep their
  * schedules (their results stay correct). */
 LAB_API lab_status lab_hierarchy_autotune(lab_hierarchy h, int exact, lab_stream s);
+/* SpGEMM table sizing tuner: time C = A*B under every sizing of the hash row classes
+ * (the symbolic tables' size against the product bound, the numeric tables' fill) and
+ * keep the fastest for products of matrices of A's and B's shapes; later products of
+ * such shapes (lab_spgemm, the Galerkin products of lab_amg_setup) use it.  The
+ * results do not depend on the sizing (every class accumulates in the reference's
+ * order).  lab_hierarchy_tune_products tunes both Galerkin products of every level of
+ * a built hierarchy, so the next setup of the same operator runs tuned.  No
+ * counterpart in the reference (its SpGEMM descriptors, linalg_math.h:408-440, hold
+ * no tuning). */
+LAB_API lab_status lab_spgemm_autotune(lab_csr A, lab_csr B, double* best_us, lab_stream s);
+LAB_API lab_status lab_hierarchy_tune_products(lab_hierarchy h, lab_stream s);
+/* The tuned plans (SpMV schedules from lab_spmv_autotune / lab_hierarchy_autotune,
+ * SpGEMM sizings) are cached per process, keyed by the operands' shapes (rows,
+ * columns, nonzeros; SpMV also by exactness): a matrix of a cached shape is not timed
+ * again.  save / load keep the cache in a text file across processes (a file with a
+ * bad header or entry is refused with LAB_BAD_ARG and nothing is loaded); clear empties
+ * it.  Host only. */
+LAB_API lab_status lab_tune_cache_save(const char* path);
+LAB_API lab_status lab_tune_cache_load(const char* path);
+LAB_API lab_status lab_tune_cache_clear(void);
 LAB_API lab_status lab_hierarchy_save(lab_hierarchy h, const char* path, lab_stream s);
 LAB_API lab_status lab_hierarchy_load(const char* path, lab_hierarchy* h, lab_stream s);
 

@@ -120,6 +120,11 @@ _SIGS = {
     "lab_precond_create_ssor": [_p, _d, C.POINTER(_p), _p],
     "lab_spmv_autotune": [_p, _i, C.POINTER(_d), _p],
     "lab_hierarchy_autotune": [_p, _i, _p],
+    "lab_spgemm_autotune": [_p, _p, C.POINTER(_d), _p],
+    "lab_hierarchy_tune_products": [_p, _p],
+    "lab_tune_cache_save": [C.c_char_p],
+    "lab_tune_cache_load": [C.c_char_p],
+    "lab_tune_cache_clear": [],
     "lab_hierarchy_save": [_p, C.c_char_p, _p],
     "lab_hierarchy_load": [C.c_char_p, C.POINTER(_p), _p],
     "lab_amg_cycle": [_p, C.POINTER(AmgOptions), _p, _p, _p],

@@ -65,8 +65,23 @@ namespace lab
 
     // sparse products (spgemm.cu)
     lab_status transpose(const lab_csr_impl* A, lab_csr_impl** T, cudaStream_t s);
+    // Table sizing of the hash SpGEMM row classes (spgemm.cu gemm_class): symbolic
+    // tables hold >= sym / 2 x the row's product bound, numeric tables are filled to
+    // at most fill_num / fill_den.  Results do not depend on it (only table sizes).
+    struct gemm_tune
+    {
+        int sym      = 2;
+        int fill_num = 3;
+        int fill_den = 4;
+    };
+    // The tuned sizing for products of matrices of A's and B's shapes (tune.cu
+    // cache; the defaults when none was tuned) and its store.
+    gemm_tune gemm_tune_lookup(const lab_csr_impl* A, const lab_csr_impl* B);
+    void      gemm_tune_store(const lab_csr_impl* A, const lab_csr_impl* B, gemm_tune t);
     lab_status spgemm(const lab_csr_impl* A, const lab_csr_impl* B, lab_csr_impl** C,
                       cudaStream_t s);
+    lab_status spgemm_tuned(const lab_csr_impl* A, const lab_csr_impl* B, lab_csr_impl** C,
+                            cudaStream_t s, gemm_tune tune);
     lab_status row_lengths(const int32_t* rp, int64_t m, int32_t* len, cudaStream_t s);
     lab_status spgeam(double alpha, const lab_csr_impl* A, double beta, const lab_csr_impl* B,
                       lab_csr_impl** C, cudaStream_t s);

@@ -1,5 +1,6 @@
 // SpGEMM, SpGEAM and transpose on the ESC engine (esc.cuh), plus the tier
 // classification shared with the AMG prolongation builders.
+#include "amg.cuh"
 #include "esc.cuh"
 
 namespace lab
@@ -686,29 +687,33 @@ namespace lab
     // larger row and checks for overflow, and its overflow rows get 4096 slots).  Numeric (by the exact column count of
     // rows with ub > 32): 1..6 = tables of 64..2048 slots (count <= 3/4 of the
     // slots), 7 = global sort tier.
-    __device__ __forceinline__ int gemm_class(int phase, int ub, int cnt)
+    // Row class of a product row.  Phase 0 (symbolic, by the product bound ub): the
+    // smallest table of 128..1024 slots with slots >= sym / 2 x ub (sym = 2 by
+    // default; the bound is loose for Galerkin products, many products per column,
+    // and rows that fill 3/4 of the 1024-slot table are retried with 4096 slots, then
+    // the global sort tier).  Phase 1 (numeric, by the exact count): the smallest
+    // table of 64..2048 slots filled to at most fill_num / fill_den (3/4 by default:
+    // fewer slots to clear and compact, more tables per SM, a few more probes);
+    // larger rows go to the sort tier.  The class only sizes the table: every class
+    // accumulates in the same order, so results do not depend on the tuning.
+    __device__ __forceinline__ int gemm_class(int phase, int ub, int cnt, gemm_tune t)
     {
         if(ub <= kEscLaneCap)
             return 0;
         if(phase == 0)
         {
-            // the bound is loose for Galerkin products (many products per column):
-            // rows bounded above 512 start in the 1024-slot table and only the ones
-            // that fill it are retried with 4096 slots (then the global sort tier)
             int c = 1, hs = 128;
-            while(c < 4 && 2 * ub > hs)
+            while(c < 4 && t.sym * ub > 2 * hs)
             {
                 c++;
                 hs <<= 1;
             }
             return c;
         }
-        // exact counts: a table may fill to 3/4 (fewer slots to clear and compact,
-        // twice the occupancy of a half-full table, a few more probes)
-        if(4 * cnt > 3 * 2048)
+        if(t.fill_den * cnt > t.fill_num * 2048)
             return 7;
         int c = 1, hs = 64;
-        while(4 * cnt > 3 * hs)
+        while(t.fill_den * cnt > t.fill_num * hs)
         {
             c++;
             hs <<= 1;
@@ -717,7 +722,8 @@ namespace lab
     }
 
     __global__ void k_gemm_class_count(int phase, const int32_t* __restrict__ upper,
-                                       const int32_t* __restrict__ rp, int64_t m, int* hist)
+                                       const int32_t* __restrict__ rp, int64_t m, int* hist,
+                                       gemm_tune t)
     {
         __shared__ int sh[kHashClasses];
         if(threadIdx.x < kHashClasses)
@@ -729,7 +735,7 @@ namespace lab
             const int64_t i = base + threadIdx.x;
             int           c = -1;
             if(i < m)
-                c = gemm_class(phase, upper[i], rp ? rp[i + 1] - rp[i] : 0);
+                c = gemm_class(phase, upper[i], rp ? rp[i + 1] - rp[i] : 0, t);
             warp_append(sh, c, kHashClasses);
         }
         __syncthreads();
@@ -739,7 +745,7 @@ namespace lab
 
     __global__ void k_gemm_class_fill(int phase, const int32_t* __restrict__ upper,
                                       const int32_t* __restrict__ rp, int64_t m, int* cursor,
-                                      int32_t* rows)
+                                      int32_t* rows, gemm_tune t)
     {
         for(int64_t base = blockIdx.x * (int64_t)blockDim.x; base < m;
             base += (int64_t)gridDim.x * blockDim.x)
@@ -747,7 +753,7 @@ namespace lab
             const int64_t i = base + threadIdx.x;
             int           c = -1;
             if(i < m)
-                c = gemm_class(phase, upper[i], rp ? rp[i + 1] - rp[i] : 0);
+                c = gemm_class(phase, upper[i], rp ? rp[i + 1] - rp[i] : 0, t);
             const int p = warp_append(cursor, c, kHashClasses);
             if(c >= 0)
                 rows[p] = (int32_t)i;
@@ -773,11 +779,12 @@ namespace lab
     // anyway: the count kernel and an asynchronous copy of the histogram into
     // pinned host memory, then (after the sync) the class starts and the fill.
     static lab_status gemm_class_count(int phase, const int32_t* upper, const int32_t* rp,
-                                       int64_t m, int* dev_hist, int* host_hist, cudaStream_t s)
+                                       int64_t m, int* dev_hist, int* host_hist, cudaStream_t s,
+                                       gemm_tune t)
     {
         LAB_CUDA(cudaMemsetAsync(dev_hist, 0, sizeof(int) * kHashClasses, s));
         const unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(m, 256), 4096);
-        LAB_LAUNCH(k_gemm_class_count, grid, 256, 0, s, phase, upper, rp, m, dev_hist);
+        LAB_LAUNCH(k_gemm_class_count, grid, 256, 0, s, phase, upper, rp, m, dev_hist, t);
         LAB_CUDA(cudaMemcpyAsync(host_hist, dev_hist, sizeof(int) * kHashClasses,
                                  cudaMemcpyDeviceToHost, s));
         return LAB_OK;
@@ -785,7 +792,7 @@ namespace lab
 
     static lab_status gemm_class_fill(int phase, const int32_t* upper, const int32_t* rp,
                                       int64_t m, const int* host_hist, int* dev_start,
-                                      gemm_classes& g, cudaStream_t s)
+                                      gemm_classes& g, cudaStream_t s, gemm_tune t)
     {
         for(int c = 0; c < kHashClasses; c++)
             g.start[c + 1] = g.start[c] + host_hist[c];
@@ -794,7 +801,7 @@ namespace lab
         LAB_TRY(g.rows.alloc((size_t)m + 1, s));
         const unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(m, 256), 4096);
         LAB_LAUNCH(k_gemm_class_fill, grid, 256, 0, s, phase, upper, rp, m, dev_start,
-                   g.rows.get());
+                   g.rows.get(), t);
         return LAB_OK;
     }
 
@@ -916,6 +923,12 @@ namespace lab
     lab_status spgemm(const lab_csr_impl* A, const lab_csr_impl* B, lab_csr_impl** C,
                       cudaStream_t s)
     {
+        return spgemm_tuned(A, B, C, s, gemm_tune_lookup(A, B));
+    }
+
+    lab_status spgemm_tuned(const lab_csr_impl* A, const lab_csr_impl* B, lab_csr_impl** C,
+                            cudaStream_t s, gemm_tune tune)
+    {
         if(A->n != B->m)
         {
             set_error("spgemm: inner dimensions differ (%lld vs %lld)", (long long)A->n,
@@ -942,7 +955,7 @@ namespace lab
         dbuf<int> dh;
         LAB_TRY(dh.alloc(4 * kHashClasses, s));
         if(m > 0)
-            LAB_TRY(gemm_class_count(0, upper.get(), nullptr, m, dh.get(), hp + 1, s));
+            LAB_TRY(gemm_class_count(0, upper.get(), nullptr, m, dh.get(), hp + 1, s, tune));
         LAB_CUDA(cudaMemcpyAsync(hp, ovf.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         LAB_CUDA(cudaStreamSynchronize(s)); // the overflow flag and the class counts
         if(hp[0])
@@ -955,7 +968,8 @@ namespace lab
 
         // ---- symbolic: lane tier (<= 32 products), hash classes, overflow -> global sort
         gemm_classes gs;
-        LAB_TRY(gemm_class_fill(0, upper.get(), nullptr, m, hp + 1, dh.get() + kHashClasses, gs, s));
+        LAB_TRY(gemm_class_fill(0, upper.get(), nullptr, m, hp + 1, dh.get() + kHashClasses, gs, s,
+                                tune));
         dbuf<int32_t> counts, ovf_rows, ovf2_rows, rp;
         dbuf<int>     novf_d;
         LAB_TRY(counts.alloc((size_t)m + 1, s));
@@ -996,7 +1010,7 @@ namespace lab
             // the numeric classes (by exact count) are counted before the one sync
             // that reads the nonzero total (and the 4096-slot overflow count)
             LAB_TRY(gemm_class_count(1, upper.get(), rp.get(), m, dh.get() + 2 * kHashClasses,
-                                     hp + 16, s));
+                                     hp + 16, s, tune));
             LAB_TRY(copy_d2h_sync(&nnz32, rp.get() + m, sizeof(int32_t), s));
             const int novf2 = hp[32];
             if(pass == 1 || novf2 == 0)
@@ -1026,7 +1040,7 @@ namespace lab
         gemm_classes gn;
         if(st == LAB_OK)
             st = gemm_class_fill(1, upper.get(), rp.get(), m, hp + 16, dh.get() + 3 * kHashClasses,
-                                 gn, s);
+                                 gn, s, tune);
         if(st == LAB_OK)
         {
             stream_fork f(s, m); // lane tier and hash classes side by side

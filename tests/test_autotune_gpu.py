@@ -48,3 +48,36 @@ def test_hierarchy_autotune_solves_like_oracle(gpu, oracle):
     assert info.converged == 1
     assert abs(info.iterations - ito) <= 1
     assert np.max(np.abs(x.cpu().numpy() - xo)) <= 1e-6 * np.max(np.abs(xo))
+
+
+def test_spgemm_autotune_keeps_results(gpu, oracle):
+    """Tuning only sizes the hash tables: the products stay bit-identical."""
+    import ctypes as C
+    from helpers import csr_equal
+    A = P.poisson3d(24)
+    Ho = oracle.amg_setup(A)
+    dA = gpu.CsrMatrix.from_arrays(*A)
+    dP = gpu.CsrMatrix.from_arrays(*Ho.P(0)[:3], n=Ho.P(0)[3])
+    before = dA.spgemm(dP).to_numpy()
+    us = C.c_double()
+    L.call("lab_spgemm_autotune", dA.h, dP.h, C.byref(us), gpu.stream_handle())
+    assert us.value > 0
+    after = dA.spgemm(dP).to_numpy()
+    assert csr_equal(before, after)
+    assert csr_equal(after, oracle.spgemm(A, Ho.P(0)))
+
+
+def test_hierarchy_tune_products_then_setup_bit_identical(gpu, oracle):
+    """After the Galerkin products of a hierarchy are tuned, a new setup of the same
+    operator uses the tuned sizings and is still bit-identical to the oracle."""
+    from helpers import csr_equal
+    A = P.poisson3d(20)
+    dA = gpu.CsrMatrix.from_arrays(*A)
+    H = gpu.Hierarchy(dA)
+    L.call("lab_hierarchy_tune_products", H.h, gpu.stream_handle())
+    H2 = gpu.Hierarchy(dA)
+    Ho = oracle.amg_setup(A)
+    assert H2.levels == Ho.levels
+    for l in range(H2.levels + 1):
+        assert csr_equal(H2.A(l).to_numpy(), Ho.A(l))
+    L.call("lab_tune_cache_clear")
