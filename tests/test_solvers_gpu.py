@@ -324,3 +324,35 @@ def test_zero_rhs_converges_immediately(gpu):
     x, info = gpu.pcg(dA, gpu.vec(np.zeros(256)), M=M)
     assert info.converged == 1 and info.iterations == 0
     assert torch.count_nonzero(x) == 0
+
+
+@pytest.mark.parametrize("max_iter", [0, 1, 3])
+def test_pcg_stops_at_max_iter(gpu, reference, max_iter):
+    """The iteration loop runs on the device (one graph launch) and is bounded:
+    with a tolerance it cannot reach, PCG stops after max_iter + 1 iterations, the
+    reference's count (cg.cpp:136-223, iter_control::exceed_max_iter), and reports
+    LAB_NOT_CONVERGED with the same iterate."""
+    A = P.poisson3d(20)
+    b, _ = P.rhs_from_solution(*A[:3], seed=0)
+    dA, H = _setup(gpu, A)
+    x, info = gpu.pcg(dA, gpu.vec(b), M=gpu.Preconditioner.amg(H),
+                      control=gpu.iter_control(rel_tol=1e-14, abs_tol=0.0, max_iter=max_iter))
+    xr, itr = reference.amg_setup(A, kind=0).pcg(b, rel_tol=1e-14, abs_tol=1e-300,
+                                                 max_iter=max_iter)
+    assert info.converged == 0 and info.status == L.LAB_NOT_CONVERGED
+    assert info.iterations == itr == max_iter + 1
+    assert np.max(np.abs(x.cpu().numpy() - xr)) <= 1e-9 * np.max(np.abs(xr))
+
+
+def test_batched_stops_at_max_iter(gpu):
+    """The batched solve's device-side loop is bounded by max_iter too: every
+    system that cannot converge retires after max_iter + 1 iterations."""
+    mats = [P.poisson2d(s) for s in (12, 20, 9)]
+    rhs = np.concatenate([P.rhs_from_solution(*A, seed=k)[0] for k, A in enumerate(mats)])
+    S, offs = gpu.block_diag([gpu.CsrMatrix.from_arrays(*A) for A in mats])
+    M = gpu.Preconditioner.amg(gpu.Hierarchy(S))
+    x, iters, conv, info = gpu.batched_pcg(S, offs, gpu.vec(rhs), M,
+                                           control=gpu.iter_control(rel_tol=1e-15, abs_tol=0.0,
+                                                                    max_iter=4))
+    assert info.status == L.LAB_NOT_CONVERGED and not conv.any()
+    assert list(iters) == [5, 5, 5]
