@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--level", type=int, default=0,
                     help="--mode spmv: time the SpMV of hierarchy level L's operator A_L "
                          "(0: the input matrix)")
-    ap.add_argument("--spmv-alg", default=None, choices=["rowseq", "vector", "stream"],
+    ap.add_argument("--spmv-alg", default=None, choices=["rowseq", "vector", "stream", "halo"],
                     help="--mode spmv: force a schedule (default: the analysed plan)")
     ap.add_argument("--mode", default="full",
                     choices=["full", "profile", "spmv", "mixed", "batched", "batched_split",
@@ -345,7 +345,8 @@ def dominant_kernel_roofline(core, dA, m, nnz, torch, profiled=True,
             traffic = float(mt.group(1))
     alg, lanes = dA.algorithm()
     kname = {1: "k_pipe<op_spmv> (one thread per row, staged tiles)",
-             4: f"k_vstream<op_spmv> ({lanes} lanes per row, bulk-copy stage ring)"}.get(
+             4: f"k_vstream<op_spmv> ({lanes} lanes per row, bulk-copy stage ring)",
+             5: f"k_vhalo<op_spmv> ({lanes} lanes per row, x staged per chunk of rows)"}.get(
         alg, f"k_vector<op_spmv> ({lanes} lanes per row)")
     return {"bound": "hbm", "kernel": kname + " on " + label,
             "achieved": achieved, "peak": peak, "peak_source": which, "unit": "GB/s",
@@ -414,7 +415,7 @@ def run_ours(args, d):
         if args.spmv_alg:
             lanes = target.algorithm()[1]
             alg = {"rowseq": L.SPMV_ROWSEQ, "vector": L.SPMV_VECTOR,
-                   "stream": L.SPMV_VECTOR_STREAM}[args.spmv_alg]
+                   "stream": L.SPMV_VECTOR_STREAM, "halo": L.SPMV_VECTOR_HALO}[args.spmv_alg]
             target.set_algorithm(alg, lanes if lanes > 1 else 0)
         roof = dominant_kernel_roofline(core, target, m, nnz, torch,
                                         profiled=(args.matrix or "poisson") == "poisson"

@@ -144,10 +144,15 @@ typedef enum lab_spmv_alg
     LAB_SPMV_ROWSEQ  = 1, /* thread per row over shared-memory staged rows, fma in CSR order */
     LAB_SPMV_VECTOR  = 2, /* 2..32 lanes per row, vectorised loads, shuffle reduction */
     LAB_SPMV_MERGE   = 3, /* merge-path nnz split for skewed row lengths */
-    LAB_SPMV_VECTOR_STREAM = 4 /* LAB_SPMV_VECTOR with the matrix streamed through shared
+    LAB_SPMV_VECTOR_STREAM = 4, /* LAB_SPMV_VECTOR with the matrix streamed through shared
                                   memory by bulk copies (one producer warp, mbarrier
                                   stage ring) on operators of >= 8192 rows; the same
                                   per-row arithmetic, bit-identical; elsewhere as VECTOR */
+    LAB_SPMV_VECTOR_HALO = 5 /* LAB_SPMV_VECTOR on a square matrix with x staged per chunk
+                                of consecutive rows at the chunk's distinct columns in
+                                shared memory (one list per chunk, built when first
+                                forced or tuned); the same per-row arithmetic,
+                                bit-identical; elsewhere as VECTOR */
 } lab_spmv_alg;
 
 /* Row-length statistics -> algorithm and launch shape, cached on the matrix.
@@ -156,8 +161,15 @@ LAB_API lab_status lab_spmv_analysis(lab_csr A, lab_stream s);
 /* Force an algorithm (LAB_SPMV_AUTO restores the analysed choice). */
 LAB_API lab_status lab_spmv_set_algorithm(lab_csr A, lab_spmv_alg alg, int lanes);
 LAB_API lab_status lab_spmv_get_algorithm(lab_csr A, int* alg, int* lanes);
+/* Halo plan of A (built by lab_spmv_analysis for the VECTOR schedule of a square
+ * matrix): chunks of *rows_per_chunk consecutive rows, *distinct staged columns
+ * over all chunks, *direct_chunks chunks that read x directly; all 0 when A has
+ * no halo plan.  Any output may be NULL.  No counterpart in the reference. */
+LAB_API lab_status lab_spmv_halo_info(lab_csr A, int64_t* chunks, int64_t* rows_per_chunk,
+                                      int64_t* distinct, int64_t* direct_chunks);
 /* Autotuner: time every candidate SpMV schedule on this matrix (one thread per
- * row, and unless `exact` W = 2..32 lanes per row) and keep the fastest; the
+ * row, and unless `exact` W = 2..32 lanes per row in the direct, streamed and halo
+ * forms the matrix has) and keep the fastest; the
  * winner's time per SpMV in microseconds goes to *best_us (may be NULL).  With
  * exact != 0 only schedules that accumulate in CSR order (bit-identical to the
  * reference, host_matrix_vector.cpp:60-84) are candidates.  No counterpart in the

@@ -20,7 +20,8 @@ CYCLE_V, CYCLE_W, CYCLE_F = 0, 1, 2
 SMOOTH_JACOBI, SMOOTH_GS, SMOOTH_SGS, SMOOTH_SOR, SMOOTH_SSOR = range(5)
 COARSE_DIRECT, COARSE_GS = 0, 1
 PREC_FP64, PREC_FP32, PREC_FP32_BF16 = 0, 1, 2
-SPMV_AUTO, SPMV_ROWSEQ, SPMV_VECTOR, SPMV_MERGE, SPMV_VECTOR_STREAM = 0, 1, 2, 3, 4
+SPMV_AUTO, SPMV_ROWSEQ, SPMV_VECTOR, SPMV_MERGE, SPMV_VECTOR_STREAM, SPMV_VECTOR_HALO = (
+    0, 1, 2, 3, 4, 5)
 
 
 class LabError(RuntimeError):
@@ -71,6 +72,8 @@ _SIGS = {
     "lab_spmv_analysis": [_p, _p],
     "lab_spmv_set_algorithm": [_p, _i, _i],
     "lab_spmv_get_algorithm": [_p, C.POINTER(_i), C.POINTER(_i)],
+    "lab_spmv_halo_info": [_p, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64),
+                           C.POINTER(_i64)],
     "lab_spmv": [_d, _p, _p, _d, _p, _p],
     "lab_residual": [_p, _p, _p, _p, _p],
     "lab_spmm": [_d, _p, _i, _p, _i64, _d, _p, _i64, _p],

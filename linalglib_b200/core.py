@@ -143,6 +143,13 @@ class CsrMatrix:
         call("lab_spmv_get_algorithm", self.h, C.byref(a), C.byref(w))
         return a.value, w.value
 
+    def halo_info(self):
+        """(chunks, rows per chunk, distinct staged columns, chunks read directly)
+        of the matrix's halo plan; zeros when it has none."""
+        v = [C.c_int64() for _ in range(4)]
+        call("lab_spmv_halo_info", self.h, *[C.byref(x) for x in v])
+        return tuple(x.value for x in v)
+
     def spmv(self, x, y=None, alpha=1.0, beta=0.0, stream=None):
         if y is None:
             y = torch.zeros(self.m, dtype=torch.float64, device="cuda")

@@ -254,6 +254,12 @@ namespace lab
             cudaFree(p.block_row);
         if(p.merge_coords)
             cudaFree(p.merge_coords);
+        if(p.hcnt)
+            cudaFree(p.hcnt);
+        if(p.hcol)
+            cudaFree(p.hcol);
+        if(p.hloc)
+            cudaFree(p.hloc);
         p = spmv_plan();
     }
 
@@ -1008,6 +1014,9 @@ LAB_API lab_status lab_csr_structure_changed(lab_csr A, lab_stream ls)
     A->lp.dcol_state = 0;
     dfree(A->plan.block_row, s);
     dfree(A->plan.merge_coords, s);
+    dfree(A->plan.hcnt, s);
+    dfree(A->plan.hcol, s);
+    dfree(A->plan.hloc, s);
     A->plan = spmv_plan();
     if(A->tri)
     {

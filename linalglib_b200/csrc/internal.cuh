@@ -167,7 +167,30 @@ namespace lab
         int st_rows = 0;
         int st_cap  = 0;
         int stream  = 0;
+        // halo form of VECTOR (spmv_engine.cuh, k_vhalo): chunks of hrows
+        // consecutive rows; chunk c stages x at its hcnt[c] distinct columns
+        // (hcol[c * hslot ...], ascending) in shared memory and every entry names
+        // its column by hloc[j], the position in that list; hcnt[c] = -1: the chunk
+        // reads x directly.  Built once per pattern (halo_state 1; -1: not square,
+        // or no chunk can be staged) for LAB_SPMV_VECTOR_HALO and the autotuner;
+        // used while halo_use is set (that schedule forced or tuned in).
+        int       halo_state = 0;
+        int       halo_use   = 0;
+        int       hrows      = 0;
+        int       hchunks    = 0;
+        int       hslot      = 0; // largest staged count, the shared-memory entries
+        int64_t   hdistinct  = 0; // staged columns over all chunks
+        int       hdirect    = 0; // chunks left to direct reads (hcnt = -1)
+        int32_t*  hcnt       = nullptr;
+        int32_t*  hcol       = nullptr;
+        uint16_t* hloc       = nullptr;
     };
+
+    // Halo geometry: a chunk's columns are marked in a shared-memory bitmap over its
+    // column span (at most kHaloBits columns), and at most kHaloCap distinct columns
+    // are staged; chunks beyond either read x directly.
+    constexpr int kHaloBits = 1 << 18;
+    constexpr int kHaloCap  = 8192;
 
     struct csr_values_lp
     {
@@ -210,6 +233,8 @@ namespace lab
     lab_status diag_into(const lab_csr_impl* A, double* d, double* invd, cudaStream_t s);
     lab_status csr_ensure_lowp(lab_csr_impl* A, int precision, int use_bf16, cudaStream_t s);
     lab_status spmv_analyse(lab_csr_impl* A, cudaStream_t s);
+    // Builds A's halo plan (spmv_plan::hcnt/hcol/hloc) unless it was examined.
+    lab_status halo_build(lab_csr_impl* A, cudaStream_t s);
     lab_status spmm_columns(const lab_csr_impl* A, int k, const double* X, int64_t ldx, double* Y,
                             int64_t ldy, cudaStream_t s, const int* skip);
 

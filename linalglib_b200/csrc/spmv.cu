@@ -2,6 +2,8 @@
 // residual, multi-vector SpMM.
 #include "spmv_engine.cuh"
 
+#include <climits>
+
 namespace lab
 {
     __global__ void k_row_stats(const int32_t* __restrict__ rp, int64_t m, int* maxlen)
@@ -57,6 +59,179 @@ namespace lab
             atomicOr(wide, 1);
     }
 
+    // ------------------------------------------------------------ halo plan
+    // Reductions over one CTA (every thread gets the result).
+    template <int NT, class F>
+    __device__ __forceinline__ int block_reduce(int v, int* red, F f)
+    {
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            v = f(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if((threadIdx.x & 31) == 0)
+            red[threadIdx.x >> 5] = v;
+        __syncthreads();
+        int r = red[0];
+#pragma unroll
+        for(int k = 1; k < NT / 32; k++)
+            r = f(r, red[k]);
+        __syncthreads();
+        return r;
+    }
+
+    // Marks chunk c's columns (rows [c*rows, c*rows + rows)) in a bitmap over
+    // [lo, lo + 32*words); returns false (uniformly) when the chunk has no entries
+    // or its span exceeds kHaloBits.
+    template <int NT>
+    __device__ bool halo_mark(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                              int64_t m, int rows, unsigned* bm, int* red, int& lo, int& words,
+                              int& j0, int& j1)
+    {
+        const int64_t r0 = (int64_t)blockIdx.x * rows;
+        const int64_t r1 = r0 + rows < m ? r0 + rows : m;
+        j0               = rp[r0];
+        j1               = rp[r1];
+        int l = INT_MAX, h = -1;
+        for(int j = j0 + threadIdx.x; j < j1; j += NT)
+        {
+            const int c = __ldg(ci + j);
+            l           = min(l, c);
+            h           = max(h, c);
+        }
+        lo = block_reduce<NT>(l, red, [](int a, int b) { return min(a, b); });
+        h  = block_reduce<NT>(h, red, [](int a, int b) { return max(a, b); });
+        if(j1 <= j0 || (int64_t)h - lo + 1 > kHaloBits)
+            return false;
+        words = (int)(((int64_t)h - lo + 1 + 31) >> 5);
+        for(int w = threadIdx.x; w < words; w += NT)
+            bm[w] = 0u;
+        __syncthreads();
+        for(int j = j0 + threadIdx.x; j < j1; j += NT)
+        {
+            const int off = __ldg(ci + j) - lo;
+            atomicOr(bm + (off >> 5), 1u << (off & 31));
+        }
+        __syncthreads();
+        return true;
+    }
+
+    // Distinct columns per chunk: hcnt[c] = count (0 for an empty chunk), or -1
+    // (span beyond kHaloBits or more than kHaloCap columns).  stats: [0] largest
+    // count, [1] chunks at -1, [2] sum of counts.
+    template <int NT>
+    __global__ void __launch_bounds__(NT)
+        k_halo_count(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, int64_t m,
+                     int rows, int32_t* __restrict__ hcnt, int* stats)
+    {
+        extern __shared__ unsigned halo_bm[];
+        __shared__ int red[NT / 32];
+        int            lo = 0, words = 0, j0 = 0, j1 = 0;
+        const int      c  = blockIdx.x;
+        if(!halo_mark<NT>(rp, ci, m, rows, halo_bm, red, lo, words, j0, j1))
+        {
+            if(threadIdx.x == 0)
+            {
+                hcnt[c] = j1 <= j0 ? 0 : -1;
+                if(j1 > j0)
+                    atomicAdd(stats + 1, 1);
+            }
+            return;
+        }
+        int cnt = 0;
+        for(int w = threadIdx.x; w < words; w += NT)
+            cnt += __popc(halo_bm[w]);
+        cnt = block_reduce<NT>(cnt, red, [](int a, int b) { return a + b; });
+        if(threadIdx.x == 0)
+        {
+            if(cnt > kHaloCap)
+            {
+                hcnt[c] = -1;
+                atomicAdd(stats + 1, 1);
+            }
+            else
+            {
+                hcnt[c] = cnt;
+                atomicMax(stats, cnt);
+                atomicAdd(stats + 2, cnt);
+            }
+        }
+    }
+
+    // Chunk c's distinct columns in ascending order into hcol[c * slot ...] and,
+    // for every entry, the position of its column in that list (hloc).
+    template <int NT>
+    __global__ void __launch_bounds__(NT)
+        k_halo_fill(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, int64_t m,
+                    int rows, const int32_t* __restrict__ hcnt, int slot,
+                    int32_t* __restrict__ hcol, uint16_t* __restrict__ hloc)
+    {
+        extern __shared__ unsigned halo_bm[];
+        uint16_t*  pre = reinterpret_cast<uint16_t*>(halo_bm + kHaloBits / 32);
+        __shared__ int red[NT / 32];
+        const int      c = blockIdx.x;
+        if(hcnt[c] <= 0)
+            return;
+        int lo = 0, words = 0, j0 = 0, j1 = 0;
+        if(!halo_mark<NT>(rp, ci, m, rows, halo_bm, red, lo, words, j0, j1))
+            return; // not reached: the count pass staged this chunk
+        // exclusive prefix of the per-word counts: contiguous word runs per thread
+        const int per = (words + NT - 1) / NT;
+        const int w0 = min(words, (int)threadIdx.x * per), w1 = min(words, w0 + per);
+        int       own = 0;
+        for(int w = w0; w < w1; w++)
+            own += __popc(halo_bm[w]);
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        int       inc  = own;
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1)
+        {
+            const int t = __shfl_up_sync(0xffffffffu, inc, o);
+            if(lane >= o)
+                inc += t;
+        }
+        if(lane == 31)
+            red[wid] = inc;
+        __syncthreads();
+        int run = inc - own;
+        for(int k = 0; k < wid; k++)
+            run += red[k];
+        for(int w = w0; w < w1; w++)
+        {
+            pre[w] = (uint16_t)run;
+            run += __popc(halo_bm[w]);
+        }
+        __syncthreads();
+        int32_t* hc = hcol + (size_t)c * slot;
+        for(int w = threadIdx.x; w < words; w += NT)
+        {
+            unsigned b = halo_bm[w];
+            int      k = pre[w];
+            while(b)
+            {
+                hc[k++] = lo + (w << 5) + (__ffs(b) - 1);
+                b &= b - 1u;
+            }
+        }
+        for(int j = j0 + threadIdx.x; j < j1; j += NT)
+        {
+            const int off = __ldg(ci + j) - lo;
+            const int w   = off >> 5;
+            hloc[j] = (uint16_t)(pre[w] + __popc(halo_bm[w] & ((1u << (off & 31)) - 1u)));
+        }
+    }
+
+    // Rows per halo chunk: about kHaloEntries entries, at least four chunks per SM,
+    // a whole number of VECTOR passes (256 / W rows) for the matrix's lane count.
+    constexpr int kHaloEntries = 8192;
+    static int halo_rows(const lab_csr_impl* A, int w)
+    {
+        const double avg    = (double)A->nnz / (double)A->m;
+        const double target = std::min<double>(kHaloEntries,
+                                                (double)A->nnz / (4.0 * (double)num_sms()));
+        const int    pass   = std::max(1, kVectorNT / w);
+        const int    r      = (int)(target / avg) / pass * pass;
+        return std::max(pass, r);
+    }
+
     // Largest power of two <= v, clamped to 2..32.
     static int pow2_at_most(double v)
     {
@@ -64,6 +239,60 @@ namespace lab
         while(w < 32 && 2 * w <= v)
             w <<= 1;
         return w;
+    }
+
+    // Halo plan of a square matrix (LAB_SPMV_VECTOR_HALO, and the autotuner's halo
+    // candidates): distinct columns per chunk counted on the device and read back
+    // (their largest count sizes the lists and the launch's shared memory), then the
+    // lists and the per-entry positions written.  Built once per pattern; a matrix
+    // whose chunks all read x directly gets none (halo_state -1).
+    lab_status halo_build(lab_csr_impl* A, cudaStream_t s)
+    {
+        spmv_plan& p = A->plan;
+        if(p.halo_state != 0)
+            return LAB_OK;
+        p.halo_state = -1;
+        if(A->m != A->n || A->m == 0 || A->nnz == 0 || A->m > INT32_MAX)
+            return LAB_OK;
+        const double avg     = (double)A->nnz / (double)A->m;
+        const int    w       = p.alg == LAB_SPMV_VECTOR ? p.lanes : pow2_at_most(avg / 5.0);
+        const int    hrows   = halo_rows(A, w);
+        const int    hchunks = (int)ceil_div<int64_t>(A->m, hrows);
+        int          stats[3] = {0, 0, 0};
+        int*         d        = nullptr;
+        LAB_TRY(dalloc(&d, 3, s));
+        LAB_CUDA(cudaMemsetAsync(d, 0, 3 * sizeof(int), s));
+        LAB_TRY(dalloc(&p.hcnt, (size_t)hchunks, s));
+        static const cudaError_t count_attr = cudaFuncSetAttribute(
+            k_halo_count<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, kHaloBits / 8);
+        LAB_CUDA(count_attr);
+        LAB_LAUNCH(k_halo_count<256>, (unsigned)hchunks, 256, kHaloBits / 8, s, A->row_ptr,
+                   A->col_ind, A->m, hrows, p.hcnt, d);
+        const lab_status st = copy_d2h_sync(stats, d, sizeof(stats), s);
+        dfree(d, s);
+        LAB_TRY(st);
+        const int slot = stats[0];
+        if(slot == 0)
+        {
+            dfree(p.hcnt, s);
+            p.hcnt = nullptr;
+            return LAB_OK;
+        }
+        LAB_TRY(dalloc(&p.hcol, (size_t)hchunks * slot, s));
+        LAB_TRY(dalloc(&p.hloc, (size_t)A->nnz, s));
+        static const cudaError_t fill_attr =
+            cudaFuncSetAttribute(k_halo_fill<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kHaloBits / 8 + kHaloBits / 16);
+        LAB_CUDA(fill_attr);
+        LAB_LAUNCH(k_halo_fill<256>, (unsigned)hchunks, 256, kHaloBits / 8 + kHaloBits / 16, s,
+                   A->row_ptr, A->col_ind, A->m, hrows, p.hcnt, slot, p.hcol, p.hloc);
+        p.halo_state = 1;
+        p.hrows      = hrows;
+        p.hchunks    = hchunks;
+        p.hslot      = slot;
+        p.hdirect    = stats[1];
+        p.hdistinct  = stats[2];
+        return LAB_OK;
     }
 
     // Schedule choice from row statistics.  Rows of at most 32 entries (stencils up
@@ -161,6 +390,8 @@ namespace lab
             p.lanes = maxlen <= 32 ? 1 : p.vlanes;
         }
         p.analysed = 1;
+        if(p.forced && p.alg == LAB_SPMV_VECTOR && p.halo_use && !p.stream && p.halo_state == 0)
+            LAB_TRY(halo_build(A, s));
         return LAB_OK;
     }
 
@@ -257,14 +488,16 @@ LAB_API lab_status lab_spmv_set_algorithm(lab_csr A, lab_spmv_alg alg, int lanes
         A->plan.forced   = 0;
         A->plan.analysed = 0;
         A->plan.stream   = 0;
+        A->plan.halo_use = 0;
         return LAB_OK;
     }
     LAB_ARG(alg == LAB_SPMV_ROWSEQ || alg == LAB_SPMV_VECTOR || alg == LAB_SPMV_MERGE ||
-                alg == LAB_SPMV_VECTOR_STREAM,
+                alg == LAB_SPMV_VECTOR_STREAM || alg == LAB_SPMV_VECTOR_HALO,
             "unknown algorithm");
     A->plan.forced   = 1;
     A->plan.analysed = 0;
     A->plan.stream   = alg == LAB_SPMV_VECTOR_STREAM;
+    A->plan.halo_use = alg == LAB_SPMV_VECTOR_HALO;
     if(alg == LAB_SPMV_ROWSEQ)
     {
         A->plan.alg   = LAB_SPMV_ROWSEQ;
@@ -282,12 +515,31 @@ LAB_API lab_status lab_spmv_set_algorithm(lab_csr A, lab_spmv_alg alg, int lanes
 LAB_API lab_status lab_spmv_get_algorithm(lab_csr A, int* alg, int* lanes)
 {
     LAB_ARG(A, "null matrix");
+    const spmv_plan& p = A->plan;
     if(alg)
-        *alg = A->plan.alg == LAB_SPMV_VECTOR && A->plan.stream && A->plan.st_rows > 0
-                   ? LAB_SPMV_VECTOR_STREAM
-                   : A->plan.alg;
+        *alg = p.alg == LAB_SPMV_VECTOR && p.stream && p.st_rows > 0 ? LAB_SPMV_VECTOR_STREAM
+               : p.alg == LAB_SPMV_VECTOR && !p.stream && p.halo_use && p.halo_state == 1
+                   ? LAB_SPMV_VECTOR_HALO
+                   : p.alg;
     if(lanes)
-        *lanes = A->plan.lanes;
+        *lanes = p.lanes;
+    return LAB_OK;
+}
+
+LAB_API lab_status lab_spmv_halo_info(lab_csr A, int64_t* chunks, int64_t* rows_per_chunk,
+                                      int64_t* distinct, int64_t* direct_chunks)
+{
+    LAB_ARG(A, "null matrix");
+    const spmv_plan& p    = A->plan;
+    const bool       have = p.halo_state == 1;
+    if(chunks)
+        *chunks = have ? p.hchunks : 0;
+    if(rows_per_chunk)
+        *rows_per_chunk = have ? p.hrows : 0;
+    if(distinct)
+        *distinct = have ? p.hdistinct : 0;
+    if(direct_chunks)
+        *direct_chunks = have ? p.hdirect : 0;
     return LAB_OK;
 }
 

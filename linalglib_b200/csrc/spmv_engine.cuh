@@ -513,6 +513,142 @@ namespace lab
             reduce_finish_sum<NT>(contrib, red.partial, red.counter, red.out);
     }
 
+    __device__ __forceinline__ void ld4(const uint16_t* p, uint16_t (&o)[4])
+    {
+        const uint2     u = __ldg(reinterpret_cast<const uint2*>(p));
+        const uint16_t* h = reinterpret_cast<const uint16_t*>(&u);
+        o[0] = h[0], o[1] = h[1], o[2] = h[2], o[3] = h[3];
+    }
+
+    template <class Op>
+    using gather_t = std::decay_t<decltype(std::declval<const Op&>().gather(0))>;
+
+    struct halo_view
+    {
+        const int32_t*  cnt;  // per chunk: staged distinct columns, -1 = direct reads
+        const int32_t*  col;  // chunk c's distinct columns at c * slot, ascending
+        const uint16_t* loc;  // per entry: its column's position in the chunk's list
+        int             rows; // rows per chunk
+        int             slot;
+    };
+
+    // VECTOR schedule with a per-chunk halo (long rows whose columns stay near the
+    // diagonal: the coarse SA levels).  One CTA per chunk of consecutive rows first
+    // stages x at the chunk's distinct columns in shared memory, one coalesced pass
+    // over an ascending column list, then runs k_vector's per-row work -- the same
+    // lanes, the same entries per lane in the same order, the same shuffle tree --
+    // with every gather read from shared memory.  The distinct columns number about
+    // a quarter of the entries on those levels, so most of the scattered gathers
+    // that bound k_vector (one L1/TEX request per entry) disappear; the matrix
+    // stream is unchanged (16-bit local positions in place of the 16-bit offsets).
+    // Row results are bit-identical to k_vector.  Ops with a reduction keep
+    // k_vector (a thread here sums several rows, which would regroup the sum).
+    template <class Op, int NT, int W, class IT>
+    __global__ void __launch_bounds__(NT)
+        k_vhalo(csr_view<typename Op::val_t, IT> A, halo_view h, Op op, red_buf red)
+    {
+        using VT = typename Op::val_t;
+        using AT = typename Op::acc_t;
+        using GT = gather_t<Op>;
+        static_assert(!Op::kReduce, "reductions keep k_vector");
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        GT* sx = reinterpret_cast<GT*>(smem_raw);
+        if(red.skip && *red.skip)
+            return;
+        const int64_t r0  = (int64_t)blockIdx.x * h.rows;
+        const int     r1  = (int)(r0 + h.rows < A.m ? r0 + h.rows : A.m);
+        const int     cnt = h.cnt[blockIdx.x];
+        if(cnt > 0)
+        {
+            // U list entries per thread in flight: U column loads, then U gathers
+            // (ascending columns: neighbouring threads read neighbouring x)
+            constexpr int  U  = 8;
+            const int32_t* hc = h.col + (size_t)blockIdx.x * h.slot;
+            for(int k0 = threadIdx.x; k0 < cnt; k0 += NT * U)
+            {
+                int c[U];
+#pragma unroll
+                for(int u = 0; u < U; u++)
+                    c[u] = k0 + u * NT < cnt ? __ldg(hc + k0 + u * NT) : -1;
+                GT g[U];
+#pragma unroll
+                for(int u = 0; u < U; u++)
+                    if(c[u] >= 0)
+                        g[u] = op.gather(c[u]);
+#pragma unroll
+                for(int u = 0; u < U; u++)
+                    if(c[u] >= 0)
+                        sx[k0 + u * NT] = g[u];
+            }
+        }
+        __syncthreads();
+        const bool staged = cnt >= 0;
+        const int  lane   = threadIdx.x & (W - 1);
+        for(int base = (int)r0; base < r1; base += NT / W)
+        {
+            const int  row = base + (int)threadIdx.x / W;
+            AT         s   = AT(0);
+            pre_of<Op> pr{};
+            if(row < r1 && lane == 0)
+                pr = pre_load(op, row);
+            if(row < r1 && sizeof(VT) == 8)
+            {
+                const int a = A.rp[row], b = A.rp[row + 1];
+                if(staged)
+                {
+#pragma unroll 4
+                    for(int j = a + lane; j < b; j += W)
+                        s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)), sx[h.loc[j]], s);
+                }
+                else
+                {
+#pragma unroll 4
+                    for(int j = a + lane; j < b; j += W)
+                        s = acc_step<Op::kFma>(to_acc(A.v[j], AT(0)),
+                                               op.gather(col_of<IT>(A.ci[j], row)), s);
+                }
+            }
+            else if(row < r1)
+            {
+                const int a = A.rp[row], b = A.rp[row + 1];
+#pragma unroll 2
+                for(int q = (a & ~3) + 4 * lane; q < b; q += 4 * W)
+                {
+                    VT v4[4];
+                    ld4(A.v + q, v4);
+                    AT xg[4];
+                    if(staged)
+                    {
+                        uint16_t l4[4];
+                        ld4(h.loc + q, l4);
+#pragma unroll
+                        for(int t = 0; t < 4; t++)
+                            if(q + t >= a && q + t < b)
+                                xg[t] = sx[l4[t]];
+                    }
+                    else
+                    {
+                        IT c4[4];
+                        ld4(A.ci + q, c4);
+#pragma unroll
+                        for(int t = 0; t < 4; t++)
+                            if(q + t >= a && q + t < b)
+                                xg[t] = op.gather(col_of<IT>(c4[t], row));
+                    }
+#pragma unroll
+                    for(int t = 0; t < 4; t++)
+                        if(q + t >= a && q + t < b)
+                            s = acc_step<Op::kFma>(to_acc(v4[t], AT(0)), xg[t], s);
+                }
+            }
+#pragma unroll
+            for(int o = W / 2; o > 0; o >>= 1)
+                s += __shfl_xor_sync(0xffffffffu, s, o, W);
+            if(row < r1 && lane == 0)
+                finish_with(op, row, s, pr);
+        }
+    }
+
     constexpr int kRowseqNT = 256;
     constexpr int kVectorNT = 256;
 
@@ -625,6 +761,39 @@ namespace lab
         return LAB_OK;
     }
 
+    // The halo form when the matrix has one and the op has no reduction; returns
+    // false (nothing launched) otherwise.
+    template <class Op, int W, class IT>
+    bool launch_vhalo(const lab_csr_impl* A, const csr_view<typename Op::val_t, IT>& V,
+                      const Op& op, cudaStream_t s, const red_buf& red, lab_status* st)
+    {
+        const spmv_plan& p = A->plan;
+        if constexpr(Op::kReduce)
+            return false;
+        else
+        {
+            if(p.halo_state != 1 || !p.halo_use || p.stream)
+                return false;
+            using GT          = gather_t<Op>;
+            const auto kernel = k_vhalo<Op, kVectorNT, W, IT>;
+            static const cudaError_t attr = cudaFuncSetAttribute(
+                kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kHaloCap * (int)sizeof(GT));
+            *st = LAB_OK;
+            if(attr != cudaSuccess)
+            {
+                *st = cuda_status(attr, "cudaFuncSetAttribute(k_vhalo)", __FILE__, __LINE__);
+                return true;
+            }
+            const halo_view h{p.hcnt, p.hcol, p.hloc, p.hrows, p.hslot};
+            const size_t    smem = (size_t)std::max(p.hslot, 1) * sizeof(GT);
+            *st                  = [&]() -> lab_status {
+                LAB_LAUNCH(kernel, (unsigned)p.hchunks, kVectorNT, smem, s, V, h, op, red);
+                return LAB_OK;
+            }();
+            return true;
+        }
+    }
+
 }
 
 #include "vstream.cuh"
@@ -654,21 +823,31 @@ namespace lab
         case 2:
             if(launch_vstream<Op, 2, IT>(A, V, op, s, red, &st))
                 return st;
+            if(launch_vhalo<Op, 2, IT>(A, V, op, s, red, &st))
+                return st;
             return launch_vector<Op, 2, IT>(V, op, grid, s, red);
         case 4:
             if(launch_vstream<Op, 4, IT>(A, V, op, s, red, &st))
+                return st;
+            if(launch_vhalo<Op, 4, IT>(A, V, op, s, red, &st))
                 return st;
             return launch_vector<Op, 4, IT>(V, op, grid, s, red);
         case 8:
             if(launch_vstream<Op, 8, IT>(A, V, op, s, red, &st))
                 return st;
+            if(launch_vhalo<Op, 8, IT>(A, V, op, s, red, &st))
+                return st;
             return launch_vector<Op, 8, IT>(V, op, grid, s, red);
         case 16:
             if(launch_vstream<Op, 16, IT>(A, V, op, s, red, &st))
                 return st;
+            if(launch_vhalo<Op, 16, IT>(A, V, op, s, red, &st))
+                return st;
             return launch_vector<Op, 16, IT>(V, op, grid, s, red);
         default:
             if(launch_vstream<Op, 32, IT>(A, V, op, s, red, &st))
+                return st;
+            if(launch_vhalo<Op, 32, IT>(A, V, op, s, red, &st))
                 return st;
             return launch_vector<Op, 32, IT>(V, op, grid, s, red);
         }

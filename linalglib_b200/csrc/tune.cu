@@ -33,7 +33,8 @@ namespace lab
         using gemm_key = std::array<int64_t, 6>; // A m, n, nnz, B m, n, nnz
         struct spmv_entry
         {
-            int    alg = LAB_SPMV_ROWSEQ, lanes = 1, stream = 0;
+            int    alg = LAB_SPMV_ROWSEQ, lanes = 1;
+            int    form = 0; // VECTOR: 0 direct loads, 1 streamed, 2 halo
             double us  = 0.0;
         };
         struct gemm_entry
@@ -73,6 +74,7 @@ namespace lab
         {
             A->plan.forced   = 0;
             A->plan.stream   = 0;
+            A->plan.halo_use = 0;
             A->plan.analysed = 0;
             LAB_TRY(spmv_analyse(A, s)); // row statistics (and the default plan)
             if(A->m == 0 || A->nnz == 0)
@@ -87,26 +89,32 @@ namespace lab
                 auto                        hit = g_spmv_cache.find(key);
                 if(hit != g_spmv_cache.end())
                 {
-                    A->plan.alg    = hit->second.alg;
-                    A->plan.lanes  = hit->second.lanes;
-                    A->plan.stream = hit->second.stream;
-                    A->plan.forced = 1;
+                    A->plan.alg      = hit->second.alg;
+                    A->plan.lanes    = hit->second.lanes;
+                    A->plan.stream   = hit->second.form == 1;
+                    A->plan.halo_use = hit->second.form == 2;
+                    A->plan.forced   = 1;
                     if(best_us)
                         *best_us = hit->second.us;
                     return LAB_OK;
                 }
             }
+            if(!exact && A->plan.max_row > 32)
+                LAB_TRY(halo_build(A, s)); // the halo form's plan, a candidate below
+            // form: 0 direct loads, 1 streamed, 2 halo (each where the matrix has one)
             struct cand
             {
-                int alg, lanes, stream;
+                int alg, lanes, form;
             };
             std::vector<cand> cands = {{LAB_SPMV_ROWSEQ, 1, 0}};
             if(!exact)
                 for(int w : {2, 4, 8, 16, 32})
                 {
                     cands.push_back({LAB_SPMV_VECTOR, w, 0});
-                    if(A->plan.st_rows > 0) // the streamed form where the matrix has one
+                    if(A->plan.st_rows > 0)
                         cands.push_back({LAB_SPMV_VECTOR, w, 1});
+                    if(A->plan.halo_state == 1)
+                        cands.push_back({LAB_SPMV_VECTOR, w, 2});
                 }
             dbuf<double> x, y;
             LAB_TRY(x.alloc((size_t)A->n + 1, s));
@@ -120,9 +128,10 @@ namespace lab
             cand       win  = cands[0];
             for(const cand& c : cands)
             {
-                A->plan.alg    = c.alg;
-                A->plan.lanes  = c.lanes;
-                A->plan.stream = c.stream;
+                A->plan.alg      = c.alg;
+                A->plan.lanes    = c.lanes;
+                A->plan.stream   = c.form == 1;
+                A->plan.halo_use = c.form == 2;
                 op_spmv op{x.get(), y.get(), 1.0, 0.0};
                 for(int k = 0; k < kTuneWarm && st == LAB_OK; k++)
                     st = launch_rowop(A, A->val, op, s);
@@ -148,16 +157,17 @@ namespace lab
             }
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
-            A->plan.alg    = win.alg;
-            A->plan.lanes  = win.lanes;
-            A->plan.stream = win.stream;
-            A->plan.forced = 1;
+            A->plan.alg      = win.alg;
+            A->plan.lanes    = win.lanes;
+            A->plan.stream   = win.form == 1;
+            A->plan.halo_use = win.form == 2;
+            A->plan.forced   = 1;
             if(st != LAB_OK)
                 return st;
             if(best_us)
                 *best_us = 1e3 * best / kTuneReps;
             std::lock_guard<std::mutex> g(g_cache_mu);
-            g_spmv_cache[key] = {win.alg, win.lanes, win.stream, 1e3 * best / kTuneReps};
+            g_spmv_cache[key] = {win.alg, win.lanes, win.form, 1e3 * best / kTuneReps};
             return LAB_OK;
         }
 
@@ -271,7 +281,7 @@ LAB_API lab_status lab_tune_cache_save(const char* path)
     for(const auto& kv : g_spmv_cache)
         std::fprintf(f, "spmv %lld %lld %lld %lld %d %d %d %.6f\n", (long long)kv.first[0],
                      (long long)kv.first[1], (long long)kv.first[2], (long long)kv.first[3],
-                     kv.second.alg, kv.second.lanes, kv.second.stream, kv.second.us);
+                     kv.second.alg, kv.second.lanes, kv.second.form, kv.second.us);
     for(const auto& kv : g_gemm_cache)
         std::fprintf(f, "gemm %lld %lld %lld %lld %lld %lld %d %d %d %.6f\n",
                      (long long)kv.first[0], (long long)kv.first[1], (long long)kv.first[2],
@@ -311,7 +321,7 @@ LAB_API lab_status lab_tune_cache_load(const char* path)
             const bool lanes_ok = p[1] == 1 || p[1] == 2 || p[1] == 4 || p[1] == 8 ||
                                   p[1] == 16 || p[1] == 32;
             ok = (p[0] == LAB_SPMV_ROWSEQ || p[0] == LAB_SPMV_VECTOR) && lanes_ok &&
-                 (p[2] == 0 || p[2] == 1) && (a[3] == 0 || a[3] == 1);
+                 (p[2] == 0 || p[2] == 1 || p[2] == 2) && (a[3] == 0 || a[3] == 1);
             if(ok)
                 sp[{a[0], a[1], a[2], a[3]}] = {p[0], p[1], p[2], us};
         }

@@ -29,7 +29,8 @@ def test_spmv_autotune_keeps_results(gpu, oracle, name):
     dA.autotune(exact=False)
     alg, lanes = dA.algorithm()
     assert (alg, lanes) in [(L.SPMV_ROWSEQ, 1)] + [(a, w) for w in (2, 4, 8, 16, 32)
-                                                   for a in (L.SPMV_VECTOR, L.SPMV_VECTOR_STREAM)]
+                                                   for a in (L.SPMV_VECTOR, L.SPMV_VECTOR_STREAM,
+                                                             L.SPMV_VECTOR_HALO)]
     y = dA.spmv(gpu.vec(x)).cpu().numpy()
     assert np.max(np.abs(y - y_ref)) <= 1e-9
 

@@ -141,7 +141,8 @@ def test_cycle_streamed_equals_direct(gpu, prec):
     H = gpu.Hierarchy(dA)
     r = gpu.vec(np.random.default_rng(1).uniform(-1, 1, A[0].size - 1))
     mats = [H.A(l) for l in range(H.levels + 1)] + [H.R(l) for l in range(H.levels)]
-    vec_mats = [(M, M.algorithm()[1]) for M in mats if M.algorithm()[0] == L.SPMV_VECTOR]
+    vec_mats = [(M, M.algorithm()[1]) for M in mats
+                if M.algorithm()[0] in (L.SPMV_VECTOR, L.SPMV_VECTOR_HALO)]
     assert any(M.m >= 8192 for M, _ in vec_mats)
     M = gpu.Preconditioner.amg(H, gpu.amg_options(precision=prec))
     z_direct = M.apply(r).cpu().numpy()
