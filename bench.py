@@ -65,6 +65,12 @@ def parse():
     ap.add_argument("--level", type=int, default=0,
                     help="--mode spmv: time the SpMV of hierarchy level L's operator A_L "
                          "(0: the input matrix)")
+    ap.add_argument("--precision", default=None, choices=["fp64", "fp32", "fp32+bf16"],
+                    help="--mode mixed: with --profile-range, the cycle precision whose timed "
+                         "solves at rtol 1e-8 are bracketed")
+    ap.add_argument("--profile-range", action="store_true",
+                    help="--mode mixed: bracket the --precision solves with cudaProfilerStart/"
+                         "Stop (for ncu --profile-from-start off)")
     ap.add_argument("--spmv-alg", default=None, choices=["rowseq", "vector", "stream", "halo"],
                     help="--mode spmv: force a schedule (default: the analysed plan)")
     ap.add_argument("--mode", default="full",
@@ -778,7 +784,13 @@ def run_mixed(args, d):
             def solve():
                 x.zero_()
                 info.append(core.pcg(dA, bd, x=x, M=M, control=ctl)[1])
+            bracket = args.profile_range and rtol == 1e-8 and names[prec] == (args.precision
+                                                                               or "fp32")
+            if bracket:
+                torch.cuda.profiler.start()
             t, ts = _events_ms(torch, solve, max(3, args.steps))
+            if bracket:
+                torch.cuda.profiler.stop()
             if prec == L.PREC_FP64:
                 x64 = x.clone()
             err64 = float(torch.max(torch.abs(x - x64)) / torch.max(torch.abs(x64)))
