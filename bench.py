@@ -65,6 +65,10 @@ def parse():
     ap.add_argument("--level", type=int, default=0,
                     help="--mode spmv: time the SpMV of hierarchy level L's operator A_L "
                          "(0: the input matrix)")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="full mode: skip the batched, multi-RHS, differentiation and "
+                         "ILU(0) summaries added to the line after the headline's timed "
+                         "regions")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32", "fp32+bf16"],
                     help="--mode mixed: with --profile-range, the cycle precision whose timed "
                          "solves at rtol 1e-8 are bracketed")
@@ -543,6 +547,23 @@ def run_ours(args, d):
     pcg_roof = pcg_iteration_roofline(core, dA, solves, iters, roof["peak"])
     mixed, mixed_x = mixed_half(core, L, torch, dA, bd, ctl, setups, max(3, args.steps))
     setup_roof = setup_roofline(core, torch, dA, roof["peak"], setups)
+    # the other workloads (batched, multi-RHS, differentiation, ILU(0)-PCG), one GPU
+    # only, after every timed region of the headline
+    workloads = None
+    if d.world == 1 and not args.no_workloads:
+        from linalglib_b200 import problems as P
+        workloads = {}
+        for key, fn in (("batched", lambda: batched_workloads(core, P, torch, 3,
+                                                               one_by_one_reps=1)),
+                        ("adjoint", lambda: adjoint_workload(core, P, torch, 3)),
+                        ("ilu0_pcg", lambda: dict(
+                            ilu0_workload(core, torch, dA, bd, args.rtol, 3),
+                            workload=f"ILU(0)-PCG, the same {args.n}^3 system, "
+                                     f"rtol {args.rtol:g}"))):
+            try:
+                workloads.update(fn() if key == "batched" else {key: fn()})
+            except Exception as e:  # reported in the line, never hides the headline
+                workloads[key] = {"error": f"{type(e).__name__}: {e}"}
 
     if d.rank == 0:
         cpu, x_ref = None, None
@@ -576,6 +597,7 @@ def run_ours(args, d):
             "pcg_iteration_roofline": pcg_roof,
             "setup_roofline": setup_roof,
             "mixed_precision": mixed,
+            "workloads": workloads,
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": int(launches),
@@ -867,20 +889,11 @@ def run_batched_split(args, d):
     return 0
 
 
-def run_batched(args, d):
+def batched_workloads(core, P, torch, steps, n=64, one_by_one_reps=3):
     """(a) 256 2D 5-point Poisson systems, sides ~U{32..256} (seed 0), stacked block
     diagonally, one hierarchy, one segmented PCG (per-system convergence mask) to
     rtol 1e-8; against solving the systems one after another.  (b) 32 right-hand
-    sides ~U[-1,1] on the 3D 7-point n^3 operator by block PCG; against 32 solves.
-    Under torchrun (N > 1) the batch is split over the GPUs instead
-    (run_batched_split)."""
-    import torch
-    if d.world > 1:
-        return run_batched_split(args, d)
-    d.init(need_gpu=True)
-    import linalglib_b200.core as core
-    from linalglib_b200 import problems as P
-    core.init()
+    sides ~U[-1,1] on the 3D 7-point n^3 operator by block PCG; against 32 solves."""
     rng = np.random.default_rng(0)
     sides = rng.integers(32, 257, size=256)
     mats = [P.poisson2d(int(s)) for s in sides]
@@ -900,7 +913,7 @@ def run_batched(args, d):
         x.zero_()
         out["r"] = core.batched_pcg(S, offs, bd, M, x=x, control=ctl)
     batched()
-    t_b, _ = _events_ms(torch, batched, max(3, args.steps))
+    t_b, _ = _events_ms(torch, batched, max(3, steps))
     _, iters, conv, _ = out["r"]
     # one system at a time, each with its own hierarchy (setup excluded from the time)
     singles = []
@@ -913,14 +926,20 @@ def run_batched(args, d):
         for Ak, Hk, Mk, bk in singles:
             core.pcg(Ak, bk, M=Mk, control=ctl)
     one_by_one()
-    t_s, _ = _events_ms(torch, one_by_one, 3)
-    res = {"mode": "batched", "systems": {
-        "workload": "256 2D 5-point Poisson systems, sides U{32..256} seed 0",
+    t_s, _ = _events_ms(torch, one_by_one, one_by_one_reps)
+    # per-system relative residual of the batched solution (inf norms)
+    rr = S.residual(x, bd).cpu().numpy()
+    worst = max(float(np.max(np.abs(rr[int(offs[k]):int(offs[k + 1])])))
+                / max(float(np.max(np.abs(bs[int(offs[k]):int(offs[k + 1])]))), 1e-300)
+                for k in range(len(mats)))
+    res = {"systems": {
+        "workload": "256 2D 5-point Poisson systems, sides U{32..256} seed 0, rtol 1e-8",
         "rows": int(offs[-1]), "setup_ms": t_setup, "solve_ms": t_b,
         "one_by_one_ms": t_s, "speedup": t_s / t_b, "iterations_max": int(iters.max()),
-        "iterations_min": int(iters.min()), "all_converged": bool(conv.all())}}
+        "iterations_min": int(iters.min()), "all_converged": bool(conv.all()),
+        "worst_rel_residual": worst}}
+    del singles
     # (b) multi-RHS
-    n = args.n or 64
     A = P.poisson3d(n)
     dA = core.CsrMatrix.from_arrays(*A)
     dA.analyse()
@@ -933,7 +952,7 @@ def run_batched(args, d):
         X.zero_()
         out["m"] = core.multi_rhs_pcg(dA, B, M2, X=X, control=ctl)
     multi()
-    t_m, _ = _events_ms(torch, multi, max(3, args.steps))
+    t_m, _ = _events_ms(torch, multi, max(3, steps))
     _, it2, conv2, _ = out["m"]
     cols = [B[k].contiguous() for k in range(32)]
 
@@ -942,25 +961,33 @@ def run_batched(args, d):
             core.pcg(dA, bk, M=M2, control=ctl)
     per_rhs()
     t_p, _ = _events_ms(torch, per_rhs, 3)
-    res["multi_rhs"] = {"workload": f"32 RHS U[-1,1] on 3D 7-point {n}^3", "solve_ms": t_m,
-                        "one_by_one_ms": t_p, "speedup": t_p / t_m,
+    res["multi_rhs"] = {"workload": f"32 RHS U[-1,1] on 3D 7-point {n}^3, rtol 1e-8",
+                        "solve_ms": t_m, "one_by_one_ms": t_p, "speedup": t_p / t_m,
                         "iterations_max": int(it2.max()), "all_converged": bool(conv2.all())}
-    if d.rank == 0:
-        print(json.dumps(res), flush=True)
-    d.close()
-    return 0
+    return res
 
 
-def run_adjoint(args, d):
-    """Weighted 7-point graph Laplacian (lognormal sigma 1, shift 1e-3) on n^3:
-    forward SA-AMG-PCG to 1e-10, adjoint solve lambda = A^-T (x - x_target), and
-    dL/dA on the pattern; a central finite difference along b checks dL/db."""
+def run_batched(args, d):
+    """The batched workloads (batched_workloads).  Under torchrun (N > 1) the batch
+    is split over the GPUs instead (run_batched_split)."""
     import torch
+    if d.world > 1:
+        return run_batched_split(args, d)
     d.init(need_gpu=True)
     import linalglib_b200.core as core
     from linalglib_b200 import problems as P
     core.init()
-    n = args.n or 96
+    res = batched_workloads(core, P, torch, args.steps, n=args.n or 64)
+    if d.rank == 0:
+        print(json.dumps({"mode": "batched", **res}), flush=True)
+    d.close()
+    return 0
+
+
+def adjoint_workload(core, P, torch, steps, n=96):
+    """Weighted 7-point graph Laplacian (lognormal sigma 1, shift 1e-3) on n^3:
+    forward SA-AMG-PCG to 1e-10, adjoint solve lambda = A^-T (x - x_target), and
+    dL/dA on the pattern; a central finite difference along b checks dL/db."""
     A = P.graph_laplacian3d(n, sigma=1.0, shift=1e-3, seed=0)
     b, _ = P.rhs_from_solution(*A, seed=0)
     xt = core.vec(np.random.default_rng(1).standard_normal(A[0].size - 1))
@@ -982,8 +1009,8 @@ def run_adjoint(args, d):
         st["gA"] = core.adjoint_grad_A(dA, st["lam"], st["x"])
     forward()
     backward()
-    t_f, _ = _events_ms(torch, forward, max(3, args.steps))
-    t_b, _ = _events_ms(torch, backward, max(3, args.steps))
+    t_f, _ = _events_ms(torch, forward, max(3, steps))
+    t_b, _ = _events_ms(torch, backward, max(3, steps))
     # directional check of dL/db = lambda along a random direction
     v = torch.from_numpy(np.random.default_rng(2).standard_normal(A[0].size - 1)).cuda()
     h = 1e-4
@@ -993,15 +1020,26 @@ def run_adjoint(args, d):
         return 0.5 * float(torch.sum((xx - xt) ** 2))
     fd = (loss(bd + h * v) - loss(bd - h * v)) / (2 * h)
     an = float(torch.dot(st["lam"], v))
-    res = {"mode": "adjoint", "config": {"workload": f"graph Laplacian {n}^3 (lognormal sigma 1, "
-                                                     "shift 1e-3), rtol 1e-10",
-                                         "rows": int(A[0].size - 1), "nnz": int(A[2].size)},
+    res = {"config": {"workload": f"graph Laplacian {n}^3 (lognormal sigma 1, "
+                                  "shift 1e-3), rtol 1e-10",
+                      "rows": int(A[0].size - 1), "nnz": int(A[2].size)},
            "setup_ms": t_setup, "forward_ms": t_f, "adjoint_ms": t_b,
            "forward_iterations": st["fi"].iterations, "adjoint_iterations": st["ai"].iterations,
            "dLdb_directional": {"adjoint": an, "finite_difference": fd,
                                 "rel_diff": abs(an - fd) / max(abs(fd), 1e-300)}}
+    return res
+
+
+def run_adjoint(args, d):
+    """The differentiation workload (adjoint_workload)."""
+    import torch
+    d.init(need_gpu=True)
+    import linalglib_b200.core as core
+    from linalglib_b200 import problems as P
+    core.init()
+    res = adjoint_workload(core, P, torch, args.steps, n=args.n or 96)
     if d.rank == 0:
-        print(json.dumps(res), flush=True)
+        print(json.dumps({"mode": "adjoint", **res}), flush=True)
     d.close()
     return 0
 
@@ -1021,6 +1059,26 @@ def tri_bytes(rp, ci, lower):
     nnz_t = int(np.count_nonzero(ci <= rows) if lower else np.count_nonzero(ci >= rows))
     m = rp.size - 1
     return 12 * nnz_t + 4 * (m + 1) + 16 * m, nnz_t
+
+
+def ilu0_workload(core, torch, dA, bd, rtol, steps):
+    """ILU(0)-PCG (the reference's ilu_precond with cg_solver) on an already built
+    system: a step is the preconditioner build plus the solve, device-resident."""
+    ctl = core.iter_control(rel_tol=rtol, abs_tol=0.0, max_iter=5000)
+    x = torch.zeros_like(bd)
+    st = {}
+
+    def step():
+        M = core.Preconditioner.ilu0(dA)
+        x.zero_()
+        _, st["info"] = core.pcg(dA, bd, x=x, M=M, control=ctl)
+        del M
+    step()
+    t_step, _ = _events_ms(torch, step, max(3, steps))
+    rr = dA.residual(x, bd)
+    return {"step_ms": t_step, "solves_per_s": 1e3 / t_step,
+            "iterations": st["info"].iterations, "converged": bool(st["info"].converged),
+            "true_rel_residual": float(torch.max(torch.abs(rr)) / torch.max(torch.abs(bd)))}
 
 
 def run_tri(args, d):
