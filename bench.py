@@ -66,9 +66,9 @@ def parse():
                     help="--mode spmv: time the SpMV of hierarchy level L's operator A_L "
                          "(0: the input matrix)")
     ap.add_argument("--no-workloads", action="store_true",
-                    help="full mode: skip the batched, multi-RHS, differentiation and "
-                         "ILU(0) summaries added to the line after the headline's timed "
-                         "regions")
+                    help="full mode: skip the batched, multi-RHS, differentiation, "
+                         "27-point mixed-precision and ILU(0) summaries added to the line "
+                         "after the headline's timed regions")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32", "fp32+bf16"],
                     help="--mode mixed: with --profile-range, the cycle precision whose timed "
                          "solves at rtol 1e-8 are bracketed")
@@ -547,8 +547,9 @@ def run_ours(args, d):
     pcg_roof = pcg_iteration_roofline(core, dA, solves, iters, roof["peak"])
     mixed, mixed_x = mixed_half(core, L, torch, dA, bd, ctl, setups, max(3, args.steps))
     setup_roof = setup_roofline(core, torch, dA, roof["peak"], setups)
-    # the other workloads (batched, multi-RHS, differentiation, ILU(0)-PCG), one GPU
-    # only, after every timed region of the headline
+    # the other workloads (batched, multi-RHS, differentiation, the 160^3 27-point
+    # mixed-precision system, ILU(0)-PCG), one GPU only, after every timed region of
+    # the headline
     workloads = None
     if d.world == 1 and not args.no_workloads:
         from linalglib_b200 import problems as P
@@ -556,6 +557,9 @@ def run_ours(args, d):
         for key, fn in (("batched", lambda: batched_workloads(core, P, torch, 3,
                                                                one_by_one_reps=1)),
                         ("adjoint", lambda: adjoint_workload(core, P, torch, 3)),
+                        ("mixed_config3", lambda: mixed_workload(
+                            core, L, P, torch, 3, matrix="diffusion27", n=160,
+                            rtols=(1e-10,))),
                         ("ilu0_pcg", lambda: dict(
                             ilu0_workload(core, torch, dA, bd, args.rtol, 3),
                             workload=f"ILU(0)-PCG, the same {args.n}^3 system, "
@@ -761,24 +765,20 @@ def _rel_res(torch, dA, x, b):
     return float(torch.max(torch.abs(r)) / torch.max(torch.abs(b)))
 
 
-def run_mixed(args, d):
+def mixed_workload(core, L, P, torch, steps, matrix=None, n=None, rtols=(1e-8, 1e-10),
+                   bracket=None):
     """27-point variable-coefficient diffusion (lognormal sigma 1.5, z x100) on an
-    n^3 grid (default; --matrix poisson: the 3D 7-point Poisson problem, omega 1):
-    one FP64 SA hierarchy, PCG with the FP64, FP32 and FP32+BF16 cycles to rtol
-    1e-8 and 1e-10; error of each against the FP64 solve."""
-    import torch
-    d.init(need_gpu=True)
-    import linalglib_b200.core as core
-    from linalglib_b200 import _lib as L
-    from linalglib_b200 import problems as P
-    core.init()
-    if args.matrix == "poisson":
+    n^3 grid (default; matrix "poisson": the 3D 7-point Poisson problem, omega 1):
+    one FP64 SA hierarchy, PCG with the FP64, FP32 and FP32+BF16 cycles to each rtol;
+    error of each against the FP64 solve.  bracket: the precision whose timed solves
+    at rtol 1e-8 run between cudaProfilerStart and cudaProfilerStop."""
+    if matrix == "poisson":
         # the 7-point Poisson problem with the reference's smoother weight
-        n = args.n or 128
+        n = n or 128
         A = P.poisson3d(n)
         omega, wl = 1.0, f"SA-AMG-PCG, 3D 7-point Poisson {n}^3, omega 1"
     else:
-        n = args.n or 160
+        n = n or 160
         A = P.diffusion27(n, sigma=1.5, zscale=100.0, seed=0)
         omega, wl = 2.0 / 3.0, (f"SA-AMG-PCG, 27-point diffusion {n}^3 (lognormal sigma 1.5, "
                                 "z x100), omega 2/3")
@@ -789,12 +789,11 @@ def run_mixed(args, d):
     xtd = core.vec(xt)
     H = core.Hierarchy(dA)  # warm-up (module loading, pool growth)
     t_setup, _ = _events_ms(torch, lambda: core.Hierarchy(dA), 3)
-    res = {"mode": "mixed", "config": {"workload": wl,
-                                       "rows": int(A[0].size - 1), "nnz": int(A[2].size),
-                                       "levels": H.levels},
+    res = {"config": {"workload": wl, "rows": int(A[0].size - 1), "nnz": int(A[2].size),
+                      "levels": H.levels},
            "setup_ms": t_setup, "runs": []}
     names = {L.PREC_FP64: "fp64", L.PREC_FP32: "fp32", L.PREC_FP32_BF16: "fp32+bf16"}
-    for rtol in (1e-8, 1e-10):
+    for rtol in rtols:
         ctl = core.iter_control(rel_tol=rtol, abs_tol=0.0, max_iter=1000)
         x64 = None
         for prec in (L.PREC_FP64, L.PREC_FP32, L.PREC_FP32_BF16):
@@ -806,12 +805,11 @@ def run_mixed(args, d):
             def solve():
                 x.zero_()
                 info.append(core.pcg(dA, bd, x=x, M=M, control=ctl)[1])
-            bracket = args.profile_range and rtol == 1e-8 and names[prec] == (args.precision
-                                                                               or "fp32")
-            if bracket:
+            brk = bracket is not None and rtol == 1e-8 and names[prec] == bracket
+            if brk:
                 torch.cuda.profiler.start()
-            t, ts = _events_ms(torch, solve, max(3, args.steps))
-            if bracket:
+            t, ts = _events_ms(torch, solve, max(3, steps))
+            if brk:
                 torch.cuda.profiler.stop()
             if prec == L.PREC_FP64:
                 x64 = x.clone()
@@ -826,8 +824,21 @@ def run_mixed(args, d):
         for r in res["runs"]:
             if r["rtol"] == rtol:
                 r["speedup_vs_fp64"] = base["solve_ms"] / r["solve_ms"]
+    return res
+
+
+def run_mixed(args, d):
+    """The mixed-precision workload (mixed_workload)."""
+    import torch
+    d.init(need_gpu=True)
+    import linalglib_b200.core as core
+    from linalglib_b200 import _lib as L
+    from linalglib_b200 import problems as P
+    core.init()
+    res = mixed_workload(core, L, P, torch, args.steps, matrix=args.matrix, n=args.n,
+                         bracket=(args.precision or "fp32") if args.profile_range else None)
     if d.rank == 0:
-        print(json.dumps(res), flush=True)
+        print(json.dumps({"mode": "mixed", **res}), flush=True)
     d.close()
     return 0
 
