@@ -363,90 +363,176 @@ namespace lab
             }
     }
 
-    // Dense inverse by Gauss-Jordan with partial pivoting, one CTA (n <= 1024).
-    __global__ void __launch_bounds__(1024)
-        k_gauss_jordan(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                       const double* __restrict__ v, int n, double* M, double* I, int* singular)
+    // Dense inverse of the coarsest operator by Gauss-Jordan with partial pivoting
+    // (n <= kCoarseDenseMax), the whole GPU per pivot column: k_gj_pivot (one CTA)
+    // picks the pivot -- the first row of the largest |M[r][c]|, r >= c, as a
+    // sequential scan with a strict comparison picks it (a NaN never wins; a NaN on
+    // the diagonal is kept) -- swaps, scales the pivot row and saves column c;
+    // k_gj_elim then subtracts f_r x (pivot row) from every other row of M and I
+    // with f_r from the saved column.  Columns of M left of c are exact zeros in
+    // rows c and p and never reach I, so their updates are skipped; every entry of
+    // I gets the same operations in the same order as a one-CTA sweep.
+    constexpr int kCoarseDenseMax = 4096;
+
+    __global__ void k_gj_init(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                              const double* __restrict__ v, int n, double* M, double* I)
     {
-        const int t  = threadIdx.x;
-        const int NT = blockDim.x;
-        for(size_t k = t; k < (size_t)n * n; k += NT)
+        const size_t nn = (size_t)n * n;
+        for(size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn;
+            k += (size_t)gridDim.x * blockDim.x)
         {
             M[k] = 0.0;
-            I[k] = 0.0;
+            I[k] = (k / n == k % n) ? 1.0 : 0.0;
         }
-        __syncthreads();
-        for(int i = t; i < n; i += NT)
-        {
-            I[(size_t)i * n + i] = 1.0;
+    }
+
+    __global__ void k_gj_scatter(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                 const double* __restrict__ v, int n, double* M)
+    {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i < n)
             for(int j = rp[i]; j < rp[i + 1]; j++)
                 M[(size_t)i * n + ci[j]] += v[j];
-        }
-        __syncthreads();
+    }
+
+    // Pivot step of column c by one CTA (1024 threads): pivot choice, row swap,
+    // scaling of the pivot row, column c saved to fcol.  Returns false (uniformly)
+    // when the column has no nonzero pivot (*singular set).
+    __device__ bool gj_pivot_step(double* M, double* I, int n, int c, double* fcol,
+                                  int* singular)
+    {
+        __shared__ double s_v[32];
+        __shared__ int    s_r[32];
         __shared__ int    s_piv;
         __shared__ double s_pv;
+        const int         t = threadIdx.x, lane = t & 31, wid = t >> 5;
+        double            bv = -1.0; // below every |x|; NaN never replaces it
+        int               br = n;
+        for(int r = c + t; r < n; r += blockDim.x)
+        {
+            const double a = fabs(M[(size_t)r * n + c]);
+            if(a > bv)
+            {
+                bv = a;
+                br = r;
+            }
+        }
+        // largest value, lowest row among equal values
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+        {
+            const double ov  = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int    orw = __shfl_xor_sync(0xffffffffu, br, o);
+            if(ov > bv || (ov == bv && orw < br))
+            {
+                bv = ov;
+                br = orw;
+            }
+        }
+        if(lane == 0)
+        {
+            s_v[wid] = bv;
+            s_r[wid] = br;
+        }
+        __syncthreads();
+        if(t == 0)
+        {
+            for(int w = 1; w < (int)(blockDim.x >> 5); w++)
+                if(s_v[w] > bv || (s_v[w] == bv && s_r[w] < br))
+                {
+                    bv = s_v[w];
+                    br = s_r[w];
+                }
+            const double ac = fabs(M[(size_t)c * n + c]);
+            s_piv = isnan(ac) ? c : br;
+            s_pv  = isnan(ac) ? ac : bv;
+            if(s_pv == 0.0)
+                *singular = 1;
+        }
+        __syncthreads();
+        if(s_pv == 0.0)
+            return false;
+        const int p = s_piv;
+        if(p != c)
+        {
+            for(int k = c + t; k < n; k += blockDim.x)
+            {
+                const double a       = M[(size_t)c * n + k];
+                M[(size_t)c * n + k] = M[(size_t)p * n + k];
+                M[(size_t)p * n + k] = a;
+            }
+            for(int k = t; k < n; k += blockDim.x)
+            {
+                const double a       = I[(size_t)c * n + k];
+                I[(size_t)c * n + k] = I[(size_t)p * n + k];
+                I[(size_t)p * n + k] = a;
+            }
+        }
+        __syncthreads();
+        const double inv = 1.0 / M[(size_t)c * n + c];
+        __syncthreads();
+        for(int k = c + t; k < n; k += blockDim.x)
+            M[(size_t)c * n + k] *= inv;
+        for(int k = t; k < n; k += blockDim.x)
+            I[(size_t)c * n + k] *= inv;
+        for(int r = t; r < n; r += blockDim.x)
+            if(r != c) // row c is being scaled; the elimination skips it
+                fcol[r] = M[(size_t)r * n + c];
+        return true;
+    }
+
+    // Entry (r, k), r != c, of the elimination of column c (f = the saved M[r][c]).
+    __device__ __forceinline__ void gj_elim_entry(double* M, double* I, int n, int c, int r,
+                                                  int k, double f)
+    {
+        if(k == c)
+        {
+            I[(size_t)r * n + c] -= f * I[(size_t)c * n + c];
+            M[(size_t)r * n + c] = 0.0;
+            return;
+        }
+        if(k > c)
+            M[(size_t)r * n + k] -= f * M[(size_t)c * n + k];
+        I[(size_t)r * n + k] -= f * I[(size_t)c * n + k];
+    }
+
+    __global__ void __launch_bounds__(1024)
+        k_gj_pivot(double* M, double* I, int n, int c, double* fcol, int* singular)
+    {
+        if(*singular)
+            return;
+        gj_pivot_step(M, I, n, c, fcol, singular);
+    }
+
+    // grid (ceil(n / 256), n): row blockIdx.y, columns blockIdx.x * 256 + threadIdx.x
+    __global__ void __launch_bounds__(256)
+        k_gj_elim(double* M, double* I, int n, int c, const double* __restrict__ fcol,
+                  const int* singular)
+    {
+        const int r = blockIdx.y;
+        const int k = blockIdx.x * 256 + threadIdx.x;
+        if(*singular || r == c || k >= n)
+            return;
+        gj_elim_entry(M, I, n, c, r, k, fcol[r]);
+    }
+
+    // The same steps in one CTA for small coarsest levels (n <= kCoarseDenseOneCta),
+    // where a pair of launches per column would cost more than the work.
+    constexpr int kCoarseDenseOneCta = 256;
+    __global__ void __launch_bounds__(1024)
+        k_gj_small(double* M, double* I, int n, double* fcol, int* singular)
+    {
         for(int c = 0; c < n; c++)
         {
-            if(t == 0)
-            {
-                int    p  = c;
-                double pv = fabs(M[(size_t)c * n + c]);
-                for(int r = c + 1; r < n; r++)
-                {
-                    double a = fabs(M[(size_t)r * n + c]);
-                    if(a > pv)
-                    {
-                        pv = a;
-                        p  = r;
-                    }
-                }
-                s_piv = p;
-                s_pv  = pv;
-            }
-            __syncthreads();
-            if(s_pv == 0.0)
-            {
-                if(t == 0)
-                    *singular = 1;
+            if(!gj_pivot_step(M, I, n, c, fcol, singular))
                 return;
-            }
-            int p = s_piv;
-            if(p != c)
-                for(int k = t; k < n; k += NT)
-                {
-                    double a             = M[(size_t)c * n + k];
-                    M[(size_t)c * n + k] = M[(size_t)p * n + k];
-                    M[(size_t)p * n + k] = a;
-                    a                    = I[(size_t)c * n + k];
-                    I[(size_t)c * n + k] = I[(size_t)p * n + k];
-                    I[(size_t)p * n + k] = a;
-                }
             __syncthreads();
-            const double inv = 1.0 / M[(size_t)c * n + c];
-            __syncthreads();
-            for(int k = t; k < n; k += NT)
+            for(int q = threadIdx.x; q < n * n; q += blockDim.x)
             {
-                M[(size_t)c * n + k] *= inv;
-                I[(size_t)c * n + k] *= inv;
-            }
-            __syncthreads();
-            for(size_t q = t; q < (size_t)n * n; q += NT)
-            {
-                int r = (int)(q / n), k = (int)(q % n);
-                if(r == c || k == c)
-                    continue;
-                double f = M[(size_t)r * n + c];
-                M[q] -= f * M[(size_t)c * n + k];
-                I[q] -= f * I[(size_t)c * n + k];
-            }
-            __syncthreads();
-            for(int r = t; r < n; r += NT)
+                const int r = q / n, k = q % n;
                 if(r != c)
-                {
-                    double f             = M[(size_t)r * n + c];
-                    I[(size_t)r * n + c] -= f * I[(size_t)c * n + c];
-                    M[(size_t)r * n + c] = 0.0;
-                }
+                    gj_elim_entry(M, I, n, c, r, k, fcol[r]);
+            }
             __syncthreads();
         }
     }
@@ -735,19 +821,38 @@ namespace lab
         const int     n = (int)A->m;
         if(n <= 1 || coarse_mode != LAB_COARSE_DIRECT || h->coarse_inv || h->coarse_singular)
             return LAB_OK;
-        if(n > 1024)
+        if(n > kCoarseDenseMax)
         {
             h->coarse_singular = 2; // too large for the dense path: GS sweeps are used
             return LAB_OK;
         }
-        dbuf<double> M;
+        dbuf<double> M, fcol;
         dbuf<int>    sing;
         LAB_TRY(M.alloc((size_t)n * n, s));
+        LAB_TRY(fcol.alloc((size_t)n, s));
         LAB_TRY(sing.alloc(1, s));
         LAB_TRY(dalloc(&h->coarse_inv, (size_t)n * n, s));
         LAB_CUDA(cudaMemsetAsync(sing.get(), 0, sizeof(int), s));
-        LAB_LAUNCH(k_gauss_jordan, 1, 1024, 0, s, A->row_ptr, A->col_ind, A->val, n, M.get(),
-                   h->coarse_inv, sing.get());
+        const unsigned ginit = (unsigned)std::min<int64_t>(
+            ceil_div<int64_t>((int64_t)n * n, 256), (int64_t)num_sms() * 8);
+        LAB_LAUNCH(k_gj_init, ginit, 256, 0, s, A->row_ptr, A->col_ind, A->val, n, M.get(),
+                   h->coarse_inv);
+        LAB_LAUNCH(k_gj_scatter, (unsigned)ceil_div(n, 256), 256, 0, s, A->row_ptr, A->col_ind,
+                   A->val, n, M.get());
+        if(n <= kCoarseDenseOneCta)
+            LAB_LAUNCH(k_gj_small, 1, 1024, 0, s, M.get(), h->coarse_inv, n, fcol.get(),
+                       sing.get());
+        else
+        {
+            const dim3 gel((unsigned)ceil_div(n, 256), (unsigned)n);
+            for(int c = 0; c < n; c++)
+            {
+                LAB_LAUNCH(k_gj_pivot, 1, 1024, 0, s, M.get(), h->coarse_inv, n, c,
+                           fcol.get(), sing.get());
+                LAB_LAUNCH(k_gj_elim, gel, 256, 0, s, M.get(), h->coarse_inv, n, c,
+                           (const double*)fcol.get(), (const int*)sing.get());
+            }
+        }
         int hs = 0;
         LAB_TRY(copy_d2h_sync(&hs, sing.get(), sizeof(int), s));
         if(hs)
