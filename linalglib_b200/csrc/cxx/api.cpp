@@ -962,21 +962,39 @@ namespace linalg
         if(ok(lab_spgemm(A.device(), B.device(), &out, nullptr), "csrgemm_nnz"))
             C.adopt(out, true);
     }
+    // C = alpha A B + beta D (host_csrgemm.cpp:92-182): alpha is applied to A's values
+    // before the products, (alpha a_ij) b_jk (line 122), as the reference forms them,
+    // so alpha != 1 rounds the same way; beta D is added after all products of a row,
+    // entry by entry, p + beta d (lines 140-158), which is SpGEAM's 1 * P + beta * D.
+    // (The reference's host path leaves D out of the pattern, host_csrgemm.cpp:186-213,
+    // and runs with beta = 0 only.)
     void csrgemm_solve(double alpha, const csr_matrix<double>& A, const csr_matrix<double>& B,
-                       double, const csr_matrix<double>&, csr_matrix<double>& C, csrgemm_algorithm,
-                       const csrgemm_descr*)
+                       double beta, const csr_matrix<double>& D, csr_matrix<double>& C,
+                       csrgemm_algorithm, const csrgemm_descr*)
     {
-        lab_csr out = nullptr;
-        if(!ok(lab_spgemm(A.device(), B.device(), &out, nullptr), "csrgemm_solve"))
-            return;
+        lab_csr left = A.device(), scaled = nullptr;
         if(alpha != 1.0)
         {
-            lab_csr scaled = nullptr;
-            if(ok(lab_spgeam(alpha, out, 0.0, out, &scaled, nullptr), "csrgemm_solve scale"))
-            {
-                lab_csr_destroy(out);
-                out = scaled;
-            }
+            if(!ok(lab_spgeam(alpha, A.device(), 0.0, A.device(), &scaled, nullptr),
+                   "csrgemm_solve alpha"))
+                return;
+            left = scaled;
+        }
+        lab_csr out = nullptr;
+        const bool done = ok(lab_spgemm(left, B.device(), &out, nullptr), "csrgemm_solve");
+        if(scaled)
+            lab_csr_destroy(scaled);
+        if(!done)
+            return;
+        if(beta != 0.0 && D.get_nnz() > 0)
+        {
+            lab_csr sum = nullptr;
+            const bool added = ok(lab_spgeam(1.0, out, beta, D.device(), &sum, nullptr),
+                                  "csrgemm_solve beta D");
+            lab_csr_destroy(out);
+            if(!added)
+                return;
+            out = sum;
         }
         C.adopt(out, true);
     }

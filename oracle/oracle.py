@@ -340,6 +340,8 @@ class Reference:
         L.ref_spgemm.argtypes = [_i, _i, _i, _p, _p, _p, _i, _i, _i, _p, _p, _p]
         L.ref_spgeam.restype = _p
         L.ref_spgeam.argtypes = [_d, _i, _i, _i, _p, _p, _p, _d, _i, _p, _p, _p]
+        L.ref_csrgemm.restype = _p
+        L.ref_csrgemm.argtypes = [_d, _i, _i, _i, _p, _p, _p, _i, _i, _i, _p, _p, _p]
         L.ref_transpose.restype = _p
         L.ref_transpose.argtypes = [_i, _i, _i, _p, _p, _p]
         L.ref_mat_dims.argtypes = [_p, _p, _p, _p]
@@ -401,6 +403,14 @@ class Reference:
         b = self._arr(B)
         M = self.L.ref_spgemm(a[3], a[4], a[5], _ptr(a[0]), _ptr(a[1]), _ptr(a[2]),
                               b[3], b[4], b[5], _ptr(b[0]), _ptr(b[1]), _ptr(b[2]))
+        return self._mat(M)
+
+    def csrgemm(self, alpha, A, B):
+        """C = alpha * A * B through the reference's csrgemm_nnz / csrgemm_solve."""
+        a = self._arr(A)
+        b = self._arr(B)
+        M = self.L.ref_csrgemm(alpha, a[3], a[4], a[5], _ptr(a[0]), _ptr(a[1]), _ptr(a[2]),
+                               b[3], b[4], b[5], _ptr(b[0]), _ptr(b[1]), _ptr(b[2]))
         return self._mat(M)
 
     def spgeam(self, alpha, A, beta, B):

@@ -340,6 +340,26 @@ void* ref_spgemm(int ma, int na, int nnza, const int* rpa, const int* cia, const
     return C;
 }
 
+// C = alpha * A * B through the descriptor form csrgemm_nnz + csrgemm_solve
+// (linalg_math.cpp:330-357, host_csrgemm.cpp:195-245) with beta = 0 and an empty D,
+// the form the reference's host path runs.
+void* ref_csrgemm(double alpha, int ma, int na, int nnza, const int* rpa, const int* cia,
+                  const double* va, int mb, int nb, int nnzb, const int* rpb, const int* cib,
+                  const double* vb)
+{
+    quiet_scope        q;
+    csr_matrix<double> A, B, D;
+    to_csr(A, ma, na, nnza, rpa, cia, va);
+    to_csr(B, mb, nb, nnzb, rpb, cib, vb);
+    csr_matrix<double>* C = new csr_matrix<double>();
+    csrgemm_descr*      d = nullptr;
+    create_csrgemm_descr(&d);
+    csrgemm_nnz(A, B, D, *C, csrgemm_algorithm::default_algorithm, d);
+    csrgemm_solve(alpha, A, B, 0.0, D, *C, csrgemm_algorithm::default_algorithm, d);
+    destroy_csrgemm_descr(d);
+    return C;
+}
+
 // C = alpha*A + beta*B through csrgeam (linalg_math.cpp:275-307).
 void* ref_spgeam(double alpha, int m, int n, int nnza, const int* rpa, const int* cia,
                  const double* va, double beta, int nnzb, const int* rpb, const int* cib,

@@ -108,3 +108,64 @@ def test_cxx_matrix_members_and_mtx(gpu, reference, tmp_path_factory, tmp_path):
     xl, xu = xs[:m], xs[m:]
     assert np.array_equal(xl.view(np.int64), reference.trsv(A, np.ones(m), True, False).view(np.int64))
     assert np.array_equal(xu.view(np.int64), reference.trsv(A, np.ones(m), False, False).view(np.int64))
+
+
+def _random_csr(rng, m, n, per_row):
+    """Sorted distinct columns, per_row per row on average, values U[-1, 1]."""
+    rows = np.repeat(np.arange(m), rng.integers(1, 2 * per_row, size=m))
+    key = np.unique(rows.astype(np.int64) * n + rng.integers(0, n, size=rows.size))
+    rp = np.zeros(m + 1, dtype=np.int64)
+    np.add.at(rp, key // n + 1, 1)
+    return (np.cumsum(rp).astype(np.int32), (key % n).astype(np.int32),
+            rng.uniform(-1, 1, key.size), n)
+
+
+def _write_mtx_exact(path, A):
+    rp, ci, v, n = A
+    m = rp.size - 1
+    rows = np.repeat(np.arange(m), np.diff(rp))
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{m} {n} {ci.size}\n")
+        for r, c, x in zip(rows, ci, v):
+            f.write(f"{r + 1} {c + 1} {float(x)!r}\n")
+
+
+@pytest.fixture(scope="module")
+def csrgemm_exe(tmp_path_factory):
+    return _compile(tmp_path_factory, "csrgemm_example")
+
+
+@pytest.mark.parametrize("alpha, beta", [(1.0, 0.0), (0.3, 0.0), (-1.7, 0.45)])
+def test_cxx_csrgemm_matches_reference(gpu, reference, csrgemm_exe, tmp_path, alpha, beta):
+    """C = alpha A B (+ beta D) through csrgemm_nnz / csrgemm_solve: bit-identical to
+    the reference's csrgemm (alpha applied to A's values before the products); the
+    beta D term, which the reference's host path does not run, equals its SpGEAM of
+    the product and D."""
+    from helpers import csr_diff, csr_equal
+    rng = np.random.default_rng(17)
+    A = _random_csr(rng, 400, 300, 6)
+    B = _random_csr(rng, 300, 250, 5)
+    D = _random_csr(rng, 400, 250, 4)
+    paths = []
+    for name, M in (("A", A), ("B", B), ("D", D)):
+        paths.append(str(tmp_path / f"{name}.mtx"))
+        _write_mtx_exact(paths[-1], M)
+    out = subprocess.run([csrgemm_exe, *paths, repr(alpha), repr(beta)], capture_output=True,
+                         text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    t = out.stdout.split()
+    m, n, nnz = int(t[0]), int(t[1]), int(t[2])
+    rp = np.array(t[3:4 + m], dtype=np.int32)
+    ci = np.array(t[4 + m:4 + m + nnz], dtype=np.int32)
+    v = np.array([float.fromhex(x) for x in t[4 + m + nnz:4 + m + 2 * nnz]])
+    ours = (rp, ci, v, n)
+    ref = reference.csrgemm(alpha, A, B)
+    if beta != 0.0:
+        ref = reference.spgeam(1.0, ref, beta, D)
+    assert csr_equal(ours, ref), csr_diff(ours, ref)
+    if alpha != 1.0:
+        # the scaled-after form would differ: the reference rounds (alpha a) b
+        scaled_after = reference.spgeam(alpha, reference.spgemm(A, B), 0.0,
+                                        reference.spgemm(A, B))
+        assert not np.array_equal(scaled_after[2], reference.csrgemm(alpha, A, B)[2])
