@@ -1253,11 +1253,12 @@ namespace lab
     // both get these plans, so they run identical cycles.
     lab_status hierarchy_plans(hierarchy_impl* h, cudaStream_t s)
     {
+        // every level's statistics with one host round trip
+        LAB_TRY(spmv_analyse_batch(h->A + 1, h->levels, s));
         for(int l = 1; l <= h->levels; l++)
         {
             lab_csr_impl* Al = h->A[l];
-            LAB_TRY(spmv_analyse(Al, s));
-            spmv_plan& p = Al->plan;
+            spmv_plan&    p  = Al->plan;
             if(p.forced || Al->m == 0)
                 continue;
             if(Al->m <= 16)

@@ -869,6 +869,21 @@ namespace lab
     {
         const int  L     = h->levels;
         const bool lowp  = o->precision != LAB_PREC_FP64;
+        {
+            // the SpMV plans of every operator, prolongation and restriction with one
+            // host round trip (the per-level calls below then find them analysed)
+            std::vector<lab_csr_impl*> all;
+            for(int l = 0; l <= L; l++)
+            {
+                all.push_back(h->A[l]);
+                if(l < L)
+                {
+                    all.push_back(h->P[l]);
+                    all.push_back(h->R[l]);
+                }
+            }
+            LAB_TRY(spmv_analyse_batch(all.data(), (int)all.size(), s));
+        }
         for(int l = 0; l <= L; l++)
         {
             lab_csr_impl* A = h->A[l];

@@ -233,6 +233,8 @@ namespace lab
     lab_status diag_into(const lab_csr_impl* A, double* d, double* invd, cudaStream_t s);
     lab_status csr_ensure_lowp(lab_csr_impl* A, int precision, int use_bf16, cudaStream_t s);
     lab_status spmv_analyse(lab_csr_impl* A, cudaStream_t s);
+    // The same for several matrices with one host round trip (nulls skipped).
+    lab_status spmv_analyse_batch(lab_csr_impl* const* mats, int count, cudaStream_t s);
     // Builds A's halo plan (spmv_plan::hcnt/hcol/hloc) unless it was examined.
     lab_status halo_build(lab_csr_impl* A, cudaStream_t s);
     lab_status spmm_columns(const lab_csr_impl* A, int k, const double* X, int64_t ldx, double* Y,

@@ -3,6 +3,7 @@
 #include "spmv_engine.cuh"
 
 #include <climits>
+#include <vector>
 
 namespace lab
 {
@@ -309,90 +310,146 @@ namespace lab
     // then a 16-bit offset copy is built once per pattern and the row kernels read
     // it in place of the int32 columns in every precision (2 instead of 4 index
     // bytes per entry; the column, and so the arithmetic, is the same).
+    // Analysis of several matrices with one host round trip: every matrix's statistics
+    // kernels (and 16-bit offset copy) are enqueued, all statistics come back in one
+    // copy, then each plan is finished.  Matrices already analysed are skipped.
+    lab_status spmv_analyse_batch(lab_csr_impl* const* mats, int count, cudaStream_t s)
+    {
+        struct item
+        {
+            lab_csr_impl* A;
+            int           st_rows = 0;
+            bool          build   = false; // 16-bit offset copy enqueued
+        };
+        std::vector<item> todo;
+        for(int k = 0; k < count; k++)
+            if(mats[k] && !mats[k]->plan.analysed)
+            {
+                bool dup = false;
+                for(const item& t : todo)
+                    dup = dup || t.A == mats[k];
+                if(!dup)
+                    todo.push_back(item{mats[k]});
+            }
+        if(todo.empty())
+            return LAB_OK;
+        // per matrix: longest row, offsets too wide for 16 bits, largest stream tile
+        const int        nt = (int)todo.size();
+        std::vector<int> stats(3 * (size_t)nt, 0);
+        int*             d  = nullptr;
+        LAB_TRY(dalloc(&d, 3 * (size_t)nt, s));
+        LAB_CUDA(cudaMemsetAsync(d, 0, 3 * sizeof(int) * (size_t)nt, s));
+        lab_status st = LAB_OK;
+        for(int k = 0; k < nt && st == LAB_OK; k++)
+        {
+            lab_csr_impl* A  = todo[k].A;
+            int*          dk = d + 3 * k;
+            if(A->m == 0)
+                continue;
+            st = [&]() -> lab_status {
+                spmv_plan&     p    = A->plan;
+                const unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(A->m, 256), 2048);
+                LAB_LAUNCH(k_row_stats, grid, 256, 0, s, A->row_ptr, A->m, dk);
+                if(A->m >= kStreamMinRows && A->nnz > 0)
+                {
+                    // tiles of at most about kStreamTileEntries entries and a whole
+                    // number of consumer passes (8 warps x 32 / W rows, W the lane count
+                    // the VECTOR plan takes), so every consumer warp has rows in every
+                    // tile; a multiple of 4 rows keeps the row-pointer copy 16-byte aligned
+                    const double avg = (double)A->nnz / (double)A->m;
+                    const int    w   = p.forced && p.alg == LAB_SPMV_VECTOR ? p.lanes
+                                                                           : pow2_at_most(avg / 5.0);
+                    const int    rpp = kStreamConsumers * 32 / w;
+                    const int    str =
+                        std::min(1024, rpp * std::max(1, (int)(kStreamTileEntries / avg / rpp)));
+                    todo[k].st_rows   = str;
+                    const int64_t ntl = ceil_div<int64_t>(A->m, str);
+                    LAB_LAUNCH(k_tile_max,
+                               (unsigned)std::min<int64_t>(ceil_div<int64_t>(ntl, 256), 1024), 256, 0,
+                               s, A->row_ptr, A->m, str, dk + 2);
+                }
+                // square matrices only: a prolongation's or restriction's col - row
+                // spans the ratio of the two grids and does not fit
+                if(A->lp.dcol_state == 0 && A->nnz > 0 && A->m == A->n)
+                {
+                    LAB_TRY(dalloc(&A->lp.dcol, (size_t)A->nnz, s));
+                    todo[k].build = true;
+                    // lanes per row: the largest power of two <= the mean row length
+                    const double avg = (double)A->nnz / (double)A->m;
+                    int          w   = 1;
+                    while(w < 32 && 2 * w <= avg)
+                        w <<= 1;
+                    const unsigned g = (unsigned)std::min<int64_t>(
+                        ceil_div<int64_t>(A->m * (int64_t)w, 256), (int64_t)num_sms() * 8);
+                    switch(w)
+                    {
+                    case 1: LAB_LAUNCH(k_dcol_build<1>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, dk + 1); break;
+                    case 2: LAB_LAUNCH(k_dcol_build<2>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, dk + 1); break;
+                    case 4: LAB_LAUNCH(k_dcol_build<4>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, dk + 1); break;
+                    case 8: LAB_LAUNCH(k_dcol_build<8>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, dk + 1); break;
+                    case 16: LAB_LAUNCH(k_dcol_build<16>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, dk + 1); break;
+                    default: LAB_LAUNCH(k_dcol_build<32>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, dk + 1); break;
+                    }
+                }
+                return LAB_OK;
+            }();
+        }
+        if(st == LAB_OK)
+            st = copy_d2h_sync(stats.data(), d, sizeof(int) * stats.size(), s);
+        dfree(d, s);
+        if(st != LAB_OK)
+        {
+            // an enqueued offset copy whose check did not come back is dropped
+            for(const item& t : todo)
+                if(t.build)
+                {
+                    dfree(t.A->lp.dcol, s);
+                    t.A->lp.dcol = nullptr;
+                }
+            return st;
+        }
+        for(int k = 0; k < nt; k++)
+        {
+            lab_csr_impl* A  = todo[k].A;
+            spmv_plan&    p  = A->plan;
+            const int*    sk = stats.data() + 3 * k;
+            if(A->m > 0)
+            {
+                // stage capacity: the largest tile plus the alignment slack of its
+                // copies (start rounded down to 16 bytes, quads read past the row end)
+                const int cap = sk[2] + 16;
+                p.st_rows     = todo[k].st_rows > 0 && cap <= kStreamMaxCap ? todo[k].st_rows : 0;
+                p.st_cap      = p.st_rows ? cap : 0;
+                if(todo[k].build)
+                {
+                    A->lp.dcol_state = sk[1] ? -1 : 1;
+                    if(sk[1])
+                    {
+                        dfree(A->lp.dcol, s);
+                        A->lp.dcol = nullptr;
+                    }
+                }
+            }
+            const int maxlen = sk[0];
+            p.max_row        = maxlen;
+            p.avg_row        = A->m > 0 ? (double)A->nnz / (double)A->m : 0.0;
+            p.vlanes         = pow2_at_most(p.avg_row / 5.0);
+            if(!p.forced)
+            {
+                p.alg   = maxlen <= 32 ? LAB_SPMV_ROWSEQ : LAB_SPMV_VECTOR;
+                p.lanes = maxlen <= 32 ? 1 : p.vlanes;
+            }
+            p.analysed = 1;
+            if(p.forced && p.alg == LAB_SPMV_VECTOR && p.halo_use && !p.stream &&
+               p.halo_state == 0)
+                LAB_TRY(halo_build(A, s));
+        }
+        return LAB_OK;
+    }
+
     lab_status spmv_analyse(lab_csr_impl* A, cudaStream_t s)
     {
-        spmv_plan& p = A->plan;
-        if(p.analysed)
-            return LAB_OK;
-        // longest row, offsets too wide for 16 bits, largest stream tile
-        int stats[3] = {0, 0, 0};
-        int st_rows  = 0;
-        if(A->m > 0)
-        {
-            int* d = nullptr;
-            LAB_TRY(dalloc(&d, 3, s));
-            LAB_CUDA(cudaMemsetAsync(d, 0, 3 * sizeof(int), s));
-            unsigned grid = (unsigned)std::min<int64_t>(ceil_div<int64_t>(A->m, 256), 2048);
-            LAB_LAUNCH(k_row_stats, grid, 256, 0, s, A->row_ptr, A->m, d);
-            if(A->m >= kStreamMinRows && A->nnz > 0)
-            {
-                // tiles of at most about kStreamTileEntries entries and a whole number
-                // of consumer passes (8 warps x 32 / W rows, W the lane count the
-                // VECTOR plan takes), so every consumer warp has rows in every tile;
-                // a multiple of 4 rows keeps the row-pointer copy 16-byte aligned
-                const double avg = (double)A->nnz / (double)A->m;
-                const int    w   = p.forced && p.alg == LAB_SPMV_VECTOR ? p.lanes
-                                                                       : pow2_at_most(avg / 5.0);
-                const int    rpp = kStreamConsumers * 32 / w;
-                st_rows = std::min(1024, rpp * std::max(1, (int)(kStreamTileEntries / avg / rpp)));
-                const int64_t nt = ceil_div<int64_t>(A->m, st_rows);
-                LAB_LAUNCH(k_tile_max, (unsigned)std::min<int64_t>(ceil_div<int64_t>(nt, 256), 1024),
-                           256, 0, s, A->row_ptr, A->m, st_rows, d + 2);
-            }
-            // square matrices only: a prolongation's or restriction's col - row
-            // spans the ratio of the two grids and does not fit
-            const bool build = A->lp.dcol_state == 0 && A->nnz > 0 && A->m == A->n;
-            if(build)
-            {
-                LAB_TRY(dalloc(&A->lp.dcol, (size_t)A->nnz, s));
-                // lanes per row: the largest power of two <= the mean row length
-                const double avg = (double)A->nnz / (double)A->m;
-                int          w   = 1;
-                while(w < 32 && 2 * w <= avg)
-                    w <<= 1;
-                const unsigned g = (unsigned)std::min<int64_t>(
-                    ceil_div<int64_t>(A->m * (int64_t)w, 256), (int64_t)num_sms() * 8);
-                switch(w)
-                {
-                case 1: LAB_LAUNCH(k_dcol_build<1>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
-                case 2: LAB_LAUNCH(k_dcol_build<2>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
-                case 4: LAB_LAUNCH(k_dcol_build<4>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
-                case 8: LAB_LAUNCH(k_dcol_build<8>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
-                case 16: LAB_LAUNCH(k_dcol_build<16>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
-                default: LAB_LAUNCH(k_dcol_build<32>, g, 256, 0, s, A->row_ptr, A->col_ind, A->m, A->lp.dcol, d + 1); break;
-                }
-            }
-            lab_status st = copy_d2h_sync(stats, d, sizeof(stats), s);
-            dfree(d, s);
-            LAB_TRY(st);
-            // stage capacity: the largest tile plus the alignment slack of its copies
-            // (start rounded down to 16 bytes, quads read past the row end)
-            const int cap = stats[2] + 16;
-            p.st_rows     = st_rows > 0 && cap <= kStreamMaxCap ? st_rows : 0;
-            p.st_cap      = p.st_rows ? cap : 0;
-            if(build)
-            {
-                A->lp.dcol_state = stats[1] ? -1 : 1;
-                if(stats[1])
-                {
-                    dfree(A->lp.dcol, s);
-                    A->lp.dcol = nullptr;
-                }
-            }
-        }
-        const int maxlen = stats[0];
-        p.max_row = maxlen;
-        p.avg_row = A->m > 0 ? (double)A->nnz / (double)A->m : 0.0;
-        p.vlanes  = pow2_at_most(p.avg_row / 5.0);
-        if(!p.forced)
-        {
-            p.alg   = maxlen <= 32 ? LAB_SPMV_ROWSEQ : LAB_SPMV_VECTOR;
-            p.lanes = maxlen <= 32 ? 1 : p.vlanes;
-        }
-        p.analysed = 1;
-        if(p.forced && p.alg == LAB_SPMV_VECTOR && p.halo_use && !p.stream && p.halo_state == 0)
-            LAB_TRY(halo_build(A, s));
-        return LAB_OK;
+        return spmv_analyse_batch(&A, 1, s);
     }
 
     // SpMM: column-major X (n x k), Y (m x k); one pass over A per column block of
