@@ -233,8 +233,72 @@ namespace lab
         F_COUNT  = 8
     };
 
+    // Host-side resources of a PCG workspace (pinned flag slots, two events, the
+    // capture stream), kept per device for reuse when a workspace goes away: a
+    // caller that builds a new matrix for every solve then pays no page-locking,
+    // event or stream creation per solve, and no cudaFreeHost (which synchronises
+    // the device).  At most kResPool sets per device are kept; the lists are never
+    // destroyed (workspaces can be released during static destruction).
+    struct pcg_host_res
+    {
+        int*         hflags = nullptr;
+        cudaEvent_t  ev[2]  = {nullptr, nullptr};
+        cudaStream_t cap    = nullptr;
+    };
+    constexpr size_t kResPool = 16;
+    static std::mutex& res_mu()
+    {
+        static std::mutex* mu = new std::mutex;
+        return *mu;
+    }
+    static std::map<int, std::vector<pcg_host_res>>& res_pool()
+    {
+        static auto* pool = new std::map<int, std::vector<pcg_host_res>>;
+        return *pool;
+    }
+    static lab_status res_take(int dev, pcg_host_res* out)
+    {
+        {
+            std::lock_guard<std::mutex> g(res_mu());
+            auto&                       v = res_pool()[dev];
+            if(!v.empty())
+            {
+                *out = v.back();
+                v.pop_back();
+                return LAB_OK;
+            }
+        }
+        pcg_host_res r;
+        LAB_CUDA(cudaMallocHost(&r.hflags, sizeof(int) * F_COUNT * 2));
+        LAB_CUDA(cudaEventCreateWithFlags(&r.ev[0], cudaEventDisableTiming));
+        LAB_CUDA(cudaEventCreateWithFlags(&r.ev[1], cudaEventDisableTiming));
+        LAB_CUDA(cudaStreamCreateWithFlags(&r.cap, cudaStreamNonBlocking));
+        *out = r;
+        return LAB_OK;
+    }
+    static void res_give(int dev, const pcg_host_res& r)
+    {
+        {
+            std::lock_guard<std::mutex> g(res_mu());
+            auto&                       v = res_pool()[dev];
+            if(v.size() < kResPool && r.hflags && r.ev[0] && r.ev[1] && r.cap)
+            {
+                v.push_back(r);
+                return;
+            }
+        }
+        if(r.hflags)
+            cudaFreeHost(r.hflags);
+        for(auto e : r.ev)
+            if(e)
+                cudaEventDestroy(e);
+        if(r.cap)
+            cudaStreamDestroy(r.cap);
+    }
+
     struct pcg_ws
     {
+        int           dev   = 0; // device the host-side resources belong to
         int64_t       m     = 0;
         double*       r     = nullptr;
         double*       z     = nullptr;
@@ -272,13 +336,12 @@ namespace lab
             for(void* x : dp)
                 if(x)
                     cudaFree(x);
-            if(hflags)
-                cudaFreeHost(hflags);
-            for(auto& e : ev)
-                if(e)
-                    cudaEventDestroy(e);
-            if(cap)
-                cudaStreamDestroy(cap);
+            pcg_host_res res;
+            res.hflags = hflags;
+            res.ev[0]  = ev[0];
+            res.ev[1]  = ev[1];
+            res.cap    = cap;
+            res_give(dev, res);
         }
     };
 
@@ -460,10 +523,13 @@ namespace lab
         LAB_TRY(dalloc(&w->counters, 16, s));
         LAB_CUDA(cudaMemsetAsync(w->counters, 0, sizeof(unsigned int) * 16, s));
         LAB_CUDA(cudaMemsetAsync(w->flags, 0, sizeof(int) * F_COUNT, s));
-        LAB_CUDA(cudaMallocHost(&w->hflags, sizeof(int) * F_COUNT * 2));
-        LAB_CUDA(cudaEventCreateWithFlags(&w->ev[0], cudaEventDisableTiming));
-        LAB_CUDA(cudaEventCreateWithFlags(&w->ev[1], cudaEventDisableTiming));
-        LAB_CUDA(cudaStreamCreateWithFlags(&w->cap, cudaStreamNonBlocking));
+        LAB_CUDA(cudaGetDevice(&w->dev));
+        pcg_host_res res;
+        LAB_TRY(res_take(w->dev, &res));
+        w->hflags = res.hflags;
+        w->ev[0]  = res.ev[0];
+        w->ev[1]  = res.ev[1];
+        w->cap    = res.cap;
         return LAB_OK;
     }
 
