@@ -395,7 +395,9 @@ typedef enum lab_smoother
 
 typedef enum lab_coarse
 {
-    LAB_COARSE_DIRECT = 0, /* dense inverse built at setup, applied as a dense matvec */
+    LAB_COARSE_DIRECT = 0, /* dense inverse (Gauss-Jordan with partial pivoting) built with
+                              the preconditioner, applied as a dense matvec; a coarsest
+                              level above 4096 rows falls back to LAB_COARSE_GS */
     LAB_COARSE_GS     = 1  /* the reference's 1000 (V) / 100 (W, F) lexicographic GS sweeps */
 } lab_coarse;
 
