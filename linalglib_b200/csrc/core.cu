@@ -589,11 +589,50 @@ namespace lab
         }
     }
 
+    // Short arrays (n <= kScanSmall): one CTA takes the tiles in sequence with a
+    // running carry -- one launch instead of three (the setup scans many short
+    // per-level arrays, where the launches cost more than the work).
+    constexpr int64_t kScanSmall = 4 * kScanTile;
+
+    template <class T>
+    __global__ void __launch_bounds__(kScanThreads) k_scan_small(T* x, int64_t n)
+    {
+        __shared__ T sw[32];
+        __shared__ T tot;
+        T            carry = 0;
+        for(int64_t t0 = 0; t0 < n; t0 += kScanTile)
+        {
+            const int64_t base = t0 + (int64_t)threadIdx.x * kScanItems;
+            T             loc[kScanItems];
+            T             s = 0;
+#pragma unroll
+            for(int k = 0; k < kScanItems; k++)
+            {
+                loc[k] = (base + k < n) ? x[base + k] : T(0);
+                s += loc[k];
+            }
+            T ex = block_exclusive_scan<T>(s, sw, &tot) + carry;
+#pragma unroll
+            for(int k = 0; k < kScanItems; k++)
+            {
+                if(base + k < n)
+                    x[base + k] = ex;
+                ex += loc[k];
+            }
+            carry += tot; // read by every thread before the next tile's scan writes it
+        }
+    }
+
     template <class T>
     static lab_status scan_impl(T* x, int64_t n, cudaStream_t s)
     {
         if(n <= 0)
             return LAB_OK;
+        if(n <= kScanSmall)
+        {
+            LAB_LAUNCH(k_scan_small<T>, 1, kScanThreads, 0, s, x, n);
+            return LAB_OK;
+        }
         int64_t nb = ceil_div<int64_t>(n, kScanTile);
         dbuf<T> bsum;
         LAB_TRY(bsum.alloc((size_t)nb, s));
