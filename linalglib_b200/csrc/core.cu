@@ -594,8 +594,10 @@ namespace lab
     // per-level arrays, where the launches cost more than the work).
     constexpr int64_t kScanSmall = 4 * kScanTile;
 
+    // x[0..n) = exclusive scan of src[0..n_src) followed by zeros (src may be x).
     template <class T>
-    __global__ void __launch_bounds__(kScanThreads) k_scan_small(T* x, int64_t n)
+    __global__ void __launch_bounds__(kScanThreads)
+        k_scan_small(const T* src, int64_t n_src, T* x, int64_t n)
     {
         __shared__ T sw[32];
         __shared__ T tot;
@@ -608,7 +610,7 @@ namespace lab
 #pragma unroll
             for(int k = 0; k < kScanItems; k++)
             {
-                loc[k] = (base + k < n) ? x[base + k] : T(0);
+                loc[k] = (base + k < n_src) ? src[base + k] : T(0);
                 s += loc[k];
             }
             T ex = block_exclusive_scan<T>(s, sw, &tot) + carry;
@@ -630,7 +632,7 @@ namespace lab
             return LAB_OK;
         if(n <= kScanSmall)
         {
-            LAB_LAUNCH(k_scan_small<T>, 1, kScanThreads, 0, s, x, n);
+            LAB_LAUNCH(k_scan_small<T>, 1, kScanThreads, 0, s, (const T*)x, n, x, n);
             return LAB_OK;
         }
         int64_t nb = ceil_div<int64_t>(n, kScanTile);
@@ -677,13 +679,21 @@ namespace lab
     lab_status counts_to_rowptr(const int32_t* counts, int32_t* rp, int64_t n, int64_t* total,
                                 cudaStream_t s)
     {
-        if(counts != rp)
-            LAB_LAUNCH(k_counts_to_rowptr, (unsigned)ceil_div<int64_t>(n + 1, 256), 256, 0, s,
-                       counts, rp, n);
+        if(n + 1 <= kScanSmall)
+        {
+            // one launch: the counts (and a zero for rp[n]) scanned straight into rp
+            LAB_LAUNCH(k_scan_small<int32_t>, 1, kScanThreads, 0, s, counts, n, rp, n + 1);
+        }
         else
-            LAB_CUDA(cudaMemsetAsync(rp + n, 0, sizeof(int32_t), s));
+        {
+            if(counts != rp)
+                LAB_LAUNCH(k_counts_to_rowptr, (unsigned)ceil_div<int64_t>(n + 1, 256), 256, 0, s,
+                           counts, rp, n);
+            else
+                LAB_CUDA(cudaMemsetAsync(rp + n, 0, sizeof(int32_t), s));
+            LAB_TRY(scan_i32(rp, n + 1, s));
+        }
         // 64-bit total check: counts are int32 and sums above 2^31 would wrap.
-        LAB_TRY(scan_i32(rp, n + 1, s));
         if(total)
         {
             int32_t t = 0;
